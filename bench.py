@@ -1,0 +1,439 @@
+#!/usr/bin/env python
+"""Benchmark of the per-frame warp-field Gauss-Newton solve.
+
+Metric: ms per GN solve at N=2048 nodes / M~300k correspondences (the
+640x480 two-cylinder frame), 5 GN x 20 PCG iterations.  One step = one full
+solve: re-skin, assemble, block-Jacobi PCG and the clamped DQ node update for
+every GN iteration, then the energy at the final transforms.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Multi-GPU runs (torchrun, one rank per GPU) are independent replicas: the
+solve of one frame does not shard (it needs a global reduction every PCG
+iteration and is L2-sized), so each rank solves its own copy of the frame
+and the job-level figure is the max-over-ranks time / (N * K).
+
+`--impl reference` times CUDAFusion's own solver (kernels/solver_kernels.cu,
+src/warp_field.cu) rebuilt for sm_100a, on the same inputs and parameters.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ms/GN solve at 2k nodes/300k corr, learned-init vs plain at equal energy"
+L2_FLUSH_BYTES = 256 << 20
+HBM_FALLBACK_GBS = 6650.0
+
+# solve parameters of the workload: GaussNewtonSolver::Params defaults
+# (include/solver.h:15-21) with 5 GN x 20 PCG iterations, and the per-node
+# update clamps of config/params.yaml:45-46 (max_update_rot/trans)
+GN_ITERS, PCG_ITERS, PCG_TOL, LAMBDA_SMOOTH, LAMBDA_DAMP = 5, 20, 1e-4, 1.0, 1e-2
+MAX_ROT, MAX_TRANS, UPDATE_SCALE = 0.12, 0.04, 1.0
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = (
+        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+        "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    import torch
+
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def algorithmic_bytes(N, M, nnzb, pcg_iters_used):
+    """Algorithmic bytes per launch of the hot kernels (the per-unit counts of
+    the workload model: a correspondence payload of 72 B read once, node DQs
+    and nodes, the BSR values written once; per PCG iteration the BSR values
+    and column indices, the block-Jacobi inverses and 12 passes over 6N-float
+    vectors)."""
+    b_asm = 72 * M + N * (32 + 96) + nnzb * 144 + 24 * N + 8
+    b_pcg_it = nnzb * (144 + 4) + 4 * (N + 1) + 144 * N + 12 * 24 * N
+    return {"assembly": b_asm, "pcg": b_pcg_it * pcg_iters_used, "pcg_per_iteration": b_pcg_it}
+
+
+def cpu_baseline(problem, nthreads, reps=3):
+    """The oracle (FP32, reference operation order) on the host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    prm = O.params(gn_iterations=GN_ITERS, pcg_iterations=PCG_ITERS, pcg_tolerance=PCG_TOL,
+                   lambda_smooth=LAMBDA_SMOOTH, lambda_damping=LAMBDA_DAMP)
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        O.gn_solve(problem, prm, max_rot=MAX_ROT, max_trans=MAX_TRANS, scale=UPDATE_SCALE, precision="f32",
+                   nthreads=nthreads)
+        times.append((time.perf_counter() - t0) * 1e3)
+    return {
+        "value": statistics.median(times),
+        "unit": "ms",
+        "cores": nthreads,
+        "kind": "port",
+        "sample": f"the full solve of the same frame ({GN_ITERS} GN x {PCG_ITERS} PCG), median of {reps}, "
+                  "FP32 C oracle with OpenMP",
+    }
+
+
+def load_traffic(kernel):
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            d = json.load(f)
+        return d.get(kernel, {}).get("dram_bytes_per_launch")
+    except Exception:
+        return None
+
+
+def run_b200(args, world, rank, local):
+    import torch
+
+    from cudafusion_b200 import synth
+    from cudafusion_b200.solver import DeviceProblem, GaussNewtonSolver, Params
+
+    problem = synth.config2()
+    N, M = problem.num_nodes, problem.num_corrs
+    prm = Params(gn_iterations=GN_ITERS, pcg_iterations=PCG_ITERS, pcg_tolerance=PCG_TOL,
+                 lambda_smooth=LAMBDA_SMOOTH, lambda_damping=LAMBDA_DAMP)
+    solver = GaussNewtonSolver(prm, max_nodes=8192, max_corrs=max(M, 1))
+    dp = DeviceProblem(problem)
+    T = dp.init_transforms.clone()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    def step():
+        T.copy_(dp.init_transforms)
+        flush.fill_(1)
+        solver.gn_solve(dp, T, MAX_ROT, MAX_TRANS, UPDATE_SCALE, stats=False)
+
+    stats = solver.gn_solve(dp, T, MAX_ROT, MAX_TRANS, UPDATE_SCALE, stats=True)
+    for _ in range(args.warmup):
+        step()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    sampler = ClockSampler(local) if rank == 0 else None
+    barrier(world)
+    if sampler:
+        sampler.start()
+    launches0 = solver.launch_count()
+    solver.profile_enable(True)
+    t_wall = time.perf_counter()
+    for k in range(args.steps):
+        T.copy_(dp.init_transforms)
+        flush.fill_(1)
+        evs[k][0].record()
+        solver.gn_solve(dp, T, MAX_ROT, MAX_TRANS, UPDATE_SCALE, stats=False)
+        evs[k][1].record()
+    barrier(world)
+    t_wall = time.perf_counter() - t_wall
+    clocks = sampler.stop() if sampler else None
+    phases = solver.profile_read()
+    solver.profile_enable(False)
+    launches = solver.launch_count() - launches0
+    per_step = [a.elapsed_time(b) for a, b in evs]
+    total_ms = max_over_ranks(sum(per_step), world)
+    value = total_ms / (args.steps * world)
+
+    # end to end through the public API: pinned host inputs -> device, solve,
+    # transforms + energy back to the host, every step
+    h_nodes = torch.from_numpy(problem.nodes.view(np.uint8).reshape(-1).copy()).pin_memory()
+    h_canon = torch.from_numpy(np.ascontiguousarray(problem.canon)).pin_memory()
+    h_corrs = torch.from_numpy(problem.corrs.view(np.uint8).reshape(-1).copy()).pin_memory()
+    h_T0 = torch.from_numpy(problem.init_transforms.view(np.uint8).reshape(-1).copy()).pin_memory()
+    h_Tout = torch.empty_like(h_T0).pin_memory()
+    e2e_steps = max(3, min(args.steps, 10))
+    barrier(world)
+    e2e_times = []
+    for k in range(e2e_steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        dp.nodes.copy_(h_nodes, non_blocking=True)
+        dp.canon.copy_(h_canon, non_blocking=True)
+        dp.corrs.copy_(h_corrs, non_blocking=True)
+        T.copy_(h_T0, non_blocking=True)
+        st = solver.gn_solve(dp, T, MAX_ROT, MAX_TRANS, UPDATE_SCALE, stats=True)
+        h_Tout.copy_(T, non_blocking=True)
+        b.record()
+        torch.cuda.synchronize()
+        e2e_times.append(a.elapsed_time(b))
+    e2e_ms = max_over_ranks(sum(e2e_times), world) / (e2e_steps * world)
+    h2d = h_nodes.numel() + h_canon.numel() * 4 + h_corrs.numel() + h_T0.numel()
+    d2h = h_Tout.numel() + 8 * (2 * 32 + 33) + 4 * 34  # transforms + the stats record + error word
+
+    if rank != 0:
+        return None
+    hbm, peak_kind = peaks()
+    pcg_used = sum(stats["pcg_iterations"]) / max(1, len(stats["pcg_iterations"]))
+    ab = algorithmic_bytes(N, M, stats["num_blocks"], pcg_used)
+    kernels = {}
+    for name, (ms, n) in phases.items():
+        kernels[name] = {"ms_per_launch": ms / max(n, 1), "launches": n, "share": None, "ms_total": ms}
+    tot = sum(v["ms_total"] for v in kernels.values()) or 1.0
+    for v in kernels.values():
+        v["share"] = v["ms_total"] / tot
+    dom = max(kernels, key=lambda k: kernels[k]["ms_total"])
+    roof = None
+    if dom in ("pcg", "assemble", "residual"):
+        key = "pcg" if dom == "pcg" else "assembly"
+        dur = kernels[dom]["ms_per_launch"]
+        if key == "assembly":
+            dur = kernels.get("assemble", {}).get("ms_per_launch", 0) + kernels.get("residual", {}).get("ms_per_launch", 0)
+        achieved = ab[key] / (dur * 1e-3) / 1e9
+        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": load_traffic(dom), "algorithmic_bytes_per_launch": ab[key],
+                "ms_per_launch": dur, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
+    nthreads = os.cpu_count() or 1
+    cpu = cpu_baseline(problem, nthreads) if not args.no_cpu_baseline else None
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "ms",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": value * world,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": f"two-cylinder 640x480 frame, N={N} nodes, M={M} correspondences, "
+                        f"{GN_ITERS} GN x {PCG_ITERS} PCG, plain init",
+            "nodes": N, "corrs": M, "gn_iterations": GN_ITERS, "pcg_iterations": PCG_ITERS,
+            "pcg_tolerance": PCG_TOL, "lambda_smooth": LAMBDA_SMOOTH, "lambda_damping": LAMBDA_DAMP,
+            "max_rot": MAX_ROT, "max_trans": MAX_TRANS, "l2": "flushed between steps (256 MiB write)",
+            "parallelism": f"replicas x{world}", "blocks": stats["num_blocks"],
+        },
+        "roofline": roof,
+        "kernels": kernels,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "gpu_launches_per_step": launches / args.steps,
+        "clocks": clocks,
+        "energy_initial": stats["energy_initial"],
+        "energy_final": stats["energy_final"],
+        "pcg_iterations": stats["pcg_iterations"],
+        "wall_s_timed_region": t_wall,
+    }
+    return line
+
+
+def run_reference(args, world, rank, local):
+    import torch
+
+    if rank != 0:
+        return None
+    so = os.path.join(ROOT, "oracle", "_ref", "libcfref_cuda.so")
+    if not os.path.exists(so):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libcfref_cuda.so was not built "
+                "(needs the reference sources: make -C oracle ref)"}
+    from cudafusion_b200 import synth
+
+    ref = ctypes.CDLL(so)
+    ref.ref_create.restype = ctypes.c_void_p
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    problem = synth.config2()
+    N, M = problem.num_nodes, problem.num_corrs
+    ip = (ctypes.c_int * 3)(GN_ITERS, PCG_ITERS, 0)
+    fp = (ctypes.c_float * 4)(PCG_TOL, LAMBDA_SMOOTH, 1.0, LAMBDA_DAMP)
+    h = ctypes.c_void_p(ref.ref_create(ip, fp, 8192))
+    rc = ref.ref_upload(h, P(problem.nodes), N, P(problem.canon), P(problem.corrs), M, P(problem.init_transforms))
+    if rc != 0:
+        return {"impl": "reference", "unavailable": f"reference upload failed with cudaError {rc}"}
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    ms = ctypes.c_float()
+
+    def one():
+        ref.ref_set_transforms(h, P(problem.init_transforms), N)
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        rc = ref.ref_gn_solve_timed(h, GN_ITERS, ctypes.c_float(MAX_ROT), ctypes.c_float(MAX_TRANS),
+                                    ctypes.c_float(UPDATE_SCALE), ctypes.byref(ms))
+        if rc != 0:
+            raise RuntimeError(f"reference solve failed with cudaError {rc}")
+        return ms.value
+
+    for _ in range(args.warmup):
+        one()
+    sampler = ClockSampler(local)
+    sampler.start()
+    times = [one() for _ in range(args.steps)]
+    clocks = sampler.stop()
+    value = sum(times) / len(times)
+    # end to end: host structs uploaded by the reference's own DeviceArray /
+    # WarpField uploads, solve, transforms downloaded
+    Tout = np.zeros(N, problem.init_transforms.dtype)
+    e2e = []
+    for _ in range(max(3, min(args.steps, 5))):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ref.ref_upload(h, P(problem.nodes), N, P(problem.canon), P(problem.corrs), M, P(problem.init_transforms))
+        ref.ref_gn_solve(h, GN_ITERS, ctypes.c_float(MAX_ROT), ctypes.c_float(MAX_TRANS), ctypes.c_float(UPDATE_SCALE))
+        ref.ref_get_transforms(h, P(Tout), N)
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    h2d = problem.nodes.nbytes + problem.canon.nbytes + problem.corrs.nbytes + 2 * problem.init_transforms.nbytes
+    return {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "ms",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": value,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": f"two-cylinder 640x480 frame, N={N} nodes, M={M} correspondences, "
+                        f"{GN_ITERS} GN x {PCG_ITERS} PCG, plain init",
+            "implementation": "CUDAFusion GaussNewtonSolver::solve + WarpField::apply_twist_increment + warp_point, "
+                              "rebuilt for sm_100a with --use_fast_math (oracle/_ref/libcfref_cuda.so)",
+            "l2": "flushed between steps (256 MiB write)",
+            "parallelism": "single GPU (rank 0 of the launch)",
+        },
+        "cpu_baseline": {"value": value, "unit": "ms", "cores": 1, "kind": "reference",
+                         "sample": "the reference path is CUDA: the full solve timed on the GPU, one host thread"},
+        "e2e": {"value": statistics.median(e2e), "unit": "ms", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(problem.init_transforms.nbytes)},
+        "clocks": clocks,
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            line = run_reference(args, world, rank, local)
+        else:
+            line = run_b200(args, world, rank, local)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,148 @@
+"""ctypes binding of the C ABI (include/cudafusion_b200.h).
+
+Loading fails loudly when libcfb200.so is missing: there is no fallback path.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcfb200.so")
+
+CF_OK = 0
+CF_ERR_INVALID_ARG = 1
+CF_ERR_OOM = 2
+CF_ERR_NON_FINITE = 3
+CF_ERR_TIMEOUT = 4
+CF_ERR_CUDA = 5
+CF_ERR_CAPACITY = 6
+CF_ERR_NOT_IMPLEMENTED = 7
+CF_ERR_NO_DEVICE = 8
+
+CF_OPT_ARAP_CONSISTENT = 1
+CF_OPT_PCG_CTAS = 2
+CF_MAX_GN_ITERS = 32
+CF_PROF_SLOTS = 12
+
+# Every symbol the public header declares (the ABI test checks the list
+# against include/cudafusion_b200.h).
+EXPORTS = [
+    "cf_status_string",
+    "cf_gn_params_default",
+    "cf_gn_create",
+    "cf_gn_destroy",
+    "cf_gn_set_params",
+    "cf_gn_get_params",
+    "cf_gn_set_option",
+    "cf_gn_check",
+    "cf_gn_linearize_solve",
+    "cf_gn_invalidate_pattern",
+    "cf_gn_get_system",
+    "cf_gn_solve",
+    "cf_warp_apply_twist",
+    "cf_warp_skin_points",
+    "cf_gn_profile_enable",
+    "cf_gn_profile_read",
+    "cf_gn_profile_name",
+    "cf_gn_launch_count",
+    "cf_get_version",
+    "cf_last_cuda_error",
+]
+
+
+class GNParams(ctypes.Structure):
+    """cf_gn_params = GaussNewtonSolver::Params (include/solver.h:13-22)."""
+
+    _fields_ = [
+        ("gn_iterations", ctypes.c_int),
+        ("pcg_iterations", ctypes.c_int),
+        ("pcg_tolerance", ctypes.c_float),
+        ("lambda_smooth", ctypes.c_float),
+        ("lambda_rot", ctypes.c_float),
+        ("lambda_damping", ctypes.c_float),
+        ("debug", ctypes.c_int),
+    ]
+
+
+class Problem(ctypes.Structure):
+    _fields_ = [
+        ("nodes", ctypes.c_void_p),
+        ("num_nodes", ctypes.c_int),
+        ("canon_points", ctypes.c_void_p),
+        ("corrs", ctypes.c_void_p),
+        ("num_corrs", ctypes.c_int),
+        ("max_rot", ctypes.c_float),
+        ("max_trans", ctypes.c_float),
+        ("update_scale", ctypes.c_float),
+    ]
+
+
+class SolveStats(ctypes.Structure):
+    _fields_ = [
+        ("energy_initial", ctypes.c_double),
+        ("energy_final", ctypes.c_double),
+        ("energy_per_iter", ctypes.c_double * CF_MAX_GN_ITERS),
+        ("pcg_iterations", ctypes.c_int * CF_MAX_GN_ITERS),
+        ("pcg_residual", ctypes.c_double * CF_MAX_GN_ITERS),
+        ("gn_iterations_run", ctypes.c_int),
+        ("num_blocks", ctypes.c_int),
+        ("precond_fallbacks", ctypes.c_int),
+        ("error_flags", ctypes.c_int),
+    ]
+
+
+class CFError(RuntimeError):
+    def __init__(self, status, where=""):
+        self.status = status
+        msg = lib().cf_status_string(status).decode()
+        buf = ctypes.create_string_buffer(256)
+        lib().cf_last_cuda_error(buf, 256)
+        detail = buf.value.decode()
+        super().__init__(f"{where}: {msg} ({status})" + (f" [{detail}]" if detail else ""))
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m cudafusion_b200.build` "
+                "(there is no CPU fallback)"
+            )
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i, f = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+        L.cf_status_string.restype = ctypes.c_char_p
+        L.cf_status_string.argtypes = [i]
+        L.cf_gn_profile_name.restype = ctypes.c_char_p
+        L.cf_gn_params_default.argtypes = [ctypes.POINTER(GNParams)]
+        L.cf_gn_create.argtypes = [ctypes.POINTER(GNParams), i, i, ctypes.POINTER(vp)]
+        L.cf_gn_destroy.argtypes = [vp]
+        L.cf_gn_set_params.argtypes = [vp, ctypes.POINTER(GNParams)]
+        L.cf_gn_get_params.argtypes = [vp, ctypes.POINTER(GNParams)]
+        L.cf_gn_set_option.argtypes = [vp, i, i]
+        L.cf_gn_check.argtypes = [vp, vp]
+        L.cf_gn_linearize_solve.argtypes = [vp, vp, i, vp, vp, i, vp, vp]
+        L.cf_gn_invalidate_pattern.argtypes = [vp]
+        L.cf_gn_get_system.argtypes = [vp, ctypes.POINTER(i), ctypes.POINTER(i), vp, vp, vp, vp, vp]
+        L.cf_gn_solve.argtypes = [vp, ctypes.POINTER(Problem), vp, ctypes.POINTER(SolveStats), vp]
+        L.cf_warp_apply_twist.argtypes = [vp, vp, i, f, f, f, vp]
+        L.cf_warp_skin_points.argtypes = [vp, vp, vp, i, vp, vp, i, vp, vp]
+        L.cf_gn_profile_enable.argtypes = [vp, i]
+        L.cf_gn_profile_read.argtypes = [vp, vp, vp, i]
+        L.cf_gn_profile_name.argtypes = [i]
+        L.cf_gn_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+        L.cf_get_version.argtypes = [ctypes.POINTER(i)] * 3
+        L.cf_last_cuda_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+        for name in EXPORTS:
+            if name not in ("cf_status_string", "cf_gn_profile_name"):
+                getattr(L, name).restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def check(status, where=""):
+    if status != CF_OK:
+        raise CFError(status, where)
+    return status

@@ -1,0 +1,646 @@
+// cf_api.cu — C ABI of the warp-field solve (include/cudafusion_b200.h).
+//
+// Host-side responsibilities: argument checks and status codes, the block
+// pattern (built on the host from the node graph like the reference,
+// kernels/solver_kernels.cu:498-541), the PCG row partition, and the launch
+// sequence.  Every device computation happens in cf_kernels.cu.
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "cf_internal.h"
+
+using namespace cf;
+
+// Phase slots of the profiler (cf_gn_profile_*).
+enum ProfSlot {
+  kProfPack = 0, kProfBinScan, kProfScatter, kProfExpand, kProfNodePlain, kProfResidual, kProfAssemble,
+  kProfPcg, kProfEnergy, kProfTwist, kProfSkin, kProfOther
+};
+static const char* kProfNames[CF_PROF_SLOTS] = {"pack_count", "bin_scan", "bin_scatter", "expand",
+                                                "node_plain", "residual", "assemble", "pcg",
+                                                "final_energy", "apply_twist", "skin_points", "other"};
+
+struct ProfEvent {
+  int slot;
+  cudaEvent_t a, b;
+};
+
+struct cf_gn {
+  cf_gn_params params;
+  int max_nodes = 0, max_corrs = 0;
+  int device = 0, sms = 0;
+  int arap_consistent = 0;
+  int pcg_ctas_override = 0;
+  Work w;
+  Pattern p;
+  int pattern_N = -1;
+  bool pattern_valid = false;
+  std::vector<int> h_row_ptr, h_col_idx;
+  DevStats* h_stats = nullptr;  // pinned
+  int last_gn = 0;
+  long long launches = 0;
+  bool profile = false;
+  std::vector<ProfEvent> prof_pool;  // events created once, reused
+  size_t prof_used = 0;
+  double prof_ms[CF_PROF_SLOTS] = {0};
+  int prof_n[CF_PROF_SLOTS] = {0};
+};
+
+namespace {
+
+thread_local char g_last_error[256] = {0};
+
+cf_status from_cuda(cudaError_t e) {
+  if (e == cudaSuccess) return CF_OK;
+  snprintf(g_last_error, sizeof(g_last_error), "%s", cudaGetErrorString(e));
+  if (e == cudaErrorMemoryAllocation) return CF_ERR_OOM;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return CF_ERR_NO_DEVICE;
+  return CF_ERR_CUDA;
+}
+
+#define CF_TRY(expr)                        \
+  do {                                      \
+    cudaError_t e_ = (expr);                \
+    if (e_ != cudaSuccess) return from_cuda(e_); \
+  } while (0)
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  return cudaMalloc((void**)p, n * sizeof(T));
+}
+
+template <typename T>
+void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+void free_pattern(Pattern& p) {
+  dfree(p.row_ptr); dfree(p.col_idx); dfree(p.diag_pos); dfree(p.trans_pos);
+  dfree(p.upper_pos); dfree(p.upper_row); dfree(p.arap_row_ptr); dfree(p.arap_row_inc);
+  dfree(p.arap_blk_ptr); dfree(p.arap_blk_edge); dfree(p.edge_ijk); dfree(p.values);
+  dfree(p.seg_off); dfree(p.seg_cnt); dfree(p.pcg_row_begin);
+  p = Pattern();
+}
+
+void free_work(Work& w) {
+  dfree(w.pk_src); dfree(w.pk_dst); dfree(w.pk_nrm); dfree(w.pk_ids); dfree(w.pk_ws);
+  dfree(w.c_srcfw); dfree(w.c_nres); dfree(w.cnt); dfree(w.node_total); dfree(w.inc_start);
+  dfree(w.inc); dfree(w.trip); dfree(w.rhs); dfree(w.plain); dfree(w.x); dfree(w.z); dfree(w.p0); dfree(w.p1);
+  dfree(w.partials); dfree(w.barrier); dfree(w.err); dfree(w.e_data_part); dfree(w.e_arap_part); dfree(w.stats);
+}
+
+cudaError_t alloc_work(Work& w, int max_nodes, int max_corrs, int bin_ctas_max) {
+  w.max_nodes = max_nodes;
+  w.max_corrs = max_corrs;
+  w.bin_ctas_max = bin_ctas_max;
+  size_t M = (size_t)max_corrs, N = (size_t)max_nodes;
+  cudaError_t e;
+#define A_(ptr, n) if ((e = dalloc(&(ptr), (n))) != cudaSuccess) return e
+  A_(w.pk_src, M); A_(w.pk_dst, M); A_(w.pk_nrm, M); A_(w.pk_ids, M); A_(w.pk_ws, M);
+  A_(w.c_srcfw, M); A_(w.c_nres, M);
+  A_(w.cnt, (size_t)bin_ctas_max * N); A_(w.node_total, N); A_(w.inc_start, N + 1);
+  A_(w.inc, 4 * M); A_(w.trip, 16 * M);
+  A_(w.rhs, 6 * N); A_(w.plain, N); A_(w.x, 6 * N); A_(w.z, 6 * N); A_(w.p0, 6 * N); A_(w.p1, 6 * N);
+  A_(w.partials, (size_t)2 * 2 * kMaxPcgCtas); A_(w.barrier, 1); A_(w.err, 1);
+  A_(w.e_data_part, (size_t)kEnergyCtas); A_(w.e_arap_part, N); A_(w.stats, 1);
+#undef A_
+  return cudaSuccess;
+}
+
+int cdiv(int a, int b) { return (a + b - 1) / b; }
+
+// Brackets one launch (or a short launch sequence) of phase `slot` with
+// events when profiling is on; counts kernel launches always.
+struct Timed {
+  cf_gn* h;
+  cudaStream_t s;
+  ProfEvent* ev = nullptr;
+  Timed(cf_gn* h_, cudaStream_t s_, int slot, int nkernels) : h(h_), s(s_) {
+    h->launches += nkernels;
+    if (!h->profile) return;
+    if (h->prof_used == h->prof_pool.size()) {
+      ProfEvent pe;
+      pe.slot = slot;
+      cudaEventCreate(&pe.a);
+      cudaEventCreate(&pe.b);
+      h->prof_pool.push_back(pe);
+    }
+    ev = &h->prof_pool[h->prof_used++];
+    ev->slot = slot;
+    h->prof_n[slot] += nkernels;
+    cudaEventRecord(ev->a, s);
+  }
+  ~Timed() {
+    if (ev) cudaEventRecord(ev->b, s);
+  }
+};
+
+// Folds recorded event pairs into the per-slot totals (synchronises).
+void prof_collect(cf_gn* h) {
+  for (size_t i = 0; i < h->prof_used; i++) {
+    ProfEvent& pe = h->prof_pool[i];
+    cudaEventSynchronize(pe.b);
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, pe.a, pe.b) == cudaSuccess) h->prof_ms[pe.slot] += ms;
+  }
+  h->prof_used = 0;
+}
+
+// Builds the pattern and every topology-derived array from host nodes.
+cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes, int N) {
+  // kernels/solver_kernels.cu:498-541: diagonal + directed edges both ways
+  std::vector<std::vector<int>> rows(N);
+  for (int i = 0; i < N; i++) rows[i].push_back(i);
+  for (int i = 0; i < N; i++) {
+    int nn = std::min(nodes[i].num_neighbors, CF_K_GRAPH);
+    for (int k = 0; k < nn; k++) {
+      int nb = nodes[i].neighbors[k];
+      if (nb < 0 || nb >= N) continue;
+      rows[i].push_back(nb);
+      rows[nb].push_back(i);
+    }
+  }
+  std::vector<int> row_ptr(N + 1), col_idx;
+  for (int i = 0; i < N; i++) {
+    row_ptr[i] = (int)col_idx.size();
+    auto& c = rows[i];
+    std::sort(c.begin(), c.end());
+    c.erase(std::unique(c.begin(), c.end()), c.end());
+    col_idx.insert(col_idx.end(), c.begin(), c.end());
+  }
+  row_ptr[N] = (int)col_idx.size();
+  const int nnzb = row_ptr[N];
+  auto find = [&](int r, int c) -> int {
+    auto b = col_idx.begin() + row_ptr[r], e = col_idx.begin() + row_ptr[r + 1];
+    auto it = std::lower_bound(b, e, c);
+    return (it != e && *it == c) ? (int)(it - col_idx.begin()) : -1;
+  };
+  std::vector<int> diag_pos(N), trans_pos(nnzb), upper_pos, upper_row, upper_of_pos(nnzb, -1);
+  int max_up = 1;
+  for (int i = 0; i < N; i++) {
+    diag_pos[i] = find(i, i);
+    for (int q = row_ptr[i]; q < row_ptr[i + 1]; q++) trans_pos[q] = find(col_idx[q], i);
+    for (int q = diag_pos[i]; q < row_ptr[i + 1]; q++) {
+      upper_of_pos[q] = (int)upper_pos.size();
+      upper_pos.push_back(q);
+      upper_row.push_back(i);
+    }
+    max_up = std::max(max_up, row_ptr[i + 1] - diag_pos[i]);
+  }
+  const int n_upper = (int)upper_pos.size();
+  // ARAP edges in the reference's visiting order (solver_kernels.cu:225-233)
+  std::vector<int> eijk;
+  for (int i = 0; i < N; i++) {
+    int nn = std::min(nodes[i].num_neighbors, CF_K_GRAPH);
+    for (int k = 0; k < nn; k++) {
+      int j = nodes[i].neighbors[k];
+      if (j < 0 || j >= N || j <= i) continue;
+      eijk.push_back(i); eijk.push_back(j); eijk.push_back(k);
+    }
+  }
+  const int n_edges = (int)eijk.size() / 3;
+  std::vector<int> arow_ptr(N + 1, 0), ablk_ptr(n_upper + 1, 0);
+  for (int e = 0; e < n_edges; e++) {
+    arow_ptr[eijk[3 * e] + 1]++;
+    arow_ptr[eijk[3 * e + 1] + 1]++;
+    int u = upper_of_pos[find(eijk[3 * e], eijk[3 * e + 1])];
+    ablk_ptr[u + 1]++;
+  }
+  for (int i = 0; i < N; i++) arow_ptr[i + 1] += arow_ptr[i];
+  for (int u = 0; u < n_upper; u++) ablk_ptr[u + 1] += ablk_ptr[u];
+  std::vector<int> arow_inc(std::max(1, arow_ptr[N])), ablk_edge(std::max(1, ablk_ptr[n_upper]));
+  {
+    std::vector<int> fr(arow_ptr.begin(), arow_ptr.end() - 1), fb(ablk_ptr.begin(), ablk_ptr.end() - 1);
+    for (int e = 0; e < n_edges; e++) {
+      int i = eijk[3 * e], j = eijk[3 * e + 1];
+      arow_inc[fr[i]++] = (e << 1) | 0;
+      arow_inc[fr[j]++] = (e << 1) | 1;
+      ablk_edge[fb[upper_of_pos[find(i, j)]]++] = e;
+    }
+  }
+  // PCG partition: contiguous rows with balanced block counts
+  int G = h->pcg_ctas_override > 0 ? h->pcg_ctas_override : std::min(h->sms, std::max(1, N / 8));
+  G = std::max(1, std::min({G, N, kMaxPcgCtas}));
+  std::vector<int> rb;
+  int smem = 0;
+  bool a_smem = true;
+  for (int attempt = 0; attempt < 64; attempt++) {
+    rb.assign(1, 0);
+    long long target = ((long long)nnzb + G - 1) / G;
+    int start = 0;
+    for (int c = 0; c < G; c++) {
+      int remaining_ctas = G - c;
+      if (start >= N) { rb.push_back(N); continue; }
+      int end = start + 1;
+      if (remaining_ctas == 1) {
+        end = N;
+      } else {
+        while (end < N - (remaining_ctas - 1) && row_ptr[end] - row_ptr[start] < target) end++;
+      }
+      rb.push_back(end);
+      start = end;
+    }
+    rb.back() = N;
+    int max_b = 0, max_r = 0;
+    for (int c = 0; c < G; c++) {
+      max_b = std::max(max_b, row_ptr[rb[c + 1]] - row_ptr[rb[c]]);
+      max_r = std::max(max_r, rb[c + 1] - rb[c]);
+    }
+    const int limit = 200 * 1024;
+    a_smem = true;
+    smem = pcg_smem_bytes(max_b, max_r, true);
+    if (smem > limit) {
+      a_smem = false;
+      smem = pcg_smem_bytes(max_b, max_r, false);
+    }
+    if (smem > limit) {
+      if (G >= std::min(N, kMaxPcgCtas)) return CF_ERR_CAPACITY;
+      G = std::min(std::min(N, kMaxPcgCtas), G * 2);
+      continue;
+    }
+    CF_TRY(pcg_prepare(smem, a_smem));
+    int cap = pcg_max_active_ctas(smem, a_smem);
+    if (cap <= 0) return CF_ERR_CAPACITY;
+    if (G > cap) {
+      G = cap;
+      continue;
+    }
+    break;
+  }
+  // the rows of a CTA must not be empty
+  std::vector<int> rb2(1, 0);
+  for (size_t c = 1; c < rb.size(); c++)
+    if (rb[c] > rb2.back()) rb2.push_back(rb[c]);
+  G = (int)rb2.size() - 1;
+
+  free_pattern(h->p);
+  Pattern& p = h->p;
+  p.N = N;
+  p.nnzb = nnzb;
+  p.n_upper = n_upper;
+  p.n_edges = n_edges;
+  p.max_upper_row = max_up;
+  p.pcg_ctas = G;
+  p.pcg_smem = smem;
+  p.pcg_a_in_smem = a_smem ? 1 : 0;
+  auto up = [](int** d, const std::vector<int>& v) -> cudaError_t {
+    cudaError_t e = dalloc(d, v.size());
+    if (e != cudaSuccess) return e;
+    return v.empty() ? cudaSuccess : cudaMemcpy(*d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice);
+  };
+  CF_TRY(up(&p.row_ptr, row_ptr));
+  CF_TRY(up(&p.col_idx, col_idx));
+  CF_TRY(up(&p.diag_pos, diag_pos));
+  CF_TRY(up(&p.trans_pos, trans_pos));
+  CF_TRY(up(&p.upper_pos, upper_pos));
+  CF_TRY(up(&p.upper_row, upper_row));
+  CF_TRY(up(&p.arap_row_ptr, arow_ptr));
+  CF_TRY(up(&p.arap_row_inc, arow_inc));
+  CF_TRY(up(&p.arap_blk_ptr, ablk_ptr));
+  CF_TRY(up(&p.arap_blk_edge, ablk_edge));
+  CF_TRY(up(&p.edge_ijk, eijk));
+  CF_TRY(up(&p.pcg_row_begin, rb2));
+  CF_TRY(dalloc(&p.values, (size_t)nnzb * 36));
+  CF_TRY(dalloc(&p.seg_off, (size_t)nnzb));
+  CF_TRY(dalloc(&p.seg_cnt, (size_t)nnzb));
+  CF_TRY(cudaMemset(p.values, 0, sizeof(float) * (size_t)std::max(1, nnzb) * 36));
+  h->h_row_ptr = row_ptr;
+  h->h_col_idx = col_idx;
+  h->pattern_N = N;
+  h->pattern_valid = true;
+  return CF_OK;
+}
+
+cf_status ensure_pattern(cf_gn* h, const cf_deform_node* d_nodes, int N, cudaStream_t s) {
+  if (h->pattern_valid && h->pattern_N == N) return CF_OK;
+  std::vector<cf_deform_node> hn(N);
+  CF_TRY(cudaMemcpyAsync(hn.data(), d_nodes, sizeof(cf_deform_node) * (size_t)N, cudaMemcpyDeviceToHost, s));
+  CF_TRY(cudaStreamSynchronize(s));
+  return build_pattern_host(h, hn, N);
+}
+
+// Per-solve binning of correspondence incidences (counting sort by node,
+// then per-row grouping by block column).
+cf_status bin_correspondences(cf_gn* h, const cf_correspondence* corrs, const float* canon, int M, int N,
+                              cudaStream_t s) {
+  Work& w = h->w;
+  if (M > 0) {
+    int bin_ctas = std::min(w.bin_ctas_max, std::max(1, cdiv(M, kThreads)));
+    int chunk = cdiv(cdiv(M, bin_ctas), kThreads) * kThreads;
+    bin_ctas = cdiv(M, chunk);
+    { Timed t(h, s, kProfPack, 1); CF_TRY(launch_pack_count(w, corrs, canon, M, N, bin_ctas, chunk, s)); }
+    { Timed t(h, s, kProfBinScan, 2); CF_TRY(launch_bin_scan(w, N, bin_ctas, s)); }
+    { Timed t(h, s, kProfScatter, 1); CF_TRY(launch_bin_scatter(w, M, N, bin_ctas, chunk, s)); }
+  } else {
+    CF_TRY(cudaMemsetAsync(w.inc_start, 0, sizeof(int) * (size_t)(N + 1), s));
+  }
+  { Timed t(h, s, kProfExpand, 1); CF_TRY(launch_expand(w, h->p, N, s)); }
+  return CF_OK;
+}
+
+SolveArgs make_args(const cf_gn* h, const cf_deform_node* nodes, int N, int M) {
+  SolveArgs a;
+  memset(&a, 0, sizeof(a));
+  a.nodes = nodes;
+  a.N = N;
+  a.M = M;
+  a.lambda_smooth = h->params.lambda_smooth;
+  a.lambda_damping = h->params.lambda_damping;
+  a.pcg_iterations = std::max(0, h->params.pcg_iterations);
+  a.pcg_tolerance = h->params.pcg_tolerance;
+  a.arap_consistent = h->arap_consistent;
+  a.spin_limit = 1u << 22;
+  return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cf_status_string(cf_status s) {
+  switch (s) {
+    case CF_OK: return "ok";
+    case CF_ERR_INVALID_ARG: return "invalid argument";
+    case CF_ERR_OOM: return "device out of memory";
+    case CF_ERR_NON_FINITE: return "non-finite value in the solution or energy";
+    case CF_ERR_TIMEOUT: return "in-kernel barrier timed out";
+    case CF_ERR_CUDA: return "CUDA error";
+    case CF_ERR_CAPACITY: return "size exceeds the handle's capacity";
+    case CF_ERR_NOT_IMPLEMENTED: return "not implemented";
+    case CF_ERR_NO_DEVICE: return "no CUDA device";
+  }
+  return "unknown status";
+}
+
+cf_status cf_gn_params_default(cf_gn_params* p) {
+  if (!p) return CF_ERR_INVALID_ARG;
+  p->gn_iterations = 3;
+  p->pcg_iterations = 10;
+  p->pcg_tolerance = 1e-4f;
+  p->lambda_smooth = 1.0f;
+  p->lambda_rot = 1.0f;
+  p->lambda_damping = 1e-2f;
+  p->debug = 0;
+  return CF_OK;
+}
+
+cf_status cf_gn_create(const cf_gn_params* params, int max_nodes, int max_corrs, cf_gn** out) {
+  if (!out) return CF_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (!params || max_nodes <= 0 || max_corrs < 0 || max_corrs >= (1 << 27)) return CF_ERR_INVALID_ARG;
+  if (params->gn_iterations < 0 || params->gn_iterations > CF_MAX_GN_ITERS || params->pcg_iterations < 0)
+    return CF_ERR_INVALID_ARG;
+  int dev = 0, count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    snprintf(g_last_error, sizeof(g_last_error), "%s", cudaGetErrorString(e));
+    return CF_ERR_NO_DEVICE;
+  }
+  CF_TRY(cudaGetDevice(&dev));
+  cf_gn* h = new cf_gn();
+  h->params = *params;
+  h->max_nodes = max_nodes;
+  h->max_corrs = max_corrs;
+  h->device = dev;
+  cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, dev);
+  e = alloc_work(h->w, max_nodes, max_corrs, 2 * h->sms);
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&h->h_stats, sizeof(DevStats));
+  if (e != cudaSuccess) {
+    free_work(h->w);
+    delete h;
+    return from_cuda(e);
+  }
+  *out = h;
+  return CF_OK;
+}
+
+cf_status cf_gn_destroy(cf_gn* h) {
+  if (!h) return CF_ERR_INVALID_ARG;
+  cudaDeviceSynchronize();
+  free_pattern(h->p);
+  free_work(h->w);
+  if (h->h_stats) cudaFreeHost(h->h_stats);
+  for (auto& pe : h->prof_pool) {
+    cudaEventDestroy(pe.a);
+    cudaEventDestroy(pe.b);
+  }
+  delete h;
+  return CF_OK;
+}
+
+cf_status cf_gn_set_params(cf_gn* h, const cf_gn_params* params) {
+  if (!h || !params || params->gn_iterations < 0 || params->gn_iterations > CF_MAX_GN_ITERS ||
+      params->pcg_iterations < 0)
+    return CF_ERR_INVALID_ARG;
+  h->params = *params;
+  return CF_OK;
+}
+
+cf_status cf_gn_get_params(const cf_gn* h, cf_gn_params* params) {
+  if (!h || !params) return CF_ERR_INVALID_ARG;
+  *params = h->params;
+  return CF_OK;
+}
+
+cf_status cf_gn_set_option(cf_gn* h, int option, int value) {
+  if (!h) return CF_ERR_INVALID_ARG;
+  switch (option) {
+    case CF_OPT_ARAP_CONSISTENT:
+      h->arap_consistent = value ? 1 : 0;
+      return CF_OK;
+    case CF_OPT_PCG_CTAS:
+      if (value < 0 || value > kMaxPcgCtas) return CF_ERR_INVALID_ARG;
+      h->pcg_ctas_override = value;
+      h->pattern_valid = false;
+      return CF_OK;
+  }
+  return CF_ERR_INVALID_ARG;
+}
+
+cf_status cf_gn_invalidate_pattern(cf_gn* h) {
+  if (!h) return CF_ERR_INVALID_ARG;
+  h->pattern_valid = false;
+  return CF_OK;
+}
+
+cf_status cf_gn_linearize_solve(cf_gn* h, const cf_correspondence* d_corrs, int num_corrs,
+                                const cf_deform_node* d_nodes, const cf_dual_quat* d_transforms, int num_nodes,
+                                float* d_delta_x, void* stream) {
+  if (!h || num_corrs < 0 || num_nodes < 0) return CF_ERR_INVALID_ARG;
+  if (num_nodes > h->max_nodes || num_corrs > h->max_corrs) return CF_ERR_CAPACITY;
+  if (num_nodes == 0) return CF_OK;
+  if (!d_nodes || !d_transforms || !d_delta_x || (num_corrs > 0 && !d_corrs)) return CF_ERR_INVALID_ARG;
+  if ((reinterpret_cast<uintptr_t>(d_corrs) & 3u) || (reinterpret_cast<uintptr_t>(d_transforms) & 15u))
+    return CF_ERR_INVALID_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  cf_status st = ensure_pattern(h, d_nodes, num_nodes, s);
+  if (st != CF_OK) return st;
+  Work& w = h->w;
+  CF_TRY(cudaMemsetAsync(w.stats, 0, sizeof(DevStats), s));
+  CF_TRY(cudaMemsetAsync(w.err, 0, sizeof(int), s));
+  st = bin_correspondences(h, d_corrs, nullptr, num_corrs, num_nodes, s);
+  if (st != CF_OK) return st;
+  SolveArgs a = make_args(h, d_nodes, num_nodes, num_corrs);
+  a.delta_x = d_delta_x;
+  { Timed t(h, s, kProfResidual, 1); CF_TRY(launch_residual(w, num_corrs, num_nodes, false, s)); }
+  { Timed t(h, s, kProfAssemble, 1); CF_TRY(launch_assemble(w, h->p, a, d_transforms, s)); }
+  { Timed t(h, s, kProfPcg, 1); CF_TRY(launch_pcg(w, h->p, a, 0, s)); }
+  h->last_gn = 1;
+  return CF_OK;
+}
+
+cf_status cf_gn_solve(cf_gn* h, const cf_problem* prob, cf_dual_quat* d_transforms, cf_solve_stats* stats,
+                      void* stream) {
+  if (!h || !prob || prob->num_nodes < 0 || prob->num_corrs < 0) return CF_ERR_INVALID_ARG;
+  const int N = prob->num_nodes, M = prob->num_corrs;
+  if (N > h->max_nodes || M > h->max_corrs) return CF_ERR_CAPACITY;
+  if (stats) memset(stats, 0, sizeof(*stats));
+  if (N == 0) return CF_OK;
+  if (!prob->nodes || !d_transforms || (M > 0 && (!prob->corrs || !prob->canon_points))) return CF_ERR_INVALID_ARG;
+  if ((reinterpret_cast<uintptr_t>(prob->corrs) & 3u) || (reinterpret_cast<uintptr_t>(d_transforms) & 15u))
+    return CF_ERR_INVALID_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  cf_status st = ensure_pattern(h, prob->nodes, N, s);
+  if (st != CF_OK) return st;
+  Work& w = h->w;
+  CF_TRY(cudaMemsetAsync(w.stats, 0, sizeof(DevStats), s));
+  CF_TRY(cudaMemsetAsync(w.err, 0, sizeof(int), s));
+  st = bin_correspondences(h, prob->corrs, prob->canon_points, M, N, s);
+  if (st != CF_OK) return st;
+  SolveArgs a = make_args(h, prob->nodes, N, M);
+  a.transforms = d_transforms;
+  a.max_rot = prob->max_rot;
+  a.max_trans = prob->max_trans;
+  a.update_scale = prob->update_scale;
+  { Timed t(h, s, kProfNodePlain, 1); CF_TRY(launch_node_plain(w, prob->nodes, d_transforms, N, s)); }
+  const int G = h->params.gn_iterations;
+  for (int g = 0; g < G; g++) {
+    { Timed t(h, s, kProfResidual, 1); CF_TRY(launch_residual(w, M, N, true, s)); }
+    { Timed t(h, s, kProfAssemble, 1); CF_TRY(launch_assemble(w, h->p, a, d_transforms, s)); }
+    { Timed t(h, s, kProfPcg, 1); CF_TRY(launch_pcg(w, h->p, a, g, s)); }
+  }
+  { Timed t(h, s, kProfEnergy, 2); CF_TRY(launch_final_energy(w, h->p, a, G, s)); }
+  h->last_gn = G;
+  if (!stats) return CF_OK;
+  CF_TRY(cudaMemcpyAsync(h->h_stats, w.stats, sizeof(DevStats), cudaMemcpyDeviceToHost, s));
+  int herr = 0;
+  CF_TRY(cudaMemcpyAsync(&herr, w.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CF_TRY(cudaStreamSynchronize(s));
+  const DevStats& d = *h->h_stats;
+  stats->energy_initial = d.energy[0];
+  stats->energy_final = d.energy[G];
+  for (int g = 0; g <= G && g < CF_MAX_GN_ITERS; g++) stats->energy_per_iter[g] = d.energy[g];
+  for (int g = 0; g < G; g++) {
+    stats->pcg_iterations[g] = d.pcg_iters[g];
+    stats->pcg_residual[g] = d.pcg_res[g];
+  }
+  stats->gn_iterations_run = G;
+  stats->num_blocks = h->p.nnzb;
+  stats->precond_fallbacks = d.fallbacks;
+  stats->error_flags = herr;
+  if (herr & kErrTimeoutBit) return CF_ERR_TIMEOUT;
+  if (herr & kErrNonFiniteBit) return CF_ERR_NON_FINITE;
+  return CF_OK;
+}
+
+cf_status cf_gn_profile_enable(cf_gn* h, int on) {
+  if (!h) return CF_ERR_INVALID_ARG;
+  if (h->prof_used) prof_collect(h);
+  h->profile = on != 0;
+  for (int i = 0; i < CF_PROF_SLOTS; i++) {
+    h->prof_ms[i] = 0.0;
+    h->prof_n[i] = 0;
+  }
+  return CF_OK;
+}
+
+cf_status cf_gn_profile_read(cf_gn* h, double* ms, int* launches, int n_slots) {
+  if (!h || n_slots < 0) return CF_ERR_INVALID_ARG;
+  prof_collect(h);
+  for (int i = 0; i < n_slots && i < CF_PROF_SLOTS; i++) {
+    if (ms) ms[i] = h->prof_ms[i];
+    if (launches) launches[i] = h->prof_n[i];
+  }
+  return CF_OK;
+}
+
+const char* cf_gn_profile_name(int slot) {
+  return (slot >= 0 && slot < CF_PROF_SLOTS) ? kProfNames[slot] : "";
+}
+
+cf_status cf_gn_launch_count(const cf_gn* h, long long* launches) {
+  if (!h || !launches) return CF_ERR_INVALID_ARG;
+  *launches = h->launches;
+  return CF_OK;
+}
+
+cf_status cf_gn_check(cf_gn* h, void* stream) {
+  if (!h) return CF_ERR_INVALID_ARG;
+  int herr = 0;
+  CF_TRY(cudaMemcpyAsync(&herr, h->w.err, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+  CF_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  if (herr & kErrTimeoutBit) return CF_ERR_TIMEOUT;
+  if (herr & kErrNonFiniteBit) return CF_ERR_NON_FINITE;
+  return CF_OK;
+}
+
+cf_status cf_gn_get_system(cf_gn* h, int* num_rows, int* num_blocks, int* h_row_ptr, int* h_col_idx,
+                           float* h_values, float* h_rhs, void* stream) {
+  if (!h) return CF_ERR_INVALID_ARG;
+  const int N = h->pattern_valid ? h->pattern_N : 0;
+  const int nnzb = h->pattern_valid ? h->p.nnzb : 0;
+  if (num_rows) *num_rows = N;
+  if (num_blocks) *num_blocks = nnzb;
+  if (N == 0) return CF_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (h_row_ptr) memcpy(h_row_ptr, h->h_row_ptr.data(), sizeof(int) * (N + 1));
+  if (h_col_idx) memcpy(h_col_idx, h->h_col_idx.data(), sizeof(int) * nnzb);
+  if (h_values)
+    CF_TRY(cudaMemcpyAsync(h_values, h->p.values, sizeof(float) * 36 * (size_t)nnzb, cudaMemcpyDeviceToHost, s));
+  if (h_rhs) CF_TRY(cudaMemcpyAsync(h_rhs, h->w.rhs, sizeof(float) * 6 * (size_t)N, cudaMemcpyDeviceToHost, s));
+  CF_TRY(cudaStreamSynchronize(s));
+  return CF_OK;
+}
+
+cf_status cf_warp_apply_twist(cf_dual_quat* d_transforms, const float* d_delta_x, int num_nodes, float max_rot,
+                              float max_trans, float update_scale, void* stream) {
+  if (num_nodes < 0) return CF_ERR_INVALID_ARG;
+  if (num_nodes == 0) return CF_OK;
+  if (!d_transforms || !d_delta_x || (reinterpret_cast<uintptr_t>(d_transforms) & 15u)) return CF_ERR_INVALID_ARG;
+  CF_TRY(launch_apply_twist(d_transforms, d_delta_x, num_nodes, max_rot, max_trans, update_scale,
+                            (cudaStream_t)stream));
+  return CF_OK;
+}
+
+cf_status cf_warp_skin_points(const float* d_points, const int* d_node_ids, const float* d_node_ws, int num_points,
+                              const cf_deform_node* d_nodes, const cf_dual_quat* d_transforms, int num_nodes,
+                              float* d_out, void* stream) {
+  if (num_points < 0 || num_nodes < 0) return CF_ERR_INVALID_ARG;
+  if (num_points == 0) return CF_OK;
+  if (!d_points || !d_node_ids || !d_node_ws || !d_out || (num_nodes > 0 && (!d_nodes || !d_transforms)))
+    return CF_ERR_INVALID_ARG;
+  CF_TRY(launch_skin_points(d_points, d_node_ids, d_node_ws, num_points, d_nodes, d_transforms, num_nodes, d_out,
+                            (cudaStream_t)stream));
+  return CF_OK;
+}
+
+cf_status cf_get_version(int* major, int* minor, int* patch) {
+  if (major) *major = 0;
+  if (minor) *minor = 1;
+  if (patch) *patch = 0;
+  return CF_OK;
+}
+
+cf_status cf_last_cuda_error(char* buf, size_t len) {
+  if (!buf || len == 0) return CF_ERR_INVALID_ARG;
+  snprintf(buf, len, "%s", g_last_error);
+  return CF_OK;
+}
+
+}  // extern "C"

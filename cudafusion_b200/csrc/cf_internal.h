@@ -1,0 +1,128 @@
+// cf_internal.h — structures shared by the host API (cf_api.cu) and the
+// kernel launchers (cf_kernels.cu).  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/cudafusion_b200.h"
+
+namespace cf {
+
+constexpr int kThreads = 256;
+constexpr int kErrTimeoutBit = 1;   // bounded barrier gave up
+constexpr int kErrNonFiniteBit = 2; // NaN/Inf in the solution or energy
+constexpr int kStatsSlots = CF_MAX_GN_ITERS + 1;
+
+// Device-side statistics of one solve (copied to cf_solve_stats on request).
+struct DevStats {
+  double energy[kStatsSlots];          // energy at each linearisation point; [G] = final
+  double pcg_res[CF_MAX_GN_ITERS];     // final ||r|| per GN iteration
+  int pcg_iters[CF_MAX_GN_ITERS];
+  int fallbacks;                        // Cholesky fallbacks of the last GN iteration
+  int pad_;
+};
+
+// Block pattern and everything derived from the graph topology.  Built on
+// the host (cold path, kernels/solver_kernels.cu:498-541) and uploaded.
+struct Pattern {
+  int N = 0;
+  int nnzb = 0;
+  int n_upper = 0;      // blocks with col >= row (incl. diagonal)
+  int n_edges = 0;      // ARAP edges visited by the reference (lower endpoint owns)
+  int max_upper_row = 0;  // max upper blocks in one row
+  int* row_ptr = nullptr;   // [N+1]
+  int* col_idx = nullptr;   // [nnzb]
+  int* diag_pos = nullptr;  // [N]
+  int* trans_pos = nullptr; // [nnzb] position of the transposed block
+  int* upper_pos = nullptr; // [n_upper]
+  int* upper_row = nullptr; // [n_upper]
+  int* arap_row_ptr = nullptr;  // [N+1]
+  int* arap_row_inc = nullptr;  // (edge << 1) | role, role 0 = lower endpoint
+  int* arap_blk_ptr = nullptr;  // [n_upper+1] over upper off-diagonal blocks
+  int* arap_blk_edge = nullptr;
+  int* edge_ijk = nullptr;      // [3*n_edges] i, j, k (slot in i's list)
+  // per-pattern work arrays
+  float* values = nullptr;  // [nnzb*36]
+  int* seg_off = nullptr;   // [nnzb]
+  int* seg_cnt = nullptr;   // [nnzb]
+  // PCG partition
+  int pcg_ctas = 0;
+  int* pcg_row_begin = nullptr;  // [pcg_ctas+1]
+  int pcg_smem = 0;
+  int pcg_a_in_smem = 0;
+};
+
+// Per-handle work buffers sized by (max_nodes, max_corrs).
+struct Work {
+  int max_nodes = 0, max_corrs = 0;
+  int bin_ctas_max = 0;
+  float4* pk_src = nullptr;  // xyz: canonical point (solve) or src (linearise); w: effective weight
+  float4* pk_dst = nullptr;
+  float4* pk_nrm = nullptr;
+  int4* pk_ids = nullptr;
+  float4* pk_ws = nullptr;
+  float4* c_srcfw = nullptr;  // skinned src, fw (0 = skipped)
+  float4* c_nres = nullptr;   // normal, residual
+  int* cnt = nullptr;         // [bin_ctas_max * max_nodes]
+  int* node_total = nullptr;  // [max_nodes]
+  int* inc_start = nullptr;   // [max_nodes+1]
+  int* inc = nullptr;         // [4*max_corrs]: (c << 2) | a
+  int* trip = nullptr;        // [16*max_corrs]: (c << 4) | (a << 2) | b
+  float* rhs = nullptr;       // [6*max_nodes]
+  cf_dual_quat* plain = nullptr;  // [max_nodes]
+  float* x = nullptr;         // [6*max_nodes]
+  float* z = nullptr;
+  float* p0 = nullptr;
+  float* p1 = nullptr;
+  double* partials = nullptr;  // [2 bufs][2 slots][max pcg ctas]
+  unsigned* barrier = nullptr;
+  int* err = nullptr;
+  double* e_data_part = nullptr;  // [kEnergyCtas]
+  double* e_arap_part = nullptr;  // [max_nodes] (per row / per energy CTA)
+  DevStats* stats = nullptr;
+};
+
+constexpr int kEnergyCtas = 592;  // fixed grid of the residual/energy kernels
+constexpr int kMaxPcgCtas = 1024;
+
+struct SolveArgs {
+  const cf_deform_node* nodes;
+  int N;
+  int M;
+  float lambda_smooth;
+  float lambda_damping;
+  int pcg_iterations;
+  float pcg_tolerance;
+  int arap_consistent;
+  // node update (solve) or plain delta_x output (linearise)
+  cf_dual_quat* transforms;  // in/out
+  float* delta_x;            // non-null: write dx here and do not update
+  float max_rot, max_trans, update_scale;
+  unsigned spin_limit;
+};
+
+// ---- launchers (cf_kernels.cu) ----
+cudaError_t launch_pack_count(const Work& w, const cf_correspondence* corrs, const float* canon, int M, int N,
+                              int bin_ctas, int chunk, cudaStream_t s);
+cudaError_t launch_bin_scan(const Work& w, int N, int bin_ctas, cudaStream_t s);
+cudaError_t launch_bin_scatter(const Work& w, int M, int N, int bin_ctas, int chunk, cudaStream_t s);
+cudaError_t launch_expand(const Work& w, const Pattern& p, int N, cudaStream_t s);
+cudaError_t launch_node_plain(const Work& w, const cf_deform_node* nodes, const cf_dual_quat* T, int N,
+                              cudaStream_t s);
+cudaError_t launch_residual(const Work& w, int M, int N, bool skin, cudaStream_t s);
+cudaError_t launch_assemble(const Work& w, const Pattern& p, const SolveArgs& a, const cf_dual_quat* T,
+                            cudaStream_t s);
+cudaError_t launch_pcg(const Work& w, const Pattern& p, const SolveArgs& a, int gn_slot, cudaStream_t s);
+cudaError_t launch_final_energy(const Work& w, const Pattern& p, const SolveArgs& a, int slot, cudaStream_t s);
+cudaError_t launch_apply_twist(cf_dual_quat* T, const float* dx, int N, float max_rot, float max_trans,
+                               float scale, cudaStream_t s);
+cudaError_t launch_skin_points(const float* pts, const int* ids, const float* ws, int M,
+                               const cf_deform_node* nodes, const cf_dual_quat* T, int N, float* out,
+                               cudaStream_t s);
+int pcg_smem_bytes(int max_blocks, int max_rows, bool a_in_smem);
+int pcg_max_active_ctas(int smem, bool a_in_smem);
+cudaError_t pcg_prepare(int smem, bool a_in_smem);
+int expand_smem_bytes(int max_upper_row);
+
+}  // namespace cf

@@ -1,0 +1,502 @@
+"""Seeded synthetic warp-field problems.
+
+CUDAFusion tracks real RGB-D sequences (VolumeDeform recordings referenced by
+config/params.yaml:2-3); none ship with it, so these generators build problems
+of the same shapes and statistics.  Nothing here is on the solve path: it
+creates inputs for the tests and the benchmark.
+
+Conventions follow the reference:
+  * node transforms are DualQuats centred at their node, T(p) = R(p-c)+c+t
+    (include/se3_math.cuh:379-415);
+  * a point is skinned by its 4 nearest nodes with weights
+    exp(-d^2 / (2 r^2)) normalised (src/warp_field.cu:379-404);
+  * graph edges go to the K_GRAPH=8 nearest nodes with weights
+    exp(-d^2 / (2 r^2)) (src/warp_field.cu:889, Euclidean instead of geodesic);
+  * depth normals use forward differences flipped toward the camera
+    (kernels/tsdf_kernels.cu:180-230).
+"""
+from dataclasses import dataclass, field
+
+import numpy as np
+from scipy.spatial import cKDTree
+
+from .types import CORR_DTYPE, DQ_DTYPE, K_GRAPH, K_NEIGHBORS, NODE_DTYPE, identity_transforms
+
+
+@dataclass
+class Problem:
+    """One warp-field solve: graph, correspondences with canonical points,
+    initial transforms, and (when known) the ground-truth transforms."""
+
+    nodes: np.ndarray  # NODE_DTYPE[N]
+    canon: np.ndarray  # float32[M, 3]
+    corrs: np.ndarray  # CORR_DTYPE[M] (src = canonical point)
+    init_transforms: np.ndarray  # DQ_DTYPE[N]
+    gt_transforms: np.ndarray = None  # DQ_DTYPE[N]
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def num_nodes(self):
+        return int(self.nodes.shape[0])
+
+    @property
+    def num_corrs(self):
+        return int(self.corrs.shape[0])
+
+    def save(self, path):
+        np.savez_compressed(
+            path,
+            nodes=self.nodes.view(np.uint8),
+            canon=self.canon,
+            corrs=self.corrs.view(np.uint8),
+            init_transforms=self.init_transforms.view(np.uint8),
+            gt_transforms=(self.gt_transforms if self.gt_transforms is not None else identity_transforms(0)).view(
+                np.uint8
+            ),
+        )
+
+    @staticmethod
+    def load(path):
+        z = np.load(path)
+        gt = z["gt_transforms"].view(DQ_DTYPE)
+        return Problem(
+            nodes=z["nodes"].view(NODE_DTYPE).copy(),
+            canon=z["canon"].copy(),
+            corrs=z["corrs"].view(CORR_DTYPE).copy(),
+            init_transforms=z["init_transforms"].view(DQ_DTYPE).copy(),
+            gt_transforms=gt.copy() if gt.shape[0] else None,
+        )
+
+
+# --------------------------------------------------------------------------
+# small FP64 quaternion helpers (x, y, z, w storage)
+# --------------------------------------------------------------------------
+
+
+def _qmul(a, b):
+    ax, ay, az, aw = np.moveaxis(a, -1, 0)
+    bx, by, bz, bw = np.moveaxis(b, -1, 0)
+    return np.stack(
+        [
+            aw * bx + ax * bw + ay * bz - az * by,
+            aw * by - ax * bz + ay * bw + az * bx,
+            aw * bz + ax * by - ay * bx + az * bw,
+            aw * bw - ax * bx - ay * by - az * bz,
+        ],
+        -1,
+    )
+
+
+def _qconj(q):
+    return q * np.array([-1.0, -1.0, -1.0, 1.0])
+
+
+def quat_from_rotvec(w):
+    w = np.asarray(w, np.float64)
+    th = np.linalg.norm(w, axis=-1, keepdims=True)
+    s = np.where(th > 1e-12, np.sin(0.5 * th) / np.maximum(th, 1e-300), 0.5)
+    return np.concatenate([w * s, np.cos(0.5 * th)], -1)
+
+
+def _qrotate(q, v):
+    vq = np.concatenate([v, np.zeros(v.shape[:-1] + (1,))], -1)
+    return _qmul(_qmul(q, vq), _qconj(q))[..., :3]
+
+
+def centred_dq(q, t):
+    """Centred DualQuat from rotation quaternion q and centred translation t."""
+    out = np.zeros(q.shape[0], DQ_DTYPE)
+    tq = np.concatenate([t, np.zeros((t.shape[0], 1))], -1)
+    out["real"] = q
+    out["dual"] = 0.5 * _qmul(tq, q)
+    return out
+
+
+def skin_points_f64(points, ids, ws, node_pos, transforms):
+    """FP64 DQ-blend skinning (the math of se3_math.cuh:450-510) for data
+    generation.  Returns warped points and the blended rotation quaternions."""
+    real = transforms["real"].astype(np.float64)
+    dual = transforms["dual"].astype(np.float64)
+    t = 2.0 * _qmul(dual, _qconj(real))[:, :3]
+    rc = _qrotate(real, node_pos.astype(np.float64))
+    t_plain = t + node_pos - rc  # dq_centered: plain translation
+    dual_plain = 0.5 * _qmul(np.concatenate([t_plain, np.zeros((len(t_plain), 1))], -1), real)
+    br = np.zeros((points.shape[0], 4))
+    bd = np.zeros((points.shape[0], 4))
+    wsum = np.zeros(points.shape[0])
+    for k in range(K_NEIGHBORS):
+        nid = ids[:, k]
+        w = ws[:, k].astype(np.float64)
+        ok = (nid >= 0) & (w >= 1e-8)
+        nidc = np.where(ok, nid, 0)
+        qr = real[nidc]
+        qd = dual_plain[nidc]
+        flip = np.sum(qr * br, -1) < 0
+        sgn = np.where(flip, -1.0, 1.0)[:, None]
+        wk = np.where(ok, w, 0.0)[:, None]
+        br += wk * sgn * qr
+        bd += wk * sgn * qd
+        wsum += wk[:, 0]
+    n = np.linalg.norm(br, axis=-1, keepdims=True)
+    br = br / np.maximum(n, 1e-300)
+    bd = bd / np.maximum(n, 1e-300)
+    tb = 2.0 * _qmul(bd, _qconj(br))[:, :3]
+    out = _qrotate(br, points.astype(np.float64)) + tb
+    keep = wsum < 1e-8
+    out[keep] = points[keep]
+    br[keep] = np.array([0.0, 0.0, 0.0, 1.0])
+    return out, br
+
+
+def _graph(node_pos, node_radius):
+    n = node_pos.shape[0]
+    tree = cKDTree(node_pos)
+    kq = min(K_GRAPH + 1, n)
+    d, idx = tree.query(node_pos, k=kq)
+    d = d.reshape(n, kq)[:, 1:]
+    idx = idx.reshape(n, kq)[:, 1:]
+    nb = np.full((n, K_GRAPH), -1, np.int32)
+    nw = np.zeros((n, K_GRAPH), np.float32)
+    nb[:, : kq - 1] = idx
+    r = np.maximum(node_radius, 1e-6)
+    nw[:, : kq - 1] = np.exp(-(d**2) / (2.0 * r * r))
+    return nb, nw, kq - 1
+
+
+def _skin_weights(points, node_pos, node_radius, tree=None):
+    tree = tree if tree is not None else cKDTree(node_pos)
+    d, idx = tree.query(points, k=K_NEIGHBORS, workers=-1)
+    d2 = (d.astype(np.float64)) ** 2
+    r = np.maximum(node_radius, 1e-6)
+    w = np.exp(-d2 / (2.0 * r * r))
+    s = w.sum(-1, keepdims=True)
+    w = np.where(s > 1e-8, w / np.maximum(s, 1e-300), 0.0)
+    return idx.astype(np.int32), w.astype(np.float32)
+
+
+def _make_nodes(pos, normals, radius, nb, nw, kcount):
+    nodes = np.zeros(pos.shape[0], NODE_DTYPE)
+    nodes["pos"] = pos
+    nodes["normal"] = normals
+    nodes["radius"] = radius
+    nodes["neighbors"] = nb
+    nodes["neighbor_w"] = nw
+    nodes["num_neighbors"] = kcount
+    return nodes
+
+
+def _smooth_field(rng, x, amplitude, scale, terms=3):
+    """Low-frequency random vector field with max norm `amplitude` over x."""
+    f = np.zeros((x.shape[0], 3))
+    for _ in range(terms):
+        k = rng.normal(size=3) / scale
+        a = rng.normal(size=3)
+        ph = rng.uniform(0, 2 * np.pi)
+        f += np.sin(x @ k + ph)[:, None] * a[None, :]
+    m = np.linalg.norm(f, axis=-1).max()
+    return f * (amplitude / max(m, 1e-12))
+
+
+def _fibonacci_sphere(n, rng):
+    i = np.arange(n) + 0.5
+    phi = np.arccos(1 - 2 * i / n)
+    th = np.pi * (1 + 5**0.5) * i
+    p = np.stack([np.cos(th) * np.sin(phi), np.sin(th) * np.sin(phi), np.cos(phi)], -1)
+    # random global rotation + small jitter: a blue-noise (Poisson-disk-like) set
+    q = quat_from_rotvec(rng.normal(size=3))
+    p = _qrotate(np.broadcast_to(q, (n, 4)), p)
+    p += rng.normal(scale=0.15 * np.sqrt(4 * np.pi / n), size=p.shape)
+    return p / np.linalg.norm(p, axis=-1, keepdims=True)
+
+
+def sphere_problem(
+    num_nodes=256,
+    num_corrs=20000,
+    radius=0.3,
+    node_radius=0.025,
+    max_rot_deg=15.0,
+    max_trans=0.02,
+    noise=0.001,
+    outlier_frac=0.05,
+    outlier_radius=0.05,
+    seed=1,
+    center=(0.0, 0.0, 1.0),
+):
+    """Sphere of `radius` with Poisson-disk-like nodes, uniform surface
+    correspondences, a low-frequency ground-truth warp (<= max_rot_deg,
+    <= max_trans), point-to-plane targets with sigma=`noise` along the normal
+    and `outlier_frac` uniform outliers within `outlier_radius`.  The initial
+    transforms are identity."""
+    rng = np.random.default_rng(seed)
+    c = np.asarray(center, np.float64)
+    nrm_nodes = _fibonacci_sphere(num_nodes, rng)
+    node_pos = c + radius * nrm_nodes
+    nb, nw, kc = _graph(node_pos, node_radius)
+    nodes = _make_nodes(node_pos, nrm_nodes, node_radius, nb, nw, kc)
+
+    v = rng.normal(size=(num_corrs, 3))
+    nrm = v / np.linalg.norm(v, axis=-1, keepdims=True)
+    canon = c + radius * nrm
+    tree = cKDTree(node_pos)
+    ids, ws = _skin_weights(canon, node_pos, node_radius, tree)
+
+    rotv = _smooth_field(rng, node_pos - c, np.deg2rad(max_rot_deg), radius)
+    trans = _smooth_field(rng, node_pos - c, max_trans, radius)
+    gt = centred_dq(quat_from_rotvec(rotv), trans)
+
+    live, q = skin_points_f64(canon, ids, ws, node_pos, gt)
+    n_live = _qrotate(q, nrm)
+    dst = live + rng.normal(scale=noise, size=(num_corrs, 1)) * n_live
+    n_out = int(round(outlier_frac * num_corrs))
+    out_idx = rng.choice(num_corrs, size=n_out, replace=False)
+    u = rng.normal(size=(n_out, 3))
+    u /= np.linalg.norm(u, axis=-1, keepdims=True)
+    dst[out_idx] += u * (outlier_radius * rng.uniform(0, 1, size=(n_out, 1)) ** (1 / 3))
+
+    corrs = np.zeros(num_corrs, CORR_DTYPE)
+    corrs["src"] = canon
+    corrs["dst"] = dst
+    corrs["normal"] = n_live
+    corrs["node_ids"] = ids
+    corrs["node_ws"] = ws
+    corrs["weight"] = 1.0
+    corrs["valid"] = 1
+    return Problem(
+        nodes=nodes,
+        canon=canon.astype(np.float32),
+        corrs=corrs,
+        init_transforms=identity_transforms(num_nodes),
+        gt_transforms=gt,
+        meta=dict(kind="sphere", seed=seed, num_nodes=num_nodes, num_corrs=num_corrs, outliers=n_out),
+    )
+
+
+# --------------------------------------------------------------------------
+# articulated two-cylinder surface seen by a pinhole camera
+# --------------------------------------------------------------------------
+
+
+def _rot_y(angle):
+    return quat_from_rotvec(np.array([0.0, angle, 0.0]))
+
+
+def _blue_noise_subsample(points, n, rng):
+    """Indices of exactly n points of a dense cloud, one per occupied cell of
+    a grid whose cell size is tuned to give about n cells (Poisson-disk-like),
+    and that cell size."""
+    lo = points.min(0)
+    ext = float((points.max(0) - lo).max())
+    perm = rng.permutation(points.shape[0])
+    pts = points[perm]
+    a, b = ext / (4 * n) ** 0.5 * 1e-2, ext
+    for _ in range(40):
+        h = 0.5 * (a + b)
+        keys = np.floor((pts - lo) / h).astype(np.int64)
+        k = (keys[:, 0] * 73856093) ^ (keys[:, 1] * 19349663) ^ (keys[:, 2] * 83492791)
+        cnt = np.unique(k).shape[0]
+        if cnt >= n:
+            a = h
+        else:
+            b = h
+    h = a
+    keys = np.floor((pts - lo) / h).astype(np.int64)
+    k = (keys[:, 0] * 73856093) ^ (keys[:, 1] * 19349663) ^ (keys[:, 2] * 83492791)
+    _, first = np.unique(k, return_index=True)
+    if first.shape[0] > n:
+        first = rng.choice(first, size=n, replace=False)
+    return np.sort(perm[first]), h
+
+
+def _ray_tube(dirs, axis_pt, axis_dir, radius, smin, smax):
+    """Nearest intersection of rays from the origin with a capless tube."""
+    o = -axis_pt
+    w = axis_dir
+    dw = dirs @ w
+    ow = o @ w
+    dperp = dirs - dw[:, None] * w
+    operp = o - ow * w
+    a = np.sum(dperp * dperp, -1)
+    b = 2.0 * (dperp @ operp)
+    c = operp @ operp - radius * radius
+    disc = b * b - 4 * a * c
+    ok = disc > 0
+    sq = np.sqrt(np.where(ok, disc, 0.0))
+    t = (-b - sq) / np.maximum(2 * a, 1e-300)
+    s = ow + t * dw
+    ok &= (t > 0) & (s >= smin) & (s <= smax)
+    return np.where(ok, t, np.inf), s
+
+
+def cylinder_problem(
+    width=640,
+    height=480,
+    fx=570.342,
+    fy=570.342,
+    cx=320.0,
+    cy=240.0,
+    num_nodes=2048,
+    radii=(0.06, 0.05),
+    lengths=(0.08, 0.09),
+    distance=0.14,
+    bend_deg=30.0,
+    init_bend_deg=24.0,
+    twist_deg=0.0,
+    init_twist_deg=0.0,
+    noise=0.001,
+    seed=2,
+    nodes_cache=None,
+):
+    """Articulated two-cylinder surface (radii 6 and 5 cm) bent by `bend_deg`
+    at the joint, rendered as a width x height depth image.  Canonical pose is
+    straight; the live depth is at (bend_deg, twist_deg); the initial
+    transforms are the exact warp at (init_bend_deg, init_twist_deg), i.e. a
+    warm start from the previous frame.  Correspondences are the valid depth
+    pixels with forward-difference depth normals; targets carry sigma=`noise`
+    depth noise."""
+    rng = np.random.default_rng(seed)
+    joint = np.array([0.0, 0.0, distance])
+
+    def seg2_quat(bend, twist):
+        qb = _rot_y(np.deg2rad(bend))
+        qt = quat_from_rotvec(np.array([np.deg2rad(twist), 0.0, 0.0]))
+        return _qmul(qb, qt)
+
+    q_live = seg2_quat(bend_deg, twist_deg)
+    w2 = _qrotate(q_live, np.array([1.0, 0.0, 0.0]))
+
+    u, v = np.meshgrid(np.arange(width, dtype=np.float64), np.arange(height, dtype=np.float64))
+    dirs = np.stack([(u - cx) / fx, (v - cy) / fy, np.ones_like(u)], -1).reshape(-1, 3)
+    t1, _ = _ray_tube(dirs, joint, np.array([1.0, 0.0, 0.0]), radii[0], -lengths[0], 0.0)
+    t2, _ = _ray_tube(dirs, joint, w2, radii[1], 0.0, lengths[1])
+    seg = np.where(t2 < t1, 1, 0)
+    t = np.minimum(t1, t2)
+    hit = np.isfinite(t)
+    depth = np.where(hit, t, 0.0).reshape(height, width)  # z of dir is 1 -> t is depth
+    segimg = np.where(hit, seg, -1).reshape(height, width)
+
+    # forward-difference normals from the clean depth (tsdf_kernels.cu:180-230)
+    P = dirs.reshape(height, width, 3) * depth[..., None]
+    dx = P[:-1, 1:] - P[:-1, :-1]
+    dy = P[1:, :-1] - P[:-1, :-1]
+    n = np.cross(dx, dy)
+    nn = np.linalg.norm(n, axis=-1, keepdims=True)
+    n = -n / np.maximum(nn, 1e-12)
+    d00, d01, d10 = depth[:-1, :-1], depth[:-1, 1:], depth[1:, :-1]
+    s00, s01, s10 = segimg[:-1, :-1], segimg[:-1, 1:], segimg[1:, :-1]
+    good = (d00 > 0) & (d01 > 0) & (d10 > 0) & (s00 == s01) & (s00 == s10) & (nn[..., 0] > 1e-12)
+    good &= (np.abs(d01 - d00) < 0.01) & (np.abs(d10 - d00) < 0.01)
+    vv, uu = np.nonzero(good)
+    pix = vv * width + uu
+    live = P[vv, uu]
+    nrm = n[vv, uu]
+    sg = s00[vv, uu]
+
+    # canonical point: undo the live articulation of segment 2
+    canon = live.copy()
+    m2 = sg == 1
+    qi = np.broadcast_to(_qconj(q_live), (int(m2.sum()), 4))
+    if np.any(m2):
+        canon[m2] = joint + _qrotate(qi, live[m2] - joint)
+    if nodes_cache is None:
+        # the canonical model holds the surface seen so far: sample the nodes
+        # from the visible canonical surface (blue-noise subsampling)
+        cnrm = nrm.copy()
+        if np.any(m2):
+            cnrm[m2] = _qrotate(qi, nrm[m2])
+        sel, h = _blue_noise_subsample(canon, num_nodes, rng)
+        node_pos = canon[sel]
+        node_radius = h
+        nb, nw, kc = _graph(node_pos, node_radius)
+        nodes = _make_nodes(node_pos, cnrm[sel], node_radius, nb, nw, kc)
+        tree = cKDTree(node_pos)
+    else:
+        nodes, tree = nodes_cache
+        node_pos = nodes["pos"].astype(np.float64)
+        node_radius = float(nodes["radius"][0])
+    # noisy target: depth noise along the viewing ray
+    z = depth[vv, uu] + rng.normal(scale=noise, size=vv.shape[0])
+    dst = dirs[pix] * z[:, None]
+
+    ids, ws = _skin_weights(canon, node_pos, node_radius, tree)
+    M = canon.shape[0]
+    corrs = np.zeros(M, CORR_DTYPE)
+    corrs["src"] = canon
+    corrs["dst"] = dst
+    corrs["normal"] = nrm
+    corrs["node_ids"] = ids
+    corrs["node_ws"] = ws
+    corrs["weight"] = 1.0
+    corrs["valid"] = 1
+
+    def warp_at(bend, twist):
+        q2 = seg2_quat(bend, twist)
+        on2 = node_pos[:, 0] > joint[0]
+        q = np.where(on2[:, None], np.broadcast_to(q2, (len(node_pos), 4)), np.array([0.0, 0.0, 0.0, 1.0]))
+        # centred translation: t = R (x - J) + J - x
+        t = _qrotate(q, node_pos - joint) + joint - node_pos
+        return centred_dq(q, t)
+
+    return Problem(
+        nodes=nodes,
+        canon=canon.astype(np.float32),
+        corrs=corrs,
+        init_transforms=warp_at(init_bend_deg, init_twist_deg),
+        gt_transforms=warp_at(bend_deg, twist_deg),
+        meta=dict(
+            kind="cylinders",
+            seed=seed,
+            width=width,
+            height=height,
+            num_nodes=int(nodes.shape[0]),
+            num_corrs=int(M),
+            coverage=float(hit.mean()),
+            bend_deg=bend_deg,
+            twist_deg=twist_deg,
+        ),
+    )
+
+
+# --------------------------------------------------------------------------
+# named workloads
+# --------------------------------------------------------------------------
+
+
+def config1(seed=1):
+    """Small plain solve: sphere r=0.3 m, N=256, M=20k, <=15 deg / 2 cm warp."""
+    return sphere_problem(num_nodes=256, num_corrs=20000, seed=seed)
+
+
+def config2(seed=2):
+    """Full frame: 640x480 two-cylinder depth, N=2048, M~300k."""
+    return cylinder_problem(seed=seed)
+
+
+def config3(seed=3):
+    """Precision study: 1280x960, N=8192, M~1.2M."""
+    return cylinder_problem(
+        width=1280, height=960, fx=2 * 570.342, fy=2 * 570.342, cx=640.0, cy=480.0, num_nodes=8192, seed=seed
+    )
+
+
+def config4(num_problems=64, seed=4, n_range=(500, 8000), corr_per_node=150):
+    """Batched uneven solves: N ~ U[500, 8000], M = 150 N +- 20 %, warps
+    <= 20 deg / 3 cm, sigma 1 mm, 5 % outliers (sphere generator)."""
+    rng = np.random.default_rng(seed)
+    probs = []
+    for i in range(num_problems):
+        n = int(rng.integers(n_range[0], n_range[1] + 1))
+        m = int(round(corr_per_node * n * rng.uniform(0.8, 1.2)))
+        radius = float(rng.uniform(0.2, 0.4))
+        spacing = np.sqrt(4 * np.pi * radius**2 / n)
+        probs.append(
+            sphere_problem(
+                num_nodes=n,
+                num_corrs=m,
+                radius=radius,
+                node_radius=spacing,
+                max_rot_deg=20.0,
+                max_trans=0.03,
+                seed=int(rng.integers(1 << 30)),
+            )
+        )
+    return probs

@@ -1,0 +1,249 @@
+/*
+ * cudafusion_b200.h — C ABI of the B200 (sm_100a) non-rigid warp-field solve.
+ *
+ * This library replaces one path of CUDAFusion: the per-frame Gauss-Newton +
+ * block-Jacobi PCG solve over a dual-quaternion deformation graph and the node
+ * update around it.  Every entry point below names the reference interface it
+ * stands in for (file:line inside the CUDAFusion project).
+ *
+ * Conventions
+ *  - All pointers named d_* are device pointers owned by the caller.
+ *  - `stream` is a cudaStream_t passed as void* so that this header needs no
+ *    CUDA include; NULL means the legacy default stream.
+ *  - Every call is asynchronous on `stream` unless it returns statistics to
+ *    host memory (those calls synchronise `stream` before returning).
+ *  - Calls return a cf_status; no call terminates the process (the reference's
+ *    CUDA_CHECK exits, include/types.h:14-20).
+ *  - A handle is not thread-safe: use one handle per host thread.
+ */
+#ifndef CUDAFUSION_B200_H
+#define CUDAFUSION_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define CF_API __attribute__((visibility("default")))
+#else
+#define CF_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#define CF_ALIGN16 alignas(16)
+#else
+#define CF_ALIGN16 _Alignas(16)
+#endif
+
+#define CF_K_NEIGHBORS 4 /* skinning nodes per point, include/types.h:182 */
+#define CF_K_GRAPH 8     /* graph neighbours per node, include/types.h:183 */
+#define CF_BLOCK_DIM 6   /* include/types.h:212 */
+#define CF_BLOCK_SIZE 36 /* include/types.h:213 */
+#define CF_MAX_GN_ITERS 32
+#define CF_MAX_NODES_DEFAULT 8192 /* WarpField::MAX_NODES, include/warp_field.h:14 */
+
+/* ------------------------------------------------------------------------ */
+/* Byte-compatible mirrors of the reference structs (include/types.h).       */
+/* ------------------------------------------------------------------------ */
+
+typedef struct cf_vec3 { float x, y, z; } cf_vec3;           /* float3 */
+typedef struct cf_quat { CF_ALIGN16 float x; float y, z, w; } cf_quat; /* float4 (16-B aligned) */
+
+/* DualQuat, include/types.h:86-94 (32 B, 16-B aligned).  real = rotation
+ * quaternion (x,y,z,w); dual = 0.5 * t * real.  A node transform is read as
+ * centred at its node: T(p) = R (p - c) + c + t. */
+typedef struct cf_dual_quat {
+  cf_quat real;
+  cf_quat dual;
+} cf_dual_quat;
+
+/* DeformNode, include/types.h:185-192 (96 B). */
+typedef struct cf_deform_node {
+  cf_vec3 pos;
+  cf_vec3 normal;
+  float radius;
+  int neighbors[CF_K_GRAPH];
+  float neighbor_w[CF_K_GRAPH];
+  int num_neighbors;
+} cf_deform_node;
+
+/* Correspondence, include/types.h:198-206 (76 B; `valid` is a C++ bool). */
+typedef struct cf_correspondence {
+  cf_vec3 src;    /* skinned (live) point */
+  cf_vec3 dst;    /* target point */
+  cf_vec3 normal; /* target normal */
+  int node_ids[CF_K_NEIGHBORS];
+  float node_ws[CF_K_NEIGHBORS];
+  float weight;
+  uint8_t valid;
+  uint8_t pad_[3];
+} cf_correspondence;
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------ */
+
+typedef enum cf_status {
+  CF_OK = 0,
+  CF_ERR_INVALID_ARG = 1,  /* null pointer, negative size, bad alignment */
+  CF_ERR_OOM = 2,          /* device allocation failed */
+  CF_ERR_NON_FINITE = 3,   /* a NaN/Inf reached the solution or the energy */
+  CF_ERR_TIMEOUT = 4,      /* a bounded in-kernel barrier gave up waiting */
+  CF_ERR_CUDA = 5,         /* any other CUDA runtime error */
+  CF_ERR_CAPACITY = 6,     /* a size exceeds what the handle was created for */
+  CF_ERR_NOT_IMPLEMENTED = 7,
+  CF_ERR_NO_DEVICE = 8
+} cf_status;
+
+CF_API const char* cf_status_string(cf_status s);
+
+/* ------------------------------------------------------------------------ */
+/* Solver parameters: GaussNewtonSolver::Params, include/solver.h:13-22.     */
+/* Field order and defaults are the reference's.                             */
+/* ------------------------------------------------------------------------ */
+
+typedef struct cf_gn_params {
+  int gn_iterations;    /* 3 */
+  int pcg_iterations;   /* 10 */
+  float pcg_tolerance;  /* 1e-4: absolute ||r|| stop, solver_kernels.cu:669 */
+  float lambda_smooth;  /* 1.0: ARAP weight */
+  float lambda_rot;     /* 1.0: kept for layout; the reference never reads it */
+  float lambda_damping; /* 1e-2: relative Levenberg damping, solver_kernels.cu:167-194 */
+  int debug;            /* 0 */
+} cf_gn_params;
+
+/* Fills the reference defaults (include/solver.h:15-21). */
+CF_API cf_status cf_gn_params_default(cf_gn_params* p);
+
+/* Opaque solver handle: owns the block pattern, the BSR values, the rhs, the
+ * block-Jacobi inverses and the PCG vectors (the reference allocates the same
+ * set in GaussNewtonSolver's constructor, kernels/solver_kernels.cu:486-496). */
+typedef struct cf_gn cf_gn;
+
+/* GaussNewtonSolver::GaussNewtonSolver(const Params&, int max_nodes),
+ * include/solver.h:24.  `max_corrs` bounds num_corrs of later calls (the
+ * reference sizes nothing by it because it accumulates with atomics). */
+CF_API cf_status cf_gn_create(const cf_gn_params* params, int max_nodes, int max_corrs,
+                       cf_gn** out);
+CF_API cf_status cf_gn_destroy(cf_gn* h);
+CF_API cf_status cf_gn_set_params(cf_gn* h, const cf_gn_params* params);
+CF_API cf_status cf_gn_get_params(const cf_gn* h, cf_gn_params* params);
+
+/* GaussNewtonSolver::solve, include/solver.h:29-35 and
+ * kernels/solver_kernels.cu:543-570: ONE linearisation at the given
+ * correspondences (src already skinned) -> delta_x [6*num_nodes], ordered
+ * (w_x, w_y, w_z, v_x, v_y, v_z) per node.  The transforms are read only by
+ * the ARAP term.  The block pattern is rebuilt when num_nodes differs from the
+ * previous call, exactly like the reference (solver_kernels.cu:553-561). */
+CF_API cf_status cf_gn_linearize_solve(cf_gn* h, const cf_correspondence* d_corrs,
+                                int num_corrs, const cf_deform_node* d_nodes,
+                                const cf_dual_quat* d_transforms, int num_nodes,
+                                float* d_delta_x, void* stream);
+
+/* Options (no reference counterpart; the defaults reproduce the reference):
+ *  CF_OPT_ARAP_CONSISTENT  0: the reference's ARAP rotation Jacobian
+ *                          (kernels/solver_kernels.cu:140-165, rows q x e_a);
+ *                          1: the consistent derivative e_a x q of the left
+ *                          update.  With 0 the GN energy can rise for large
+ *                          lambda_smooth, exactly as in the reference.
+ *  CF_OPT_PCG_CTAS         CTAs of the persistent PCG kernel (0 = automatic). */
+#define CF_OPT_ARAP_CONSISTENT 1
+#define CF_OPT_PCG_CTAS 2
+CF_API cf_status cf_gn_set_option(cf_gn* h, int option, int value);
+
+/* Synchronises `stream` and converts the device error flags of the last
+ * solve (bounded-barrier timeout, non-finite result) into a status. */
+CF_API cf_status cf_gn_check(cf_gn* h, void* stream);
+
+/* Forces a rebuild of the block pattern from d_nodes on the next solve (the
+ * reference keys its cache on num_nodes only, solver_kernels.cu:554; this
+ * closes that gap for callers that change topology at constant N). */
+CF_API cf_status cf_gn_invalidate_pattern(cf_gn* h);
+
+/* GaussNewtonSolver::system_matrix() / rhs(), include/solver.h:38-39: copies
+ * the last assembled system to HOST memory.  Any pointer may be NULL; the
+ * counts are returned through num_rows/num_blocks.  Synchronises `stream`. */
+CF_API cf_status cf_gn_get_system(cf_gn* h, int* num_rows, int* num_blocks,
+                           int* h_row_ptr, int* h_col_idx, float* h_values,
+                           float* h_rhs, void* stream);
+
+/* Statistics of the last solve (host copy). */
+typedef struct cf_solve_stats {
+  double energy_initial;                   /* E at the first linearisation point */
+  double energy_final;                     /* E after the last node update */
+  double energy_per_iter[CF_MAX_GN_ITERS]; /* E at each linearisation point */
+  int pcg_iterations[CF_MAX_GN_ITERS];     /* PCG iterations run per GN iteration */
+  double pcg_residual[CF_MAX_GN_ITERS];    /* final ||r|| per GN iteration */
+  int gn_iterations_run;
+  int num_blocks;          /* nnzb of the block pattern */
+  int precond_fallbacks;   /* diagonal blocks whose Cholesky failed (last GN it.) */
+  int error_flags;         /* bit 0: barrier timeout, bit 1: non-finite */
+} cf_solve_stats;
+
+/* One problem of the multi-iteration solve.  The correspondences carry the
+ * canonical point separately: each GN iteration re-skins it with the current
+ * node transforms (se3_math.cuh:450-510), which in the reference happens
+ * upstream of the solver (src/skinning_kernels.cu:29-63). */
+typedef struct cf_problem {
+  const cf_deform_node* nodes;     /* device, num_nodes */
+  int num_nodes;
+  const float* canon_points;       /* device, 3*num_corrs, xyz per correspondence */
+  const cf_correspondence* corrs;  /* device, num_corrs; src is ignored */
+  int num_corrs;
+  float max_rot;                   /* twist clamp per node (rad), <=0: off */
+  float max_trans;                 /* twist clamp per node (m),   <=0: off */
+  float update_scale;              /* 1.0 */
+} cf_problem;
+
+/* G full Gauss-Newton iterations (G = params.gn_iterations) on one problem:
+ * per iteration re-skin -> assemble -> block-Jacobi PCG -> clamped DQ update
+ * T_i <- exp(dx_i) * T_i (src/warp_field.cu:250-291), then the energy at the
+ * final transforms.  d_transforms is updated in place.  `stats` may be NULL
+ * (then the call does not synchronise). */
+CF_API cf_status cf_gn_solve(cf_gn* h, const cf_problem* problem,
+                      cf_dual_quat* d_transforms, cf_solve_stats* stats,
+                      void* stream);
+
+/* Per-phase device timing (no reference counterpart; the reference times the
+ * whole solve with std::chrono, include/fusion_app.h:386-391).  When enabled,
+ * every kernel launch of a solve is bracketed by CUDA events on the launch
+ * stream; cf_gn_profile_read synchronises and returns, per phase slot, the
+ * summed device milliseconds and the launch count since the last enable.
+ * cf_gn_launch_count returns the total kernel launches made by the handle. */
+#define CF_PROF_SLOTS 12
+CF_API cf_status cf_gn_profile_enable(cf_gn* h, int on);
+CF_API cf_status cf_gn_profile_read(cf_gn* h, double* ms, int* launches, int n_slots);
+CF_API const char* cf_gn_profile_name(int slot);
+CF_API cf_status cf_gn_launch_count(const cf_gn* h, long long* launches);
+
+/* ------------------------------------------------------------------------ */
+/* Warp field: WarpField, include/warp_field.h:12-126 (the solve-path subset)*/
+/* ------------------------------------------------------------------------ */
+
+/* WarpField::apply_twist_increment, include/warp_field.h:92-94 and
+ * src/warp_field.cu:250-291,1121-1141: per node, twist = update_scale*dx,
+ * clamp ||w||<=max_rot and ||v||<=max_trans (when > 0), then
+ * T_i <- dq_mul(dq_from_twist(twist), T_i). */
+CF_API cf_status cf_warp_apply_twist(cf_dual_quat* d_transforms, const float* d_delta_x,
+                              int num_nodes, float max_rot, float max_trans,
+                              float update_scale, void* stream);
+
+/* DQ skinning of points: warp_point, include/se3_math.cuh:450-510, as used by
+ * skin_vertices_from_voxel_knn_kernel (src/skinning_kernels.cu:29-63) with
+ * per-point node ids/weights instead of a voxel lookup.  d_out may alias
+ * d_points. */
+CF_API cf_status cf_warp_skin_points(const float* d_points, const int* d_node_ids,
+                              const float* d_node_ws, int num_points,
+                              const cf_deform_node* d_nodes,
+                              const cf_dual_quat* d_transforms, int num_nodes,
+                              float* d_out, void* stream);
+
+/* Library / device information. */
+CF_API cf_status cf_get_version(int* major, int* minor, int* patch);
+CF_API cf_status cf_last_cuda_error(char* buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUDAFUSION_B200_H */

@@ -1,0 +1,202 @@
+"""ctypes front end of the CPU oracle (oracle/cf_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py as the checker.  The product library never loads
+it.  `precision` is "f32" (reference operand order, FP32) or "f64".
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+from cudafusion_b200.types import CORR_DTYPE, DQ_DTYPE, NODE_DTYPE
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcforacle.so")
+
+_lib = None
+
+
+class GNParams(ctypes.Structure):
+    """cf_gn_params (include/cudafusion_b200.h) = GaussNewtonSolver::Params."""
+
+    _fields_ = [
+        ("gn_iterations", ctypes.c_int),
+        ("pcg_iterations", ctypes.c_int),
+        ("pcg_tolerance", ctypes.c_float),
+        ("lambda_smooth", ctypes.c_float),
+        ("lambda_rot", ctypes.c_float),
+        ("lambda_damping", ctypes.c_float),
+        ("debug", ctypes.c_int),
+    ]
+
+
+def params(gn_iterations=3, pcg_iterations=10, pcg_tolerance=1e-4, lambda_smooth=1.0, lambda_rot=1.0,
+           lambda_damping=1e-2, debug=0):
+    return GNParams(gn_iterations, pcg_iterations, pcg_tolerance, lambda_smooth, lambda_rot, lambda_damping, debug)
+
+
+def build():
+    """Compiles the oracle with the recipe in oracle/Makefile."""
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(LIB_PATH)
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def _fn(name, precision):
+    f = getattr(lib(), f"{name}_{precision}")
+    return f
+
+
+def build_pattern(nodes):
+    """kernels/solver_kernels.cu:498-541 -> (row_ptr, col_idx)."""
+    nodes = np.ascontiguousarray(nodes, NODE_DTYPE)
+    n = nodes.shape[0]
+    row_ptr = np.zeros(n + 1, np.int32)
+    f = lib().cfo_build_pattern
+    f.restype = ctypes.c_int
+    nnzb = f(_p(nodes), n, _p(row_ptr), None, 0)
+    col_idx = np.zeros(max(nnzb, 1), np.int32)
+    f(_p(nodes), n, _p(row_ptr), _p(col_idx), nnzb)
+    return row_ptr, col_idx[:nnzb]
+
+
+def exp_se3(twist, precision="f32"):
+    tw = np.ascontiguousarray(twist, np.float32)
+    out = np.zeros(16, np.float32)
+    _fn("cfo_exp_se3", precision)(_p(tw), _p(out))
+    return out.reshape(4, 4)
+
+
+def mat4_to_dq(T, precision="f32"):
+    T = np.ascontiguousarray(T, np.float32).reshape(16)
+    out = np.zeros(1, DQ_DTYPE)
+    _fn("cfo_mat4_to_dq", precision)(_p(T), _p(out))
+    return out[0]
+
+
+def dq_mul(a, b, precision="f32"):
+    a = np.ascontiguousarray(np.atleast_1d(a), DQ_DTYPE)
+    b = np.ascontiguousarray(np.atleast_1d(b), DQ_DTYPE)
+    out = np.zeros(1, DQ_DTYPE)
+    _fn("cfo_dq_mul", precision)(_p(a), _p(b), _p(out))
+    return out[0]
+
+
+def dq_centered(a, c, precision="f32"):
+    a = np.ascontiguousarray(np.atleast_1d(a), DQ_DTYPE)
+    c = np.ascontiguousarray(c, np.float32)
+    out = np.zeros(1, DQ_DTYPE)
+    _fn("cfo_dq_centered", precision)(_p(a), _p(c), _p(out))
+    return out[0]
+
+
+def dq_transform_point(a, p, precision="f32"):
+    a = np.ascontiguousarray(np.atleast_1d(a), DQ_DTYPE)
+    p = np.ascontiguousarray(p, np.float32)
+    out = np.zeros(3, np.float32)
+    _fn("cfo_dq_transform_point", precision)(_p(a), _p(p), _p(out))
+    return out
+
+
+def dq_transform_point_centered(a, p, c, precision="f32"):
+    a = np.ascontiguousarray(np.atleast_1d(a), DQ_DTYPE)
+    p = np.ascontiguousarray(p, np.float32)
+    c = np.ascontiguousarray(c, np.float32)
+    out = np.zeros(3, np.float32)
+    _fn("cfo_dq_transform_point_centered", precision)(_p(a), _p(p), _p(c), _p(out))
+    return out
+
+
+def skin(canon, ids, ws, nodes, transforms, precision="f32"):
+    canon = np.ascontiguousarray(canon, np.float32)
+    ids = np.ascontiguousarray(ids, np.int32)
+    ws = np.ascontiguousarray(ws, np.float32)
+    nodes = np.ascontiguousarray(nodes, NODE_DTYPE)
+    transforms = np.ascontiguousarray(transforms, DQ_DTYPE)
+    out = np.zeros_like(canon)
+    _fn("cfo_skin", precision)(_p(canon), _p(ids), _p(ws), canon.shape[0], _p(nodes), _p(transforms),
+                               nodes.shape[0], _p(out))
+    return out
+
+
+def apply_twist(transforms, dx, max_rot=0.0, max_trans=0.0, scale=1.0, precision="f32"):
+    T = np.array(transforms, DQ_DTYPE, copy=True)
+    dx = np.ascontiguousarray(dx, np.float32)
+    _fn("cfo_apply_twist", precision)(_p(T), _p(dx), T.shape[0], ctypes.c_float(max_rot), ctypes.c_float(max_trans),
+                                      ctypes.c_float(scale))
+    return T
+
+
+def assemble(corrs, nodes, transforms, row_ptr, col_idx, lambda_smooth=1.0, lambda_damping=1e-2,
+             precision="f64", nthreads=1):
+    corrs = np.ascontiguousarray(corrs, CORR_DTYPE)
+    nodes = np.ascontiguousarray(nodes, NODE_DTYPE)
+    transforms = np.ascontiguousarray(transforms, DQ_DTYPE)
+    n = nodes.shape[0]
+    A = np.zeros((len(col_idx), 6, 6), np.float64)
+    b = np.zeros(n * 6, np.float64)
+    f = _fn("cfo_assemble", precision)
+    f.restype = ctypes.c_double
+    e = f(_p(corrs), corrs.shape[0], _p(nodes), _p(transforms), n, _p(row_ptr), _p(col_idx),
+          ctypes.c_float(lambda_smooth), ctypes.c_float(lambda_damping), _p(A), _p(b), nthreads)
+    return A, b, e
+
+
+def linearize_solve(corrs, nodes, transforms, prm, row_ptr=None, col_idx=None, precision="f64", nthreads=1):
+    """GaussNewtonSolver::solve restated: returns (dx[N*6], iterations,
+    energy, final_r, fallbacks)."""
+    corrs = np.ascontiguousarray(corrs, CORR_DTYPE)
+    nodes = np.ascontiguousarray(nodes, NODE_DTYPE)
+    transforms = np.ascontiguousarray(transforms, DQ_DTYPE)
+    if row_ptr is None:
+        row_ptr, col_idx = build_pattern(nodes)
+    n = nodes.shape[0]
+    dx = np.zeros(n * 6, np.float32)
+    st = np.zeros(3, np.float64)
+    f = _fn("cfo_linearize_solve", precision)
+    f.restype = ctypes.c_int
+    it = f(_p(corrs), corrs.shape[0], _p(nodes), _p(transforms), n, _p(row_ptr), _p(col_idx), ctypes.byref(prm),
+           _p(dx), _p(st), nthreads)
+    return dx, it, st[0], st[1], int(st[2])
+
+
+def gn_solve(problem, prm, max_rot=0.0, max_trans=0.0, scale=1.0, transforms=None, precision="f64", nthreads=1):
+    """G GN iterations with re-skinning (the cf_gn_solve schedule).
+    Returns (transforms, energies[G+1], pcg_iters[G])."""
+    nodes = np.ascontiguousarray(problem.nodes, NODE_DTYPE)
+    corrs = np.ascontiguousarray(problem.corrs, CORR_DTYPE)
+    canon = np.ascontiguousarray(problem.canon, np.float32)
+    T = np.array(problem.init_transforms if transforms is None else transforms, DQ_DTYPE, copy=True)
+    row_ptr, col_idx = build_pattern(nodes)
+    G = prm.gn_iterations
+    energies = np.zeros(G + 1, np.float64)
+    iters = np.zeros(max(G, 1), np.int32)
+    _fn("cfo_gn_solve", precision)(_p(canon), _p(corrs), corrs.shape[0], _p(nodes), nodes.shape[0], _p(row_ptr),
+                                   _p(col_idx), ctypes.byref(prm), ctypes.c_float(max_rot),
+                                   ctypes.c_float(max_trans), ctypes.c_float(scale), _p(T), _p(energies), _p(iters),
+                                   nthreads)
+    return T, energies, iters[:G]
+
+
+def energy(problem, transforms, lambda_smooth, precision="f64", nthreads=1):
+    nodes = np.ascontiguousarray(problem.nodes, NODE_DTYPE)
+    corrs = np.ascontiguousarray(problem.corrs, CORR_DTYPE)
+    canon = np.ascontiguousarray(problem.canon, np.float32)
+    T = np.ascontiguousarray(transforms, DQ_DTYPE)
+    f = _fn("cfo_energy", precision)
+    f.restype = ctypes.c_double
+    return f(_p(canon), _p(corrs), corrs.shape[0], _p(nodes), _p(T), nodes.shape[0], ctypes.c_float(lambda_smooth),
+             nthreads)
