@@ -201,6 +201,10 @@ def run_b200(args, world, rank, local):
     prm = Params(gn_iterations=GN_ITERS, pcg_iterations=PCG_ITERS, pcg_tolerance=PCG_TOL,
                  lambda_smooth=LAMBDA_SMOOTH, lambda_damping=LAMBDA_DAMP)
     solver = GaussNewtonSolver(prm, max_nodes=8192, max_corrs=max(M, 1))
+    if args.pcg_mode:
+        from cudafusion_b200 import _lib
+
+        solver.set_option(_lib.CF_OPT_PCG_MODE, args.pcg_mode)
     dp = DeviceProblem(problem)
     T = dp.init_transforms.clone()
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
@@ -418,6 +422,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--pcg-mode", type=int, default=0, help="0 auto, 1 grid-wide, 2 single cluster")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()

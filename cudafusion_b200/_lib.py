@@ -20,6 +20,8 @@ CF_ERR_NO_DEVICE = 8
 
 CF_OPT_ARAP_CONSISTENT = 1
 CF_OPT_PCG_CTAS = 2
+CF_OPT_PCG_MODE = 3
+CF_OPT_PCG_PIPELINED = 4
 CF_MAX_GN_ITERS = 32
 CF_PROF_SLOTS = 12
 

@@ -34,6 +34,9 @@ struct cf_gn {
   int device = 0, sms = 0;
   int arap_consistent = 0;
   int pcg_ctas_override = 0;
+  int pcg_mode = 0;  // 0 auto, 1 grid-wide cooperative, 2 single cluster
+  int pcg_pipelined = 0;
+  int phase_timers = 0;
   Work w;
   Pattern p;
   int pattern_N = -1;
@@ -85,14 +88,17 @@ void free_pattern(Pattern& p) {
   dfree(p.upper_pos); dfree(p.upper_row); dfree(p.arap_row_ptr); dfree(p.arap_row_inc);
   dfree(p.arap_blk_ptr); dfree(p.arap_blk_edge); dfree(p.edge_ijk); dfree(p.values);
   dfree(p.seg_off); dfree(p.seg_cnt); dfree(p.pcg_row_begin);
+  dfree(p.clu_row_begin); dfree(p.cta_of_row); dfree(p.ustart); dfree(p.low_ptr); dfree(p.low_pack);
+  dfree(p.low_jl); dfree(p.g_vidx); dfree(p.g_halo_ptr); dfree(p.g_halo_col);
+  dfree(p.off_upper);
   p = Pattern();
 }
 
 void free_work(Work& w) {
   dfree(w.pk_src); dfree(w.pk_dst); dfree(w.pk_nrm); dfree(w.pk_ids); dfree(w.pk_ws);
   dfree(w.c_srcfw); dfree(w.c_nres); dfree(w.cnt); dfree(w.node_total); dfree(w.inc_start);
-  dfree(w.inc); dfree(w.trip); dfree(w.rhs); dfree(w.plain); dfree(w.x); dfree(w.z); dfree(w.p0); dfree(w.p1);
-  dfree(w.partials); dfree(w.barrier); dfree(w.err); dfree(w.e_data_part); dfree(w.e_arap_part); dfree(w.stats);
+  dfree(w.inc); dfree(w.trip); dfree(w.ekeys); dfree(w.rhs); dfree(w.plain); dfree(w.x); dfree(w.z); dfree(w.p0); dfree(w.p1);
+  dfree(w.partials); dfree(w.barrier); dfree(w.err); dfree(w.e_data_part); dfree(w.e_arap_part); dfree(w.stats); dfree(w.timers);
 }
 
 cudaError_t alloc_work(Work& w, int max_nodes, int max_corrs, int bin_ctas_max) {
@@ -105,10 +111,11 @@ cudaError_t alloc_work(Work& w, int max_nodes, int max_corrs, int bin_ctas_max) 
   A_(w.pk_src, M); A_(w.pk_dst, M); A_(w.pk_nrm, M); A_(w.pk_ids, M); A_(w.pk_ws, M);
   A_(w.c_srcfw, M); A_(w.c_nres, M);
   A_(w.cnt, (size_t)bin_ctas_max * N); A_(w.node_total, N); A_(w.inc_start, N + 1);
-  A_(w.inc, 4 * M); A_(w.trip, 16 * M);
+  A_(w.inc, 4 * M); A_(w.trip, 16 * M); A_(w.ekeys, 4 * M);
   A_(w.rhs, 6 * N); A_(w.plain, N); A_(w.x, 6 * N); A_(w.z, 6 * N); A_(w.p0, 6 * N); A_(w.p1, 6 * N);
-  A_(w.partials, (size_t)2 * 2 * kMaxPcgCtas); A_(w.barrier, 1); A_(w.err, 1);
+  A_(w.partials, (size_t)2 * 3 * kMaxPcgCtas); A_(w.barrier, (size_t)kMaxPcgCtas); A_(w.err, 1);
   A_(w.e_data_part, (size_t)kEnergyCtas); A_(w.e_arap_part, N); A_(w.stats, 1);
+  A_(w.timers, (size_t)kTimerSlots);
 #undef A_
   return cudaSuccess;
 }
@@ -224,60 +231,139 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
       ablk_edge[fb[upper_of_pos[find(i, j)]]++] = e;
     }
   }
-  // PCG partition: contiguous rows with balanced block counts
+  // PCG partition: contiguous rows with balanced block counts; per CTA the
+  // distinct halo columns and, per block, its operand slot ([own | halo])
+  const bool pipe = h->pcg_pipelined != 0;
   int G = h->pcg_ctas_override > 0 ? h->pcg_ctas_override : std::min(h->sms, std::max(1, N / 8));
   G = std::max(1, std::min({G, N, kMaxPcgCtas}));
-  std::vector<int> rb;
+  std::vector<int> rb2, g_vidx(std::max(1, nnzb)), g_halo_ptr, g_halo_col;
   int smem = 0;
   bool a_smem = true;
   for (int attempt = 0; attempt < 64; attempt++) {
-    rb.assign(1, 0);
+    std::vector<int> rb(1, 0);
     long long target = ((long long)nnzb + G - 1) / G;
     int start = 0;
-    for (int c = 0; c < G; c++) {
-      int remaining_ctas = G - c;
-      if (start >= N) { rb.push_back(N); continue; }
+    for (int c = 0; c < G && start < N; c++) {
+      int rem = G - c;
       int end = start + 1;
-      if (remaining_ctas == 1) {
+      if (rem == 1) {
         end = N;
       } else {
-        while (end < N - (remaining_ctas - 1) && row_ptr[end] - row_ptr[start] < target) end++;
+        while (end < N - (rem - 1) && row_ptr[end] - row_ptr[start] < target) end++;
       }
       rb.push_back(end);
       start = end;
     }
     rb.back() = N;
-    int max_b = 0, max_r = 0;
-    for (int c = 0; c < G; c++) {
-      max_b = std::max(max_b, row_ptr[rb[c + 1]] - row_ptr[rb[c]]);
-      max_r = std::max(max_r, rb[c + 1] - rb[c]);
+    const int Gc = (int)rb.size() - 1;
+    g_halo_ptr.assign(1, 0);
+    g_halo_col.clear();
+    int need_a = 0, need_noa = 0;
+    for (int c = 0; c < Gc; c++) {
+      const int r0 = rb[c], r1 = rb[c + 1];
+      std::vector<int> halo;
+      for (int q = row_ptr[r0]; q < row_ptr[r1]; q++)
+        if (col_idx[q] < r0 || col_idx[q] >= r1) halo.push_back(col_idx[q]);
+      std::sort(halo.begin(), halo.end());
+      halo.erase(std::unique(halo.begin(), halo.end()), halo.end());
+      for (int q = row_ptr[r0]; q < row_ptr[r1]; q++) {
+        int j = col_idx[q];
+        g_vidx[q] = (j >= r0 && j < r1) ? j - r0
+                                         : (r1 - r0) + (int)(std::lower_bound(halo.begin(), halo.end(), j) - halo.begin());
+      }
+      g_halo_col.insert(g_halo_col.end(), halo.begin(), halo.end());
+      g_halo_ptr.push_back((int)g_halo_col.size());
+      const int nb = row_ptr[r1] - row_ptr[r0], nr = r1 - r0, nh = (int)halo.size();
+      need_a = std::max(need_a, pcg_grid_smem_bytes(nb, nr, nh, true, pipe));
+      need_noa = std::max(need_noa, pcg_grid_smem_bytes(nb, nr, nh, false, pipe));
     }
     const int limit = 200 * 1024;
-    a_smem = true;
-    smem = pcg_smem_bytes(max_b, max_r, true);
-    if (smem > limit) {
-      a_smem = false;
-      smem = pcg_smem_bytes(max_b, max_r, false);
-    }
+    a_smem = need_a <= limit;
+    smem = a_smem ? need_a : need_noa;
     if (smem > limit) {
       if (G >= std::min(N, kMaxPcgCtas)) return CF_ERR_CAPACITY;
       G = std::min(std::min(N, kMaxPcgCtas), G * 2);
       continue;
     }
-    CF_TRY(pcg_prepare(smem, a_smem));
-    int cap = pcg_max_active_ctas(smem, a_smem);
+    int cap = pcg_max_active_ctas(smem, a_smem, pipe);
     if (cap <= 0) return CF_ERR_CAPACITY;
-    if (G > cap) {
+    if (Gc > cap) {
       G = cap;
       continue;
     }
+    rb2 = rb;
     break;
   }
-  // the rows of a CTA must not be empty
-  std::vector<int> rb2(1, 0);
-  for (size_t c = 1; c < rb.size(); c++)
-    if (rb[c] > rb2.back()) rb2.push_back(rb[c]);
+  if (rb2.empty()) return CF_ERR_CAPACITY;
   G = (int)rb2.size() - 1;
+
+  // single-cluster PCG plan: rows split over C CTAs by block count; the upper
+  // blocks live in the owner's shared memory, lower blocks are read from the
+  // owner of their transpose
+  std::vector<int> ustart(N + 1, 0), low_ptr(N + 1, 0), low_u, low_j;
+  for (int i = 0; i < N; i++) ustart[i + 1] = ustart[i] + (row_ptr[i + 1] - diag_pos[i]);
+  {
+    std::vector<std::vector<std::pair<int, int>>> lows(N);  // row i: (j, u of (j, i))
+    for (int j = 0; j < N; j++)
+      for (int q = diag_pos[j] + 1; q < row_ptr[j + 1]; q++) lows[col_idx[q]].push_back({j, upper_of_pos[q]});
+    for (int i = 0; i < N; i++) {
+      std::sort(lows[i].begin(), lows[i].end());
+      low_ptr[i + 1] = low_ptr[i] + (int)lows[i].size();
+      for (auto& pr : lows[i]) {
+        low_j.push_back(pr.first);
+        low_u.push_back(pr.second);
+      }
+    }
+  }
+  int clu_C = 0, clu_smem = 0, clu_nup = 0, clu_nlow = 0, clu_rows = 0;
+  std::vector<int> clu_rb, cta_of_row(N, 0), low_pack(std::max<size_t>(1, low_u.size())),
+      low_jl(std::max<size_t>(1, low_u.size()));
+  if (h->pcg_mode != 1) {
+    const int cands[2] = {16, 8};
+    for (int ci = 0; ci < 2 && !clu_C; ci++) {
+      const int C = cands[ci];
+      if (N < C) continue;
+      // contiguous row ranges balanced by row degree (upper + lower blocks)
+      std::vector<int> rb(1, 0);
+      long long target = ((long long)nnzb + C - 1) / C;
+      int start = 0;
+      for (int c = 0; c < C; c++) {
+        int rem = C - c;
+        int end = start + 1;
+        if (rem == 1) {
+          end = N;
+        } else {
+          while (end < N - (rem - 1) && row_ptr[end] - row_ptr[start] < target) end++;
+        }
+        rb.push_back(end);
+        start = end;
+      }
+      int nu = 0, nl = 0, nr = 0;
+      for (int c = 0; c < C; c++) {
+        nu = std::max(nu, ustart[rb[c + 1]] - ustart[rb[c]]);
+        nl = std::max(nl, low_ptr[rb[c + 1]] - low_ptr[rb[c]]);
+        nr = std::max(nr, rb[c + 1] - rb[c]);
+      }
+      int sm = pcg_cluster_smem_bytes(nu, nl, nr, C, true);
+      if (sm > 227 * 1024 - 1024) continue;
+      if (pcg_cluster_max_active(C, sm, true) < 1) continue;
+      clu_C = C;
+      clu_smem = sm;
+      clu_nup = nu;
+      clu_nlow = nl;
+      clu_rows = nr;
+      clu_rb = rb;
+    }
+    if (clu_C) {
+      for (int c = 0; c < clu_C; c++)
+        for (int r = clu_rb[c]; r < clu_rb[c + 1]; r++) cta_of_row[r] = c;
+      for (size_t l = 0; l < low_u.size(); l++) {
+        int j = low_j[l], owner = cta_of_row[j];
+        low_pack[l] = (owner << 24) | (low_u[l] - ustart[clu_rb[owner]]);
+        low_jl[l] = j - clu_rb[owner];
+      }
+    }
+  }
 
   free_pattern(h->p);
   Pattern& p = h->p;
@@ -289,6 +375,7 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
   p.pcg_ctas = G;
   p.pcg_smem = smem;
   p.pcg_a_in_smem = a_smem ? 1 : 0;
+  p.pcg_pipelined = pipe ? 1 : 0;
   auto up = [](int** d, const std::vector<int>& v) -> cudaError_t {
     cudaError_t e = dalloc(d, v.size());
     if (e != cudaSuccess) return e;
@@ -306,10 +393,35 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
   CF_TRY(up(&p.arap_blk_edge, ablk_edge));
   CF_TRY(up(&p.edge_ijk, eijk));
   CF_TRY(up(&p.pcg_row_begin, rb2));
+  CF_TRY(up(&p.g_vidx, g_vidx));
+  CF_TRY(up(&p.g_halo_ptr, g_halo_ptr));
+  CF_TRY(up(&p.g_halo_col, g_halo_col));
+  p.use_cluster = clu_C ? 1 : 0;
+  p.clu_C = clu_C;
+  p.clu_smem = clu_smem;
+  p.clu_a_in_smem = 1;
+  p.clu_nup_max = clu_nup;
+  p.clu_nlow_max = clu_nlow;
+  p.clu_rows_max = clu_rows;
+  CF_TRY(up(&p.ustart, ustart));
+  CF_TRY(up(&p.low_ptr, low_ptr));
+  if (clu_C) {
+    CF_TRY(up(&p.clu_row_begin, clu_rb));
+    CF_TRY(up(&p.cta_of_row, cta_of_row));
+    CF_TRY(up(&p.low_pack, low_pack));
+    CF_TRY(up(&p.low_jl, low_jl));
+  }
   CF_TRY(dalloc(&p.values, (size_t)nnzb * 36));
   CF_TRY(dalloc(&p.seg_off, (size_t)nnzb));
   CF_TRY(dalloc(&p.seg_cnt, (size_t)nnzb));
   CF_TRY(cudaMemset(p.values, 0, sizeof(float) * (size_t)std::max(1, nnzb) * 36));
+  {
+    std::vector<int> off_upper;
+    for (int u = 0; u < n_upper; u++)
+      if (col_idx[upper_pos[u]] != upper_row[u]) off_upper.push_back(u);
+    p.n_off = (int)off_upper.size();
+    CF_TRY(up(&p.off_upper, off_upper));
+  }
   h->h_row_ptr = row_ptr;
   h->h_col_idx = col_idx;
   h->pattern_N = N;
@@ -344,6 +456,11 @@ cf_status bin_correspondences(cf_gn* h, const cf_correspondence* corrs, const fl
   return CF_OK;
 }
 
+cudaError_t launch_pcg_any(cf_gn* h, const SolveArgs& a, int slot, cudaStream_t s) {
+  if (h->p.use_cluster) return launch_pcg_cluster(h->w, h->p, a, slot, s);
+  return launch_pcg(h->w, h->p, a, slot, s);
+}
+
 SolveArgs make_args(const cf_gn* h, const cf_deform_node* nodes, int N, int M) {
   SolveArgs a;
   memset(&a, 0, sizeof(a));
@@ -356,6 +473,7 @@ SolveArgs make_args(const cf_gn* h, const cf_deform_node* nodes, int N, int M) {
   a.pcg_tolerance = h->params.pcg_tolerance;
   a.arap_consistent = h->arap_consistent;
   a.spin_limit = 1u << 22;
+  a.timers = h->phase_timers ? h->w.timers : nullptr;
   return a;
 }
 
@@ -393,7 +511,7 @@ cf_status cf_gn_params_default(cf_gn_params* p) {
 cf_status cf_gn_create(const cf_gn_params* params, int max_nodes, int max_corrs, cf_gn** out) {
   if (!out) return CF_ERR_INVALID_ARG;
   *out = nullptr;
-  if (!params || max_nodes <= 0 || max_corrs < 0 || max_corrs >= (1 << 27)) return CF_ERR_INVALID_ARG;
+  if (!params || max_nodes <= 0 || max_corrs < 0 || max_corrs >= (1 << 26)) return CF_ERR_INVALID_ARG;
   if (params->gn_iterations < 0 || params->gn_iterations > CF_MAX_GN_ITERS || params->pcg_iterations < 0)
     return CF_ERR_INVALID_ARG;
   int dev = 0, count = 0;
@@ -454,6 +572,15 @@ cf_status cf_gn_set_option(cf_gn* h, int option, int value) {
     case CF_OPT_ARAP_CONSISTENT:
       h->arap_consistent = value ? 1 : 0;
       return CF_OK;
+    case CF_OPT_PCG_PIPELINED:
+      h->pcg_pipelined = value ? 1 : 0;
+      h->pattern_valid = false;
+      return CF_OK;
+    case CF_OPT_PCG_MODE:
+      if (value < 0 || value > 2) return CF_ERR_INVALID_ARG;
+      h->pcg_mode = value;
+      h->pattern_valid = false;
+      return CF_OK;
     case CF_OPT_PCG_CTAS:
       if (value < 0 || value > kMaxPcgCtas) return CF_ERR_INVALID_ARG;
       h->pcg_ctas_override = value;
@@ -490,7 +617,7 @@ cf_status cf_gn_linearize_solve(cf_gn* h, const cf_correspondence* d_corrs, int 
   a.delta_x = d_delta_x;
   { Timed t(h, s, kProfResidual, 1); CF_TRY(launch_residual(w, num_corrs, num_nodes, false, s)); }
   { Timed t(h, s, kProfAssemble, 1); CF_TRY(launch_assemble(w, h->p, a, d_transforms, s)); }
-  { Timed t(h, s, kProfPcg, 1); CF_TRY(launch_pcg(w, h->p, a, 0, s)); }
+  { Timed t(h, s, kProfPcg, 1); CF_TRY(launch_pcg_any(h, a, 0, s)); }
   h->last_gn = 1;
   return CF_OK;
 }
@@ -523,7 +650,7 @@ cf_status cf_gn_solve(cf_gn* h, const cf_problem* prob, cf_dual_quat* d_transfor
   for (int g = 0; g < G; g++) {
     { Timed t(h, s, kProfResidual, 1); CF_TRY(launch_residual(w, M, N, true, s)); }
     { Timed t(h, s, kProfAssemble, 1); CF_TRY(launch_assemble(w, h->p, a, d_transforms, s)); }
-    { Timed t(h, s, kProfPcg, 1); CF_TRY(launch_pcg(w, h->p, a, g, s)); }
+    { Timed t(h, s, kProfPcg, 1); CF_TRY(launch_pcg_any(h, a, g, s)); }
   }
   { Timed t(h, s, kProfEnergy, 2); CF_TRY(launch_final_energy(w, h->p, a, G, s)); }
   h->last_gn = G;
@@ -577,6 +704,21 @@ const char* cf_gn_profile_name(int slot) {
 cf_status cf_gn_launch_count(const cf_gn* h, long long* launches) {
   if (!h || !launches) return CF_ERR_INVALID_ARG;
   *launches = h->launches;
+  return CF_OK;
+}
+
+// Debug: clock64 phase cycles of CTA 0 of the grid-wide PCG, accumulated
+// over every launch since the call with reset != 0 (which also enables them).
+extern "C" CF_API cf_status cf_gn_debug_pcg_timers(cf_gn* h, int reset, long long* out, int n) {
+  if (!h) return CF_ERR_INVALID_ARG;
+  if (reset) {
+    h->phase_timers = 1;
+    CF_TRY(cudaMemset(h->w.timers, 0, sizeof(long long) * kTimerSlots));
+    return CF_OK;
+  }
+  CF_TRY(cudaDeviceSynchronize());
+  if (out && n > 0)
+    CF_TRY(cudaMemcpy(out, h->w.timers, sizeof(long long) * std::min(n, kTimerSlots), cudaMemcpyDeviceToHost));
   return CF_OK;
 }
 

@@ -228,6 +228,159 @@ __device__ __forceinline__ void jac_row(float3 src, float3 x, float3 n, float w,
   J[3] = w * n.x; J[4] = w * n.y; J[5] = w * n.z;
 }
 
+// 6x6 FP64 Cholesky inverse (se3_math.cuh:152-202); false if not SPD.
+__device__ inline bool inv6_chol_d(const double* A, double* Ainv) {
+  double L[6][6];
+#pragma unroll
+  for (int i = 0; i < 6; i++)
+#pragma unroll
+    for (int j = 0; j < 6; j++) L[i][j] = 0.0;
+  for (int i = 0; i < 6; i++)
+    for (int j = 0; j <= i; j++) {
+      double s = A[i * 6 + j];
+      for (int k = 0; k < j; k++) s -= L[i][k] * L[j][k];
+      if (i == j) {
+        if (!(s > 0.0)) return false;
+        L[i][j] = sqrt(s);
+      } else {
+        L[i][j] = s / L[j][j];
+      }
+    }
+  for (int col = 0; col < 6; col++) {
+    double y[6], x[6];
+    for (int i = 0; i < 6; i++) {
+      double s = (i == col) ? 1.0 : 0.0;
+      for (int k = 0; k < i; k++) s -= L[i][k] * y[k];
+      y[i] = s / L[i][i];
+    }
+    for (int i = 5; i >= 0; i--) {
+      double s = y[i];
+      for (int k = i + 1; k < 6; k++) s -= L[k][i] * x[k];
+      x[i] = s / L[i][i];
+    }
+    for (int i = 0; i < 6; i++) Ainv[i * 6 + col] = x[i];
+  }
+  return true;
+}
+
+// Block-Jacobi inverse of one row, (A_rr + 1e-4 I)^-1 in FP64
+// (kernels/solver_kernels.cu:358-399), computed by a group of 8 lanes of one
+// warp (lane l of the group = threadIdx.x & 7): lane 0 factors A = L L^T
+// keeping reciprocal pivots, lanes 0..5 then solve one column each.  The
+// diagonal fallback of the reference applies when the factorisation fails.
+// blk: the 36 floats of the diagonal block; S: 72 doubles of group scratch;
+// Minv: 36 doubles out.  Every lane of the warp must call it (it syncs the
+// warp); `active` is false for groups without a row.  Returns the fallback flag.
+__device__ inline bool inv6_group(const float* blk, double* S, double* Minv, bool active) {
+  const int l = threadIdx.x & 7;
+  double* L = S;       // lower factor, reciprocal pivots on the diagonal
+  double* D = S + 36;  // A + 1e-4 I
+  if (active)
+    for (int q = l; q < 36; q += 8) D[q] = (double)blk[q] + ((q % 7 == 0) ? (double)1e-4f : 0.0);
+  __syncwarp();
+  int ok = 1;
+  if (active && l == 0) {
+    for (int i = 0; i < 6 && ok; i++)
+      for (int j = 0; j <= i; j++) {
+        double s = D[i * 6 + j];
+        for (int k = 0; k < j; k++) s -= L[i * 6 + k] * L[j * 6 + k];
+        if (i == j) {
+          if (!(s > 0.0)) {
+            ok = 0;
+            break;
+          }
+          L[i * 6 + i] = 1.0 / sqrt(s);
+        } else {
+          L[i * 6 + j] = s * L[j * 6 + j];
+        }
+      }
+  }
+  ok = __shfl_sync(0xffffffffu, ok, (threadIdx.x & 31) & ~7);
+  __syncwarp();
+  if (active && l < 6) {
+    if (ok) {
+      double y[6], x[6];
+      for (int i = 0; i < 6; i++) {
+        double s = (i == l) ? 1.0 : 0.0;
+        for (int k = 0; k < i; k++) s -= L[i * 6 + k] * y[k];
+        y[i] = s * L[i * 6 + i];
+      }
+      for (int i = 5; i >= 0; i--) {
+        double s = y[i];
+        for (int k = i + 1; k < 6; k++) s -= L[k * 6 + i] * x[k];
+        x[i] = s * L[i * 6 + i];
+      }
+      for (int i = 0; i < 6; i++) Minv[i * 6 + l] = x[i];
+    } else {
+      for (int q = 0; q < 6; q++) Minv[l * 6 + q] = (q == l) ? 1.0 / (D[l * 6 + l] + (double)1e-6f) : 0.0;
+    }
+  }
+  __syncwarp();
+  return active && !ok;
+}
+
+// ---- small helpers ----
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ float sel4(float4 v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
+__device__ __forceinline__ int sel4i(int4 v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
+
+__device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
+  float y = v - c;
+  float t = s + y;
+  c = (t - s) - y;
+  s = t;
+}
+
+
+// ARAP edge (kernels/solver_kernels.cu:225-289): residual, effective weight,
+// and the two lever arms of the Jacobians.
+struct Edge {
+  float el;
+  float3 r, qi, qj;
+};
+
+__device__ __forceinline__ Edge eval_edge(const cf_deform_node* nodes, const cf_dual_quat* T, int i, int j, int k,
+                                          float lambda) {
+  Edge o;
+  const float* nwp = reinterpret_cast<const float*>(nodes + i) + 15 + k;  // neighbor_w[k]
+  float nw = fmaxf(__ldg(nwp), 0.05f);
+  float3 xi = node_pos(nodes, i), xj = node_pos(nodes, j);
+  DQ Ti = load_dq_cg(T + i), Tj = load_dq_cg(T + j);
+  float3 ti_xj = dq_transform_point_centered(Ti, xj, xi);
+  float3 ti_xi = dq_transform_point_centered(Ti, xi, xi);
+  float3 tj_xj = dq_transform_point_centered(Tj, xj, xj);
+  float3 rest = sub3(xi, xj), curr = sub3(ti_xi, tj_xj);
+  float dr = sqrtf(rest.x * rest.x + rest.y * rest.y + rest.z * rest.z);
+  float dc = sqrtf(curr.x * curr.x + curr.y * curr.y + curr.z * curr.z);
+  float strain = fabsf(dc - dr) / fmaxf(dr, 1e-6f);
+  float ratio = strain / 0.25f;
+  float sw = expf(-(ratio * ratio));
+  o.r = sub3(ti_xj, tj_xj);
+  float rn = sqrtf(o.r.x * o.r.x + o.r.y * o.r.y + o.r.z * o.r.z);
+  float el = lambda * nw * huber_w(rn, 0.05f) * sw;
+  o.el = (el > 1e-8f) ? el : 0.f;
+  o.qi = sub3(ti_xj, xi);
+  o.qj = sub3(tj_xj, xj);
+  return o;
+}
+
+// 6x3 ARAP Jacobian of kernels/solver_kernels.cu:140-165 (sgn = +1), or the
+// consistent sign (sgn = -1) on the rotation rows.
+__device__ __forceinline__ void arap_jac(float3 q, float sgn, float J[6][3]) {
+  J[0][0] = 0.f; J[0][1] = sgn * q.z; J[0][2] = -sgn * q.y;
+  J[1][0] = -sgn * q.z; J[1][1] = 0.f; J[1][2] = sgn * q.x;
+  J[2][0] = sgn * q.y; J[2][1] = -sgn * q.x; J[2][2] = 0.f;
+  J[3][0] = 1.f; J[3][1] = 0.f; J[3][2] = 0.f;
+  J[4][0] = 0.f; J[4][1] = 1.f; J[4][2] = 0.f;
+  J[5][0] = 0.f; J[5][1] = 0.f; J[5][2] = 1.f;
+}
+
+
 // ---- warp helpers ----
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll

@@ -46,11 +46,29 @@ struct Pattern {
   float* values = nullptr;  // [nnzb*36]
   int* seg_off = nullptr;   // [nnzb]
   int* seg_cnt = nullptr;   // [nnzb]
-  // PCG partition
+  int n_off = 0;            // off-diagonal upper blocks
+  int* off_upper = nullptr; // [n_off] their upper indices
+  // single-cluster PCG (cf_pcg_cluster.cu)
+  int use_cluster = 0;
+  int clu_C = 0;
+  int clu_smem = 0;
+  int clu_a_in_smem = 0;
+  int clu_nup_max = 0, clu_nlow_max = 0, clu_rows_max = 0;
+  int* clu_row_begin = nullptr;  // [clu_C+1]
+  int* cta_of_row = nullptr;     // [N]
+  int* ustart = nullptr;         // [N+1] first upper index of each row
+  int* low_ptr = nullptr;        // [N+1] lower blocks (j, i), j < i, of row i
+  int* low_pack = nullptr;       // (owner CTA << 24) | slot of block (j, i) in the owner's upper blocks
+  int* low_jl = nullptr;         // row j local to its owner CTA
+  // grid PCG partition
   int pcg_ctas = 0;
   int* pcg_row_begin = nullptr;  // [pcg_ctas+1]
   int pcg_smem = 0;
   int pcg_a_in_smem = 0;
+  int pcg_pipelined = 0;
+  int* g_vidx = nullptr;      // [nnzb] operand slot of each block's column in its CTA ([own | halo])
+  int* g_halo_ptr = nullptr;  // [pcg_ctas+1]
+  int* g_halo_col = nullptr;  // distinct columns of other CTAs touched by each CTA
 };
 
 // Per-handle work buffers sized by (max_nodes, max_corrs).
@@ -69,18 +87,20 @@ struct Work {
   int* inc_start = nullptr;   // [max_nodes+1]
   int* inc = nullptr;         // [4*max_corrs]: (c << 2) | a
   int* trip = nullptr;        // [16*max_corrs]: (c << 4) | (a << 2) | b
+  int2* ekeys = nullptr;      // [4*max_corrs]: per incidence, column keys of its 4 slots
   float* rhs = nullptr;       // [6*max_nodes]
   cf_dual_quat* plain = nullptr;  // [max_nodes]
   float* x = nullptr;         // [6*max_nodes]
   float* z = nullptr;
   float* p0 = nullptr;
   float* p1 = nullptr;
-  double* partials = nullptr;  // [2 bufs][2 slots][max pcg ctas]
-  unsigned* barrier = nullptr;
+  double* partials = nullptr;  // [2 bufs][3 slots][max pcg ctas]
+  unsigned* barrier = nullptr;  // [max pcg ctas] generation flags of the grid barrier
   int* err = nullptr;
   double* e_data_part = nullptr;  // [kEnergyCtas]
   double* e_arap_part = nullptr;  // [max_nodes] (per row / per energy CTA)
   DevStats* stats = nullptr;
+  long long* timers = nullptr;  // [kTimerSlots] phase cycles of the grid PCG (debug)
 };
 
 constexpr int kEnergyCtas = 592;  // fixed grid of the residual/energy kernels
@@ -100,7 +120,9 @@ struct SolveArgs {
   float* delta_x;            // non-null: write dx here and do not update
   float max_rot, max_trans, update_scale;
   unsigned spin_limit;
+  long long* timers;  // non-null: CTA 0 of the grid PCG accumulates phase cycles here
 };
+constexpr int kTimerSlots = 12;
 
 // ---- launchers (cf_kernels.cu) ----
 cudaError_t launch_pack_count(const Work& w, const cf_correspondence* corrs, const float* canon, int M, int N,
@@ -120,9 +142,12 @@ cudaError_t launch_apply_twist(cf_dual_quat* T, const float* dx, int N, float ma
 cudaError_t launch_skin_points(const float* pts, const int* ids, const float* ws, int M,
                                const cf_deform_node* nodes, const cf_dual_quat* T, int N, float* out,
                                cudaStream_t s);
-int pcg_smem_bytes(int max_blocks, int max_rows, bool a_in_smem);
-int pcg_max_active_ctas(int smem, bool a_in_smem);
-cudaError_t pcg_prepare(int smem, bool a_in_smem);
+int pcg_grid_smem_bytes(int nblk, int nrows, int nhalo, bool a_in_smem, bool pipelined);
+int pcg_max_active_ctas(int smem, bool a_in_smem, bool pipelined);
 int expand_smem_bytes(int max_upper_row);
+
+int pcg_cluster_smem_bytes(int nup_max, int nlow_max, int rows_max, int C, bool a_in_smem);
+int pcg_cluster_max_active(int C, int smem, bool a_in_smem);
+cudaError_t launch_pcg_cluster(const Work& w, const Pattern& p, const SolveArgs& a, int gn_slot, cudaStream_t s);
 
 }  // namespace cf

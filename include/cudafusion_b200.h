@@ -146,9 +146,18 @@ CF_API cf_status cf_gn_linearize_solve(cf_gn* h, const cf_correspondence* d_corr
  *                          1: the consistent derivative e_a x q of the left
  *                          update.  With 0 the GN energy can rise for large
  *                          lambda_smooth, exactly as in the reference.
- *  CF_OPT_PCG_CTAS         CTAs of the persistent PCG kernel (0 = automatic). */
+ *  CF_OPT_PCG_CTAS         CTAs of the grid-wide PCG kernel (0 = automatic).
+ *  CF_OPT_PCG_MODE         0: automatic; 1: grid-wide cooperative PCG;
+ *                          2: single-cluster PCG when the system fits the
+ *                          cluster's shared memory (else grid-wide).
+ *  CF_OPT_PCG_PIPELINED    0: the reference's PCG (two reductions per
+ *                          iteration); 1: pipelined PCG, the same iterates in
+ *                          exact arithmetic with one reduction per iteration
+ *                          (FP64 recurrences), grid-wide mode only. */
 #define CF_OPT_ARAP_CONSISTENT 1
 #define CF_OPT_PCG_CTAS 2
+#define CF_OPT_PCG_MODE 3
+#define CF_OPT_PCG_PIPELINED 4
 CF_API cf_status cf_gn_set_option(cf_gn* h, int option, int value);
 
 /* Synchronises `stream` and converts the device error flags of the last
