@@ -24,6 +24,7 @@ CF_OPT_PCG_MODE = 3
 CF_OPT_PCG_PIPELINED = 4
 CF_MAX_GN_ITERS = 32
 CF_PROF_SLOTS = 12
+CF_NOALLOC_MAX_NODES = 8192
 
 # Every symbol the public header declares (the ABI test checks the list
 # against include/cudafusion_b200.h).
@@ -40,6 +41,7 @@ EXPORTS = [
     "cf_gn_invalidate_pattern",
     "cf_gn_get_system",
     "cf_gn_solve",
+    "cf_energy_noalloc",
     "cf_warp_apply_twist",
     "cf_warp_skin_points",
     "cf_gn_profile_enable",
@@ -129,6 +131,7 @@ def lib():
         L.cf_gn_invalidate_pattern.argtypes = [vp]
         L.cf_gn_get_system.argtypes = [vp, ctypes.POINTER(i), ctypes.POINTER(i), vp, vp, vp, vp, vp]
         L.cf_gn_solve.argtypes = [vp, ctypes.POINTER(Problem), vp, ctypes.POINTER(SolveStats), vp]
+        L.cf_energy_noalloc.argtypes = [ctypes.POINTER(Problem), vp, f, vp, vp]
         L.cf_warp_apply_twist.argtypes = [vp, vp, i, f, f, f, vp]
         L.cf_warp_skin_points.argtypes = [vp, vp, vp, i, vp, vp, i, vp, vp]
         L.cf_gn_profile_enable.argtypes = [vp, i]

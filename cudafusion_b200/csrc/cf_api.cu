@@ -750,6 +750,17 @@ cf_status cf_gn_get_system(cf_gn* h, int* num_rows, int* num_blocks, int* h_row_
   return CF_OK;
 }
 
+cf_status cf_energy_noalloc(const cf_problem* problem, const cf_dual_quat* d_transforms, float lambda_smooth,
+                            double* d_energy, void* stream) {
+  if (!problem || !d_energy || problem->num_nodes < 0 || problem->num_corrs < 0) return CF_ERR_INVALID_ARG;
+  if (problem->num_nodes > CF_NOALLOC_MAX_NODES) return CF_ERR_CAPACITY;
+  if (problem->num_nodes > 0 && (!problem->nodes || !d_transforms)) return CF_ERR_INVALID_ARG;
+  if (problem->num_corrs > 0 && (!problem->corrs || !problem->canon_points)) return CF_ERR_INVALID_ARG;
+  if (reinterpret_cast<uintptr_t>(d_transforms) & 15u) return CF_ERR_INVALID_ARG;
+  CF_TRY(launch_energy_noalloc(problem, d_transforms, lambda_smooth, d_energy, (cudaStream_t)stream));
+  return CF_OK;
+}
+
 cf_status cf_warp_apply_twist(cf_dual_quat* d_transforms, const float* d_delta_x, int num_nodes, float max_rot,
                               float max_trans, float update_scale, void* stream) {
   if (num_nodes < 0) return CF_ERR_INVALID_ARG;

@@ -142,6 +142,8 @@ cudaError_t launch_apply_twist(cf_dual_quat* T, const float* dx, int N, float ma
 cudaError_t launch_skin_points(const float* pts, const int* ids, const float* ws, int M,
                                const cf_deform_node* nodes, const cf_dual_quat* T, int N, float* out,
                                cudaStream_t s);
+cudaError_t launch_energy_noalloc(const cf_problem* pr, const cf_dual_quat* T, float lambda, double* d_energy,
+                                  cudaStream_t s);
 int pcg_grid_smem_bytes(int nblk, int nrows, int nhalo, bool a_in_smem, bool pipelined);
 int pcg_max_active_ctas(int smem, bool a_in_smem, bool pipelined);
 int expand_smem_bytes(int max_upper_row);

@@ -225,6 +225,25 @@ CF_API cf_status cf_gn_profile_read(cf_gn* h, double* ms, int* launches, int n_s
 CF_API const char* cf_gn_profile_name(int slot);
 CF_API cf_status cf_gn_launch_count(const cf_gn* h, long long* launches);
 
+/* Allocation-free energy (no counterpart in the reference).
+ *
+ * For callers that cannot allocate device memory where they need the energy
+ * (a per-frame loop working inside a fixed memory budget owned by a host
+ * application; code that must not stall on cudaMalloc/cudaFree, which can
+ * synchronise the device and fail under memory pressure).  Computes the
+ * solve's IRLS energy E(T) = sum_c fw_c r_c^2 + sum_edges lambda_eff |r_ij|^2
+ * at d_transforms for `problem` (max_rot/max_trans/update_scale unused) and
+ * writes it to *d_energy (device).  Allocates nothing: its scratch is a static
+ * device array of this library sized for CF_NOALLOC_MAX_NODES nodes (about
+ * 260 KB, held on every GPU that loads the library until exit); larger
+ * problems return CF_ERR_CAPACITY.  The first call on a device looks the
+ * scratch address up (cudaGetSymbolAddress) and must happen before any stream
+ * capture.  Calls share the scratch: calls that overlap on the GPU race and
+ * must be serialised by the caller.  Asynchronous on `stream`. */
+#define CF_NOALLOC_MAX_NODES 8192
+CF_API cf_status cf_energy_noalloc(const cf_problem* problem, const cf_dual_quat* d_transforms,
+                                   float lambda_smooth, double* d_energy, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Warp field: WarpField, include/warp_field.h:12-126 (the solve-path subset)*/
 /* ------------------------------------------------------------------------ */
