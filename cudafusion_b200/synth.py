@@ -500,3 +500,114 @@ def config4(num_problems=64, seed=4, n_range=(500, 8000), corr_per_node=150):
             )
         )
     return probs
+
+
+# --------------------------------------------------------------------------
+# sequences (the learned-initialisation workload)
+# --------------------------------------------------------------------------
+
+
+@dataclass
+class Sequence:
+    """A two-cylinder surface articulating over time.  The canonical model
+    (nodes, surface points, their skin weights) is fixed; frame t places the
+    second segment at bend(t), twist(t) about the joint and observes every
+    model point with depth noise along its viewing ray.  Motion:
+    bend(t) = A/2 (1 - cos(2 pi (t + t0) / period)), twist(t) = W sin(2 pi (t + t1) / twist_period)."""
+
+    nodes: np.ndarray
+    canon: np.ndarray  # float32 [M, 3]
+    canon_normals: np.ndarray  # float64 [M, 3]
+    on_seg2: np.ndarray  # bool [M]
+    node_ids: np.ndarray  # int32 [M, 4]
+    node_ws: np.ndarray  # float32 [M, 4]
+    joint: np.ndarray
+    bend_amp_deg: float = 45.0
+    period: float = 60.0
+    phase: float = 0.0
+    twist_amp_deg: float = 10.0
+    twist_period: float = 150.0
+    twist_phase: float = 0.0
+    noise: float = 0.001
+    seed: int = 5
+
+    @property
+    def num_nodes(self):
+        return int(self.nodes.shape[0])
+
+    @property
+    def num_corrs(self):
+        return int(self.canon.shape[0])
+
+    def pose(self, t):
+        bend = 0.5 * self.bend_amp_deg * (1.0 - np.cos(2.0 * np.pi * (t + self.phase) / self.period))
+        twist = self.twist_amp_deg * np.sin(2.0 * np.pi * (t + self.twist_phase) / self.twist_period)
+        return bend, twist
+
+    def _seg2_quat(self, t):
+        bend, twist = self.pose(t)
+        return _qmul(_rot_y(np.deg2rad(bend)), quat_from_rotvec(np.array([np.deg2rad(twist), 0.0, 0.0])))
+
+    def gt_transforms(self, t):
+        """Exact articulation of the nodes at frame t (centred DualQuats)."""
+        q2 = self._seg2_quat(t)
+        pos = self.nodes["pos"].astype(np.float64)
+        on2 = pos[:, 0] > self.joint[0]
+        q = np.where(on2[:, None], np.broadcast_to(q2, (len(pos), 4)), np.array([0.0, 0.0, 0.0, 1.0]))
+        tr = _qrotate(q, pos - self.joint) + self.joint - pos
+        return centred_dq(q, tr)
+
+    def frame(self, t):
+        """Correspondences of frame t (src = canonical point)."""
+        rng = np.random.default_rng((self.seed, int(t)))
+        q2 = self._seg2_quat(t)
+        live = self.canon.astype(np.float64).copy()
+        nrm = self.canon_normals.copy()
+        m = self.on_seg2
+        qb = np.broadcast_to(q2, (int(m.sum()), 4))
+        live[m] = self.joint + _qrotate(qb, live[m] - self.joint)
+        nrm[m] = _qrotate(qb, nrm[m])
+        z = live[:, 2]
+        dst = live * ((z + rng.normal(scale=self.noise, size=z.shape)) / z)[:, None]
+        corrs = np.zeros(self.num_corrs, CORR_DTYPE)
+        corrs["src"] = self.canon
+        corrs["dst"] = dst
+        corrs["normal"] = nrm
+        corrs["node_ids"] = self.node_ids
+        corrs["node_ws"] = self.node_ws
+        corrs["weight"] = 1.0
+        corrs["valid"] = 1
+        return corrs
+
+    def problem(self, t, init_transforms):
+        return Problem(nodes=self.nodes, canon=self.canon, corrs=self.frame(t), init_transforms=init_transforms,
+                       gt_transforms=self.gt_transforms(t), meta=dict(kind="sequence", seed=self.seed, frame=t))
+
+
+def cylinder_sequence(seed=5, num_nodes=2048, randomize=False, **kw):
+    """The learned-initialisation workload: 640x480 two-cylinder model
+    (radii 6 and 5 cm, N=2048, M~300k), bending 0-45 deg with period 60
+    frames and twisting +-10 deg.  randomize=True draws the motion's phases,
+    periods and amplitudes from the seed (training sequences)."""
+    base = cylinder_problem(num_nodes=num_nodes, bend_deg=0.0, init_bend_deg=0.0, noise=0.0, seed=seed)
+    rng = np.random.default_rng(seed + 7919)
+    canon = base.canon
+    joint = np.array([0.0, 0.0, 0.14])
+    params = dict(bend_amp_deg=45.0, period=60.0, phase=0.0, twist_amp_deg=10.0, twist_period=150.0,
+                  twist_phase=0.0)
+    if randomize:
+        params = dict(bend_amp_deg=float(rng.uniform(30.0, 50.0)), period=float(rng.uniform(45.0, 80.0)),
+                      phase=float(rng.uniform(0.0, 80.0)), twist_amp_deg=float(rng.uniform(5.0, 12.0)),
+                      twist_period=float(rng.uniform(100.0, 200.0)), twist_phase=float(rng.uniform(0.0, 200.0)))
+    params.update(kw)
+    return Sequence(
+        nodes=base.nodes,
+        canon=canon,
+        canon_normals=base.corrs["normal"].astype(np.float64),
+        on_seg2=canon[:, 0].astype(np.float64) > joint[0],
+        node_ids=base.corrs["node_ids"].copy(),
+        node_ws=base.corrs["node_ws"].copy(),
+        joint=joint,
+        seed=seed,
+        **params,
+    )

@@ -1,0 +1,258 @@
+// cudafusion_b200.hpp — C++ drop-in for CUDAFusion's solve-path classes.
+//
+//   cudafusion_b200::GaussNewtonSolver   include/solver.h:10-89
+//   cudafusion_b200::WarpField           include/warp_field.h:12-126 (solve-path subset)
+//
+// Header-only, on top of the C ABI (cudafusion_b200.h, link libcfb200.so).
+// The classes keep the reference's constructor and method signatures and
+// its observable behaviour: every call synchronises the device before it
+// returns, solve() (re)allocates delta_x to 6*num_nodes floats
+// (solver_kernels.cu:551), apply_twist_increment() refreshes the host mirror
+// (warp_field.cu:1135-1140).  The reference's own types are accepted
+// unchanged: any array type with the members `data`, `count` and
+// `allocate(n)` (the reference's DeviceArray<T>, include/types.h:100-142)
+// and the structs DualQuat / DeformNode / Correspondence, whose byte layouts
+// are checked here at compile time.  Errors throw cudafusion_b200::Error (the
+// reference exits through CUDA_CHECK; define CF_DROPIN_EXIT_ON_ERROR to get
+// that behaviour instead).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "cudafusion_b200.h"
+
+namespace cudafusion_b200 {
+
+struct Error : std::runtime_error {
+  cf_status status;
+  Error(cf_status s, const char* where)
+      : std::runtime_error(std::string(where) + ": " + cf_status_string(s)), status(s) {}
+};
+
+inline void check(cf_status s, const char* where) {
+  if (s == CF_OK) return;
+#ifdef CF_DROPIN_EXIT_ON_ERROR
+  std::fprintf(stderr, "cudafusion_b200 error in %s: %s\n", where, cf_status_string(s));
+  std::exit(1);
+#else
+  throw Error(s, where);
+#endif
+}
+
+template <class Node, class DQ, class Corr>
+constexpr bool layouts_match() {
+  return sizeof(Node) == sizeof(cf_deform_node) && sizeof(DQ) == sizeof(cf_dual_quat) &&
+         sizeof(Corr) == sizeof(cf_correspondence) && alignof(DQ) == alignof(cf_dual_quat);
+}
+
+class GaussNewtonSolver {
+ public:
+  // GaussNewtonSolver::Params, include/solver.h:13-22 (same fields and defaults)
+  struct Params {
+    int gn_iterations = 3;
+    int pcg_iterations = 10;
+    float pcg_tolerance = 1e-4f;
+    float lambda_smooth = 1.0f;
+    float lambda_rot = 1.0f;
+    float lambda_damping = 1e-2f;
+    bool debug = false;
+  };
+
+  // include/solver.h:24.  max_corrs bounds num_corrs of later solves.
+  explicit GaussNewtonSolver(const Params& p, int max_nodes, int max_corrs = 1 << 20) : params_(p) {
+    cf_gn_params cp = to_c(p);
+    check(cf_gn_create(&cp, max_nodes, max_corrs, &h_), "GaussNewtonSolver");
+  }
+  ~GaussNewtonSolver() {
+    if (h_) cf_gn_destroy(h_);
+  }
+  GaussNewtonSolver(const GaussNewtonSolver&) = delete;
+  GaussNewtonSolver& operator=(const GaussNewtonSolver&) = delete;
+
+  // include/solver.h:29-35: one linearisation -> delta_x [6*num_nodes].
+  template <class CorrArray, class Node, class DQ, class FloatArray>
+  void solve(const CorrArray& corrs, int num_corrs, const Node* d_nodes, const DQ* d_transforms, int num_nodes,
+             FloatArray& delta_x) {
+    using Corr = typename std::remove_pointer<decltype(corrs.data)>::type;
+    static_assert(layouts_match<Node, DQ, Corr>(), "struct layouts differ from include/types.h");
+    delta_x.allocate((size_t)num_nodes * 6);
+    check(cf_gn_linearize_solve(h_, reinterpret_cast<const cf_correspondence*>(corrs.data), num_corrs,
+                                reinterpret_cast<const cf_deform_node*>(d_nodes),
+                                reinterpret_cast<const cf_dual_quat*>(d_transforms), num_nodes,
+                                reinterpret_cast<float*>(delta_x.data), nullptr),
+          "GaussNewtonSolver::solve");
+    check(cf_gn_check(h_, nullptr), "GaussNewtonSolver::solve");
+  }
+
+  // Host copies of the assembled system (system_matrix() / rhs(),
+  // include/solver.h:38-39, which return device BSR storage in the reference).
+  void system_matrix(std::vector<int>& row_ptr, std::vector<int>& col_idx, std::vector<float>& values) {
+    int n = 0, nb = 0;
+    check(cf_gn_get_system(h_, &n, &nb, nullptr, nullptr, nullptr, nullptr, nullptr), "system_matrix");
+    row_ptr.resize(n + 1);
+    col_idx.resize(nb);
+    values.resize((size_t)nb * 36);
+    check(cf_gn_get_system(h_, &n, &nb, row_ptr.data(), col_idx.data(), values.data(), nullptr, nullptr),
+          "system_matrix");
+  }
+  void rhs(std::vector<float>& b) {
+    int n = 0, nb = 0;
+    check(cf_gn_get_system(h_, &n, &nb, nullptr, nullptr, nullptr, nullptr, nullptr), "rhs");
+    b.resize((size_t)n * 6);
+    check(cf_gn_get_system(h_, &n, &nb, nullptr, nullptr, nullptr, b.data(), nullptr), "rhs");
+  }
+
+  // G full GN iterations with re-skinning from canonical points (no
+  // reference counterpart: the reference runs this loop on the host around
+  // solve(), include/fusion_app.h:256-646).
+  template <class Node, class Corr, class DQ>
+  cf_solve_stats solve_frame(const Node* d_nodes, int num_nodes, const float* d_canon, const Corr* d_corrs,
+                             int num_corrs, DQ* d_transforms, float max_rot, float max_trans,
+                             float update_scale = 1.0f) {
+    static_assert(layouts_match<Node, DQ, Corr>(), "struct layouts differ from include/types.h");
+    cf_problem pr;
+    pr.nodes = reinterpret_cast<const cf_deform_node*>(d_nodes);
+    pr.num_nodes = num_nodes;
+    pr.canon_points = d_canon;
+    pr.corrs = reinterpret_cast<const cf_correspondence*>(d_corrs);
+    pr.num_corrs = num_corrs;
+    pr.max_rot = max_rot;
+    pr.max_trans = max_trans;
+    pr.update_scale = update_scale;
+    cf_solve_stats st;
+    check(cf_gn_solve(h_, &pr, reinterpret_cast<cf_dual_quat*>(d_transforms), &st, nullptr), "solve_frame");
+    return st;
+  }
+
+  cf_gn* handle() { return h_; }
+  const Params& params() const { return params_; }
+
+ private:
+  static cf_gn_params to_c(const Params& p) {
+    cf_gn_params c;
+    c.gn_iterations = p.gn_iterations;
+    c.pcg_iterations = p.pcg_iterations;
+    c.pcg_tolerance = p.pcg_tolerance;
+    c.lambda_smooth = p.lambda_smooth;
+    c.lambda_rot = p.lambda_rot;
+    c.lambda_damping = p.lambda_damping;
+    c.debug = p.debug ? 1 : 0;
+    return c;
+  }
+  Params params_;
+  cf_gn* h_ = nullptr;
+};
+
+// The solve-path part of WarpField: node storage, transforms with
+// save/restore, the twist update.  Graph construction (add_nodes_*,
+// prune_nodes, compute_voxel_knn) stays with the reference.  Node and DQ
+// are the caller's DeformNode / DualQuat types.
+template <class Node, class DQ>
+class WarpField {
+ public:
+  static constexpr int MAX_NODES = CF_MAX_NODES_DEFAULT;  // include/warp_field.h:14
+
+  explicit WarpField(float node_radius, int max_nodes = MAX_NODES) : node_radius_(node_radius), max_nodes_(max_nodes) {
+    static_assert(sizeof(Node) == sizeof(cf_deform_node) && sizeof(DQ) == sizeof(cf_dual_quat), "layouts");
+    check_cuda(cudaMalloc(&d_nodes_, sizeof(Node) * max_nodes), "WarpField");
+    check_cuda(cudaMalloc(&d_T_, sizeof(DQ) * max_nodes), "WarpField");
+    check_cuda(cudaMalloc(&d_Tprev_, sizeof(DQ) * max_nodes), "WarpField");
+  }
+  ~WarpField() {
+    cudaFree(d_nodes_);
+    cudaFree(d_T_);
+    cudaFree(d_Tprev_);
+  }
+  WarpField(const WarpField&) = delete;
+  WarpField& operator=(const WarpField&) = delete;
+
+  int num_nodes() const { return n_; }
+  Node* device_nodes() { return d_nodes_; }
+  DQ* device_transforms() { return d_T_; }
+  DQ* device_transforms_prev() { return d_Tprev_; }
+  const Node* device_nodes() const { return d_nodes_; }
+  const DQ* device_transforms() const { return d_T_; }
+
+  // src/warp_field.cu:1160-1177: identity transforms when the count changes
+  void upload_nodes(const std::vector<Node>& nodes) {
+    const int n = (int)std::min<size_t>(nodes.size(), (size_t)max_nodes_);
+    h_nodes_.assign(nodes.begin(), nodes.begin() + n);
+    check_cuda(cudaMemcpy(d_nodes_, h_nodes_.data(), sizeof(Node) * n, cudaMemcpyHostToDevice), "upload_nodes");
+    if ((int)h_T_.size() != n) {
+      h_T_.assign(n, identity());
+      check_cuda(cudaMemcpy(d_T_, h_T_.data(), sizeof(DQ) * n, cudaMemcpyHostToDevice), "upload_nodes");
+      check_cuda(cudaMemcpy(d_Tprev_, h_T_.data(), sizeof(DQ) * n, cudaMemcpyHostToDevice), "upload_nodes");
+    }
+    n_ = n;
+  }
+  // src/warp_field.cu:1179-1192
+  void upload_transforms(const std::vector<DQ>& T) {
+    int n = (int)std::min<size_t>(T.size(), (size_t)max_nodes_);
+    if (n_ == 0) n_ = n;
+    n = std::min(n, n_);
+    h_T_.assign(T.begin(), T.begin() + n);
+    check_cuda(cudaMemcpy(d_T_, h_T_.data(), sizeof(DQ) * n, cudaMemcpyHostToDevice), "upload_transforms");
+    check_cuda(cudaMemcpy(d_Tprev_, h_T_.data(), sizeof(DQ) * n, cudaMemcpyHostToDevice), "upload_transforms");
+  }
+  std::vector<Node> download_nodes() const { return h_nodes_; }
+  std::vector<DQ> download_transforms() const { return h_T_; }
+
+  // src/warp_field.cu:1106-1119
+  void save_transforms() {
+    check_cuda(cudaMemcpy(d_Tprev_, d_T_, sizeof(DQ) * n_, cudaMemcpyDeviceToDevice), "save_transforms");
+  }
+  void restore_transforms() {
+    check_cuda(cudaMemcpy(d_T_, d_Tprev_, sizeof(DQ) * n_, cudaMemcpyDeviceToDevice), "restore_transforms");
+    h_T_.resize(n_);
+    check_cuda(cudaMemcpy(h_T_.data(), d_T_, sizeof(DQ) * n_, cudaMemcpyDeviceToHost), "restore_transforms");
+  }
+  // src/warp_field.cu:1143-1148
+  void reset_transforms() {
+    h_T_.assign(n_, identity());
+    check_cuda(cudaMemcpy(d_T_, h_T_.data(), sizeof(DQ) * n_, cudaMemcpyHostToDevice), "reset_transforms");
+  }
+  // src/warp_field.cu:1121-1141: T_i <- exp(clamp(scale * dx_i)) * T_i, then the host mirror
+  template <class FloatArray>
+  void apply_twist_increment(const FloatArray& delta_x, float max_rot, float max_trans, float update_scale = 1.0f) {
+    if (n_ == 0) return;
+    check(cf_warp_apply_twist(reinterpret_cast<cf_dual_quat*>(d_T_), reinterpret_cast<const float*>(delta_x.data),
+                              n_, max_rot, max_trans, update_scale, nullptr),
+          "apply_twist_increment");
+    check_cuda(cudaDeviceSynchronize(), "apply_twist_increment");
+    h_T_.resize(n_);
+    check_cuda(cudaMemcpy(h_T_.data(), d_T_, sizeof(DQ) * n_, cudaMemcpyDeviceToHost), "apply_twist_increment");
+  }
+
+  float node_radius() const { return node_radius_; }
+
+ private:
+  static DQ identity() {
+    cf_dual_quat d = {{0.f, 0.f, 0.f, 1.f}, {0.f, 0.f, 0.f, 0.f}};
+    DQ out;
+    static_assert(sizeof(out) == sizeof(d), "layout");
+    std::memcpy(&out, &d, sizeof(d));
+    return out;
+  }
+  static void check_cuda(cudaError_t e, const char* where) {
+    if (e != cudaSuccess) check(CF_ERR_CUDA, where);
+  }
+  float node_radius_;
+  int max_nodes_;
+  int n_ = 0;
+  Node* d_nodes_ = nullptr;
+  DQ* d_T_ = nullptr;
+  DQ* d_Tprev_ = nullptr;
+  std::vector<Node> h_nodes_;
+  std::vector<DQ> h_T_;
+};
+
+}  // namespace cudafusion_b200
