@@ -41,6 +41,7 @@ EXPORTS = [
     "cf_gn_invalidate_pattern",
     "cf_gn_get_system",
     "cf_gn_solve",
+    "cf_gn_solve_batched",
     "cf_energy_noalloc",
     "cf_warp_apply_twist",
     "cf_warp_skin_points",
@@ -131,6 +132,8 @@ def lib():
         L.cf_gn_invalidate_pattern.argtypes = [vp]
         L.cf_gn_get_system.argtypes = [vp, ctypes.POINTER(i), ctypes.POINTER(i), vp, vp, vp, vp, vp]
         L.cf_gn_solve.argtypes = [vp, ctypes.POINTER(Problem), vp, ctypes.POINTER(SolveStats), vp]
+        L.cf_gn_solve_batched.argtypes = [vp, ctypes.POINTER(Problem), i, ctypes.POINTER(vp),
+                                          ctypes.POINTER(SolveStats), vp]
         L.cf_energy_noalloc.argtypes = [ctypes.POINTER(Problem), vp, f, vp, vp]
         L.cf_warp_apply_twist.argtypes = [vp, vp, i, f, f, f, vp]
         L.cf_warp_skin_points.argtypes = [vp, vp, vp, i, vp, vp, i, vp, vp]

@@ -39,10 +39,14 @@ struct cf_gn {
   int phase_timers = 0;
   Work w;
   Pattern p;
-  int pattern_N = -1;
   bool pattern_valid = false;
   std::vector<int> h_row_ptr, h_col_idx;
-  DevStats* h_stats = nullptr;  // pinned
+  std::vector<int> pattern_key;  // problem sizes the pattern was built for
+  DevStats* h_stats = nullptr;   // pinned, [kMaxProblems]
+  // problem table: host copies (to skip unchanged uploads) and device arrays
+  std::vector<ProbDesc> h_desc;
+  std::vector<int> h_bin_prob, h_e_prob, h_node_prob;
+  Table tb;
   int last_gn = 0;
   long long launches = 0;
   bool profile = false;
@@ -90,7 +94,7 @@ void free_pattern(Pattern& p) {
   dfree(p.seg_off); dfree(p.seg_cnt); dfree(p.pcg_row_begin);
   dfree(p.clu_row_begin); dfree(p.cta_of_row); dfree(p.ustart); dfree(p.low_ptr); dfree(p.low_pack);
   dfree(p.low_jl); dfree(p.g_vidx); dfree(p.g_halo_ptr); dfree(p.g_halo_col);
-  dfree(p.off_upper);
+  dfree(p.off_upper); dfree(p.pcg_cta_off); dfree(p.pcg_prob); dfree(p.prob_edge_off);
   p = Pattern();
 }
 
@@ -99,6 +103,13 @@ void free_work(Work& w) {
   dfree(w.c_srcfw); dfree(w.c_nres); dfree(w.cnt); dfree(w.node_total); dfree(w.inc_start);
   dfree(w.inc); dfree(w.trip); dfree(w.ekeys); dfree(w.rhs); dfree(w.plain); dfree(w.x); dfree(w.z); dfree(w.p0); dfree(w.p1);
   dfree(w.partials); dfree(w.barrier); dfree(w.err); dfree(w.e_data_part); dfree(w.e_arap_part); dfree(w.stats); dfree(w.timers);
+  dfree(w.nodes_cat); dfree(w.T_cat);
+  w.cnt_cap = 0;
+}
+
+void free_table(Table& t) {
+  dfree(t.desc); dfree(t.bin_prob); dfree(t.e_prob); dfree(t.node_prob);
+  t = Table();
 }
 
 cudaError_t alloc_work(Work& w, int max_nodes, int max_corrs, int bin_ctas_max) {
@@ -110,11 +121,11 @@ cudaError_t alloc_work(Work& w, int max_nodes, int max_corrs, int bin_ctas_max) 
 #define A_(ptr, n) if ((e = dalloc(&(ptr), (n))) != cudaSuccess) return e
   A_(w.pk_src, M); A_(w.pk_dst, M); A_(w.pk_nrm, M); A_(w.pk_ids, M); A_(w.pk_ws, M);
   A_(w.c_srcfw, M); A_(w.c_nres, M);
-  A_(w.cnt, (size_t)bin_ctas_max * N); A_(w.node_total, N); A_(w.inc_start, N + 1);
+  A_(w.node_total, N); A_(w.inc_start, N + 1);
   A_(w.inc, 4 * M); A_(w.trip, 16 * M); A_(w.ekeys, 4 * M);
   A_(w.rhs, 6 * N); A_(w.plain, N); A_(w.x, 6 * N); A_(w.z, 6 * N); A_(w.p0, 6 * N); A_(w.p1, 6 * N);
   A_(w.partials, (size_t)2 * 3 * kMaxPcgCtas); A_(w.barrier, (size_t)kMaxPcgCtas); A_(w.err, 1);
-  A_(w.e_data_part, (size_t)kEnergyCtas); A_(w.e_arap_part, N); A_(w.stats, 1);
+  A_(w.e_data_part, (size_t)(kEnergyCtas + kMaxProblems)); A_(w.e_arap_part, N); A_(w.stats, (size_t)kMaxProblems);
   A_(w.timers, (size_t)kTimerSlots);
 #undef A_
   return cudaSuccess;
@@ -159,8 +170,98 @@ void prof_collect(cf_gn* h) {
   h->prof_used = 0;
 }
 
-// Builds the pattern and every topology-derived array from host nodes.
-cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes, int N) {
+template <typename T>
+cudaError_t upload_if_changed(T* d, std::vector<T>& cache, const std::vector<T>& v, cudaStream_t s) {
+  if (v.size() == cache.size() && (v.empty() || memcmp(v.data(), cache.data(), v.size() * sizeof(T)) == 0))
+    return cudaSuccess;
+  cache = v;
+  // pageable source: the copy is staged before the call returns, so the
+  // cache may change afterwards
+  return v.empty() ? cudaSuccess : cudaMemcpyAsync(d, cache.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+// Lays out the sort and energy CTAs of the problems `in` (corrs, canon,
+// nodes, T, M, N and the clamps filled in by the caller) and uploads the
+// table when it changed.  single: one problem with the single-solve grid
+// sizes.
+cf_status prepare_table(cf_gn* h, std::vector<ProbDesc> in, bool single, cudaStream_t s) {
+  Work& w = h->w;
+  Table& t = h->tb;
+  const int P = (int)in.size();
+  if (P < 1 || P > kMaxProblems) return CF_ERR_CAPACITY;
+  long long Mt = 0, Nt = 0;
+  int maxN = 0;
+  for (auto& d : in) {
+    if (d.N > kMaxProblemNodes) return CF_ERR_CAPACITY;
+    Mt += d.M;
+    Nt += d.N;
+    maxN = std::max(maxN, d.N);
+  }
+  if (Nt > w.max_nodes || Mt > w.max_corrs) return CF_ERR_CAPACITY;
+  const int B = w.bin_ctas_max;
+  std::vector<int> bin_prob, e_prob;
+  long long cnt = 0;
+  int corr_off = 0, node_off = 0;
+  for (int p = 0; p < P; p++) {
+    ProbDesc& d = in[p];
+    d.corr_off = corr_off;
+    d.node_off = node_off;
+    int bc = 0, chunk = 0;
+    if (d.M > 0) {
+      bc = single ? std::min(B, std::max(1, cdiv(d.M, kThreads)))
+                  : std::min(cdiv(d.M, kThreads), std::max(1, (int)((double)B * d.M / (double)Mt + 0.5)));
+      chunk = cdiv(cdiv(d.M, bc), kThreads) * kThreads;
+      bc = cdiv(d.M, chunk);
+    }
+    d.bin_cta0 = (int)bin_prob.size();
+    d.bin_ctas = bc;
+    d.chunk = chunk;
+    d.cnt_off = cnt;
+    cnt += (long long)bc * d.N;
+    bin_prob.insert(bin_prob.end(), bc, p);
+    const int ec = single ? kEnergyCtas
+                          : std::max(1, (int)((double)kEnergyCtas * d.M / (double)std::max(1LL, Mt) + 0.5));
+    d.e_cta0 = (int)e_prob.size();
+    d.e_ctas = ec;
+    e_prob.insert(e_prob.end(), ec, p);
+    corr_off += d.M;
+    node_off += d.N;
+  }
+  if ((int)e_prob.size() > kEnergyCtas + kMaxProblems) return CF_ERR_CAPACITY;
+  if (cnt > w.cnt_cap) {
+    dfree(w.cnt);
+    w.cnt_cap = 0;
+    CF_TRY(dalloc(&w.cnt, (size_t)cnt));
+    w.cnt_cap = cnt;
+  }
+  if (!t.desc) {
+    CF_TRY(dalloc(&t.desc, (size_t)kMaxProblems));
+    CF_TRY(dalloc(&t.bin_prob, (size_t)(B + kMaxProblems)));
+    CF_TRY(dalloc(&t.e_prob, (size_t)(kEnergyCtas + kMaxProblems)));
+    CF_TRY(dalloc(&t.node_prob, (size_t)w.max_nodes));
+  }
+  std::vector<int> node_prob;
+  node_prob.reserve((size_t)Nt);
+  for (int p = 0; p < P; p++) node_prob.insert(node_prob.end(), in[p].N, p);
+  CF_TRY(upload_if_changed(t.desc, h->h_desc, in, s));
+  CF_TRY(upload_if_changed(t.bin_prob, h->h_bin_prob, bin_prob, s));
+  CF_TRY(upload_if_changed(t.e_prob, h->h_e_prob, e_prob, s));
+  CF_TRY(upload_if_changed(t.node_prob, h->h_node_prob, node_prob, s));
+  t.P = P;
+  t.n_bin = (int)bin_prob.size();
+  t.n_e = (int)e_prob.size();
+  t.M = (int)Mt;
+  t.N = (int)Nt;
+  t.max_N = maxN;
+  return CF_OK;
+}
+
+// Builds the pattern and every topology-derived array from host nodes (the
+// problems' nodes concatenated, neighbour ids global; problem p owns rows
+// [prob_off[p], prob_off[p+1])).
+cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes, const std::vector<int>& prob_off) {
+  const int N = (int)nodes.size();
+  const int P = (int)prob_off.size() - 1;
   // kernels/solver_kernels.cu:498-541: diagonal + directed edges both ways
   std::vector<std::vector<int>> rows(N);
   for (int i = 0; i < N; i++) rows[i].push_back(i);
@@ -231,30 +332,66 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
       ablk_edge[fb[upper_of_pos[find(i, j)]]++] = e;
     }
   }
-  // PCG partition: contiguous rows with balanced block counts; per CTA the
-  // distinct halo columns and, per block, its operand slot ([own | halo])
+  // PCG partition: each problem gets a group of CTAs (in proportion to its
+  // blocks, at least one), each CTA contiguous rows of its problem with
+  // balanced block counts; per CTA the distinct halo columns and, per block,
+  // its operand slot ([own | halo])
   const bool pipe = h->pcg_pipelined != 0;
   int G = h->pcg_ctas_override > 0 ? h->pcg_ctas_override : std::min(h->sms, std::max(1, N / 8));
-  G = std::max(1, std::min({G, N, kMaxPcgCtas}));
-  std::vector<int> rb2, g_vidx(std::max(1, nnzb)), g_halo_ptr, g_halo_col;
+  G = std::max(P, std::min({G, N, kMaxPcgCtas}));
+  if (P > kMaxPcgCtas) return CF_ERR_CAPACITY;
+  std::vector<int> rb2, g_vidx(std::max(1, nnzb)), g_halo_ptr, g_halo_col, cta_off2, cta_prob2;
   int smem = 0;
   bool a_smem = true;
   for (int attempt = 0; attempt < 64; attempt++) {
-    std::vector<int> rb(1, 0);
-    long long target = ((long long)nnzb + G - 1) / G;
-    int start = 0;
-    for (int c = 0; c < G && start < N; c++) {
-      int rem = G - c;
-      int end = start + 1;
-      if (rem == 1) {
-        end = N;
-      } else {
-        while (end < N - (rem - 1) && row_ptr[end] - row_ptr[start] < target) end++;
+    // CTAs per problem: one each, the rest by largest share of blocks
+    std::vector<int> gp(P, 1);
+    {
+      std::vector<std::pair<double, int>> rem;
+      int left = G - P;
+      for (int q = 0; q < P; q++) {
+        const double share = (double)(row_ptr[prob_off[q + 1]] - row_ptr[prob_off[q]]) / std::max(1, nnzb) * G;
+        int extra = std::min(std::max(0, (int)share - 1), prob_off[q + 1] - prob_off[q] - 1);
+        extra = std::min(extra, left);
+        gp[q] += extra;
+        left -= extra;
+        rem.push_back({share - gp[q], q});
       }
-      rb.push_back(end);
-      start = end;
+      std::sort(rem.begin(), rem.end(), [](const std::pair<double, int>& x, const std::pair<double, int>& y) {
+        return x.first != y.first ? x.first > y.first : x.second < y.second;
+      });
+      for (size_t k = 0; k < rem.size() && left > 0; k++) {
+        const int q = rem[k].second;
+        if (gp[q] < prob_off[q + 1] - prob_off[q]) {
+          gp[q]++;
+          left--;
+        }
+      }
     }
-    rb.back() = N;
+    std::vector<int> rb(1, 0), cta_off(1, 0), cta_prob;
+    for (int q = 0; q < P; q++) {
+      const int q0 = prob_off[q], q1 = prob_off[q + 1];
+      const long long target = ((long long)(row_ptr[q1] - row_ptr[q0]) + gp[q] - 1) / gp[q];
+      int start = q0;
+      for (int c = 0; c < gp[q] && start < q1; c++) {
+        const int rem = gp[q] - c;
+        int end = start + 1;
+        if (rem == 1) {
+          end = q1;
+        } else {
+          while (end < q1 - (rem - 1) && row_ptr[end] - row_ptr[start] < target) end++;
+        }
+        rb.push_back(end);
+        cta_prob.push_back(q);
+        start = end;
+      }
+      if (q1 == q0) {  // a problem without nodes still owns one (empty) CTA
+        rb.push_back(q0);
+        cta_prob.push_back(q);
+      }
+      rb.back() = q1;
+      cta_off.push_back((int)cta_prob.size());
+    }
     const int Gc = (int)rb.size() - 1;
     g_halo_ptr.assign(1, 0);
     g_halo_col.clear();
@@ -286,16 +423,23 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
       continue;
     }
     int cap = pcg_max_active_ctas(smem, a_smem, pipe);
-    if (cap <= 0) return CF_ERR_CAPACITY;
+    if (cap < P) return CF_ERR_CAPACITY;
     if (Gc > cap) {
       G = cap;
       continue;
     }
     rb2 = rb;
+    cta_off2 = cta_off;
+    cta_prob2 = cta_prob;
     break;
   }
   if (rb2.empty()) return CF_ERR_CAPACITY;
   G = (int)rb2.size() - 1;
+  std::vector<int> edge_off(P + 1, 0);
+  for (int q = 0, e = 0; q <= P; q++) {
+    while (q < P && e < n_edges && eijk[3 * e] < prob_off[q]) e++;
+    edge_off[q] = (q < P) ? e : n_edges;
+  }
 
   // single-cluster PCG plan: rows split over C CTAs by block count; the upper
   // blocks live in the owner's shared memory, lower blocks are read from the
@@ -318,7 +462,7 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
   int clu_C = 0, clu_smem = 0, clu_nup = 0, clu_nlow = 0, clu_rows = 0;
   std::vector<int> clu_rb, cta_of_row(N, 0), low_pack(std::max<size_t>(1, low_u.size())),
       low_jl(std::max<size_t>(1, low_u.size()));
-  if (h->pcg_mode != 1) {
+  if (h->pcg_mode != 1 && P == 1) {
     const int cands[2] = {16, 8};
     for (int ci = 0; ci < 2 && !clu_C; ci++) {
       const int C = cands[ci];
@@ -367,6 +511,7 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
 
   free_pattern(h->p);
   Pattern& p = h->p;
+  p.P = P;
   p.N = N;
   p.nnzb = nnzb;
   p.n_upper = n_upper;
@@ -393,6 +538,9 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
   CF_TRY(up(&p.arap_blk_edge, ablk_edge));
   CF_TRY(up(&p.edge_ijk, eijk));
   CF_TRY(up(&p.pcg_row_begin, rb2));
+  CF_TRY(up(&p.pcg_cta_off, cta_off2));
+  CF_TRY(up(&p.pcg_prob, cta_prob2));
+  CF_TRY(up(&p.prob_edge_off, edge_off));
   CF_TRY(up(&p.g_vidx, g_vidx));
   CF_TRY(up(&p.g_halo_ptr, g_halo_ptr));
   CF_TRY(up(&p.g_halo_col, g_halo_col));
@@ -424,35 +572,63 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
   }
   h->h_row_ptr = row_ptr;
   h->h_col_idx = col_idx;
-  h->pattern_N = N;
   h->pattern_valid = true;
   return CF_OK;
 }
 
+// The pattern of a single problem, rebuilt when N changes (the reference's
+// cache key, kernels/solver_kernels.cu:545-549) or after invalidation.
 cf_status ensure_pattern(cf_gn* h, const cf_deform_node* d_nodes, int N, cudaStream_t s) {
-  if (h->pattern_valid && h->pattern_N == N) return CF_OK;
+  const std::vector<int> key{N};
+  if (h->pattern_valid && h->pattern_key == key) return CF_OK;
   std::vector<cf_deform_node> hn(N);
   CF_TRY(cudaMemcpyAsync(hn.data(), d_nodes, sizeof(cf_deform_node) * (size_t)N, cudaMemcpyDeviceToHost, s));
   CF_TRY(cudaStreamSynchronize(s));
-  return build_pattern_host(h, hn, N);
+  cf_status st = build_pattern_host(h, hn, {0, N});
+  if (st == CF_OK) h->pattern_key = key;
+  return st;
+}
+
+// The block-diagonal pattern of a batch, rebuilt when the problem sizes
+// change or after invalidation.
+cf_status ensure_pattern_batch(cf_gn* h, const std::vector<ProbDesc>& pr, cudaStream_t s) {
+  std::vector<int> key{-(int)pr.size()};
+  for (auto& d : pr) key.push_back(d.N);
+  if (h->pattern_valid && h->pattern_key == key) return CF_OK;
+  std::vector<int> off(1, 0);
+  for (auto& d : pr) off.push_back(off.back() + d.N);
+  std::vector<cf_deform_node> hn(off.back());
+  for (size_t q = 0; q < pr.size(); q++)
+    CF_TRY(cudaMemcpyAsync(hn.data() + off[q], pr[q].nodes, sizeof(cf_deform_node) * (size_t)pr[q].N,
+                           cudaMemcpyDeviceToHost, s));
+  CF_TRY(cudaStreamSynchronize(s));
+  for (size_t q = 0; q < pr.size(); q++)
+    for (int i = off[q]; i < off[q + 1]; i++) {
+      cf_deform_node& nd = hn[i];
+      const int nn = std::min(std::max(nd.num_neighbors, 0), CF_K_GRAPH);
+      for (int k = 0; k < CF_K_GRAPH; k++) {
+        const int j = nd.neighbors[k];
+        nd.neighbors[k] = (k < nn && j >= 0 && j < pr[q].N) ? j + off[q] : -1;
+      }
+    }
+  cf_status st = build_pattern_host(h, hn, off);
+  if (st == CF_OK) h->pattern_key = key;
+  return st;
 }
 
 // Per-solve binning of correspondence incidences (counting sort by node,
 // then per-row grouping by block column).
-cf_status bin_correspondences(cf_gn* h, const cf_correspondence* corrs, const float* canon, int M, int N,
-                              cudaStream_t s) {
+cf_status bin_correspondences(cf_gn* h, cudaStream_t s) {
   Work& w = h->w;
-  if (M > 0) {
-    int bin_ctas = std::min(w.bin_ctas_max, std::max(1, cdiv(M, kThreads)));
-    int chunk = cdiv(cdiv(M, bin_ctas), kThreads) * kThreads;
-    bin_ctas = cdiv(M, chunk);
-    { Timed t(h, s, kProfPack, 1); CF_TRY(launch_pack_count(w, corrs, canon, M, N, bin_ctas, chunk, s)); }
-    { Timed t(h, s, kProfBinScan, 2); CF_TRY(launch_bin_scan(w, N, bin_ctas, s)); }
-    { Timed t(h, s, kProfScatter, 1); CF_TRY(launch_bin_scatter(w, M, N, bin_ctas, chunk, s)); }
+  const Table& t = h->tb;
+  if (t.n_bin > 0) {
+    { Timed tm(h, s, kProfPack, 1); CF_TRY(launch_pack_count(w, t, s)); }
+    { Timed tm(h, s, kProfBinScan, 2); CF_TRY(launch_bin_scan(w, t, s)); }
+    { Timed tm(h, s, kProfScatter, 1); CF_TRY(launch_bin_scatter(w, t, s)); }
   } else {
-    CF_TRY(cudaMemsetAsync(w.inc_start, 0, sizeof(int) * (size_t)(N + 1), s));
+    CF_TRY(cudaMemsetAsync(w.inc_start, 0, sizeof(int) * (size_t)(t.N + 1), s));
   }
-  { Timed t(h, s, kProfExpand, 1); CF_TRY(launch_expand(w, h->p, N, s)); }
+  { Timed tm(h, s, kProfExpand, 1); CF_TRY(launch_expand(w, h->p, t.N, s)); }
   return CF_OK;
 }
 
@@ -474,7 +650,75 @@ SolveArgs make_args(const cf_gn* h, const cf_deform_node* nodes, int N, int M) {
   a.arap_consistent = h->arap_consistent;
   a.spin_limit = 1u << 22;
   a.timers = h->phase_timers ? h->w.timers : nullptr;
+  a.tb = h->tb;
   return a;
+}
+
+ProbDesc make_desc(const cf_correspondence* corrs, const float* canon, const cf_deform_node* nodes,
+                   cf_dual_quat* T, int M, int N, float max_rot, float max_trans, float scale) {
+  ProbDesc d;
+  memset(&d, 0, sizeof(d));
+  d.corrs = corrs;
+  d.canon = canon;
+  d.nodes = nodes;
+  d.T = T;
+  d.M = M;
+  d.N = N;
+  d.max_rot = max_rot;
+  d.max_trans = max_trans;
+  d.update_scale = scale;
+  return d;
+}
+
+}  // namespace
+
+namespace {
+
+// G GN iterations and the final energy over the current table.
+cf_status run_gn(cf_gn* h, SolveArgs& a, cudaStream_t s) {
+  Work& w = h->w;
+  { Timed t(h, s, kProfNodePlain, 1); CF_TRY(launch_node_plain(w, a.nodes, a.transforms, a.N, s)); }
+  const int G = h->params.gn_iterations;
+  for (int g = 0; g < G; g++) {
+    { Timed t(h, s, kProfResidual, 1); CF_TRY(launch_residual(w, h->tb, true, s)); }
+    { Timed t(h, s, kProfAssemble, 1); CF_TRY(launch_assemble(w, h->p, a, a.transforms, s)); }
+    { Timed t(h, s, kProfPcg, 1); CF_TRY(launch_pcg_any(h, a, g, s)); }
+  }
+  { Timed t(h, s, kProfEnergy, 2); CF_TRY(launch_final_energy(w, h->p, a, G, s)); }
+  h->last_gn = G;
+  return CF_OK;
+}
+
+// Per-problem statistics (out[o] from table problem slot_of[o], -1: none)
+// and the error word; synchronises.
+cf_status read_stats(cf_gn* h, cf_solve_stats* stats, const std::vector<int>& slot_of, int n_out, cudaStream_t s) {
+  Work& w = h->w;
+  const int P = h->tb.P, G = h->params.gn_iterations;
+  CF_TRY(cudaMemcpyAsync(h->h_stats, w.stats, sizeof(DevStats) * (size_t)P, cudaMemcpyDeviceToHost, s));
+  int herr = 0;
+  CF_TRY(cudaMemcpyAsync(&herr, w.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CF_TRY(cudaStreamSynchronize(s));
+  for (int o = 0; o < n_out; o++) {
+    cf_solve_stats* out = stats + o;
+    memset(out, 0, sizeof(*out));
+    const int q = slot_of[o];
+    if (q < 0) continue;
+    const DevStats& d = h->h_stats[q];
+    out->energy_initial = d.energy[0];
+    out->energy_final = d.energy[G];
+    for (int g = 0; g <= G && g < CF_MAX_GN_ITERS; g++) out->energy_per_iter[g] = d.energy[g];
+    for (int g = 0; g < G; g++) {
+      out->pcg_iterations[g] = d.pcg_iters[g];
+      out->pcg_residual[g] = d.pcg_res[g];
+    }
+    out->gn_iterations_run = G;
+    out->num_blocks = h->p.nnzb;
+    out->precond_fallbacks = d.fallbacks;
+    out->error_flags = herr;
+  }
+  if (herr & kErrTimeoutBit) return CF_ERR_TIMEOUT;
+  if (herr & kErrNonFiniteBit) return CF_ERR_NON_FINITE;
+  return CF_OK;
 }
 
 }  // namespace
@@ -528,7 +772,7 @@ cf_status cf_gn_create(const cf_gn_params* params, int max_nodes, int max_corrs,
   h->device = dev;
   cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, dev);
   e = alloc_work(h->w, max_nodes, max_corrs, 2 * h->sms);
-  if (e == cudaSuccess) e = cudaMallocHost((void**)&h->h_stats, sizeof(DevStats));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&h->h_stats, sizeof(DevStats) * (size_t)kMaxProblems);
   if (e != cudaSuccess) {
     free_work(h->w);
     delete h;
@@ -543,6 +787,7 @@ cf_status cf_gn_destroy(cf_gn* h) {
   cudaDeviceSynchronize();
   free_pattern(h->p);
   free_work(h->w);
+  free_table(h->tb);
   if (h->h_stats) cudaFreeHost(h->h_stats);
   for (auto& pe : h->prof_pool) {
     cudaEventDestroy(pe.a);
@@ -608,14 +853,18 @@ cf_status cf_gn_linearize_solve(cf_gn* h, const cf_correspondence* d_corrs, int 
   cudaStream_t s = (cudaStream_t)stream;
   cf_status st = ensure_pattern(h, d_nodes, num_nodes, s);
   if (st != CF_OK) return st;
+  st = prepare_table(h, {make_desc(d_corrs, nullptr, d_nodes, const_cast<cf_dual_quat*>(d_transforms), num_corrs,
+                                   num_nodes, 0.f, 0.f, 1.f)},
+                     true, s);
+  if (st != CF_OK) return st;
   Work& w = h->w;
   CF_TRY(cudaMemsetAsync(w.stats, 0, sizeof(DevStats), s));
   CF_TRY(cudaMemsetAsync(w.err, 0, sizeof(int), s));
-  st = bin_correspondences(h, d_corrs, nullptr, num_corrs, num_nodes, s);
+  st = bin_correspondences(h, s);
   if (st != CF_OK) return st;
   SolveArgs a = make_args(h, d_nodes, num_nodes, num_corrs);
   a.delta_x = d_delta_x;
-  { Timed t(h, s, kProfResidual, 1); CF_TRY(launch_residual(w, num_corrs, num_nodes, false, s)); }
+  { Timed t(h, s, kProfResidual, 1); CF_TRY(launch_residual(w, h->tb, false, s)); }
   { Timed t(h, s, kProfAssemble, 1); CF_TRY(launch_assemble(w, h->p, a, d_transforms, s)); }
   { Timed t(h, s, kProfPcg, 1); CF_TRY(launch_pcg_any(h, a, 0, s)); }
   h->last_gn = 1;
@@ -635,45 +884,70 @@ cf_status cf_gn_solve(cf_gn* h, const cf_problem* prob, cf_dual_quat* d_transfor
   cudaStream_t s = (cudaStream_t)stream;
   cf_status st = ensure_pattern(h, prob->nodes, N, s);
   if (st != CF_OK) return st;
+  st = prepare_table(h, {make_desc(prob->corrs, prob->canon_points, prob->nodes, d_transforms, M, N, prob->max_rot,
+                                   prob->max_trans, prob->update_scale)},
+                     true, s);
+  if (st != CF_OK) return st;
   Work& w = h->w;
   CF_TRY(cudaMemsetAsync(w.stats, 0, sizeof(DevStats), s));
   CF_TRY(cudaMemsetAsync(w.err, 0, sizeof(int), s));
-  st = bin_correspondences(h, prob->corrs, prob->canon_points, M, N, s);
+  st = bin_correspondences(h, s);
   if (st != CF_OK) return st;
   SolveArgs a = make_args(h, prob->nodes, N, M);
   a.transforms = d_transforms;
   a.max_rot = prob->max_rot;
   a.max_trans = prob->max_trans;
   a.update_scale = prob->update_scale;
-  { Timed t(h, s, kProfNodePlain, 1); CF_TRY(launch_node_plain(w, prob->nodes, d_transforms, N, s)); }
-  const int G = h->params.gn_iterations;
-  for (int g = 0; g < G; g++) {
-    { Timed t(h, s, kProfResidual, 1); CF_TRY(launch_residual(w, M, N, true, s)); }
-    { Timed t(h, s, kProfAssemble, 1); CF_TRY(launch_assemble(w, h->p, a, d_transforms, s)); }
-    { Timed t(h, s, kProfPcg, 1); CF_TRY(launch_pcg_any(h, a, g, s)); }
+  st = run_gn(h, a, s);
+  if (st != CF_OK || !stats) return st;
+  return read_stats(h, stats, {0}, 1, s);
+}
+
+cf_status cf_gn_solve_batched(cf_gn* h, const cf_problem* problems, int num_problems,
+                              cf_dual_quat* const* d_transforms, cf_solve_stats* stats, void* stream) {
+  if (!h || num_problems < 0 || (num_problems > 0 && (!problems || !d_transforms))) return CF_ERR_INVALID_ARG;
+  if (num_problems > kMaxProblems) return CF_ERR_CAPACITY;
+  std::vector<ProbDesc> pr;
+  std::vector<int> slot_of(num_problems, -1);
+  long long Nt = 0, Mt = 0;
+  for (int q = 0; q < num_problems; q++) {
+    const cf_problem& p = problems[q];
+    if (p.num_nodes < 0 || p.num_corrs < 0) return CF_ERR_INVALID_ARG;
+    if (p.num_nodes == 0) continue;  // nothing to solve; its statistics stay zero
+    if (!p.nodes || !d_transforms[q] || (p.num_corrs > 0 && (!p.corrs || !p.canon_points))) return CF_ERR_INVALID_ARG;
+    if ((reinterpret_cast<uintptr_t>(p.corrs) & 3u) || (reinterpret_cast<uintptr_t>(d_transforms[q]) & 15u))
+      return CF_ERR_INVALID_ARG;
+    slot_of[q] = (int)pr.size();
+    pr.push_back(make_desc(p.corrs, p.canon_points, p.nodes, d_transforms[q], p.num_corrs, p.num_nodes, p.max_rot,
+                           p.max_trans, p.update_scale));
+    Nt += p.num_nodes;
+    Mt += p.num_corrs;
   }
-  { Timed t(h, s, kProfEnergy, 2); CF_TRY(launch_final_energy(w, h->p, a, G, s)); }
-  h->last_gn = G;
+  if (Nt > h->max_nodes || Mt > h->max_corrs) return CF_ERR_CAPACITY;
+  if (stats) memset(stats, 0, sizeof(*stats) * (size_t)num_problems);
+  if (pr.empty()) return CF_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  cf_status st = ensure_pattern_batch(h, pr, s);
+  if (st != CF_OK) return st;
+  st = prepare_table(h, pr, false, s);
+  if (st != CF_OK) return st;
+  Work& w = h->w;
+  if (!w.nodes_cat) {
+    CF_TRY(dalloc(&w.nodes_cat, (size_t)w.max_nodes));
+    CF_TRY(dalloc(&w.T_cat, (size_t)w.max_nodes));
+  }
+  CF_TRY(cudaMemsetAsync(w.stats, 0, sizeof(DevStats) * pr.size(), s));
+  CF_TRY(cudaMemsetAsync(w.err, 0, sizeof(int), s));
+  { Timed t(h, s, kProfOther, 1); CF_TRY(launch_batch_gather(w, h->tb, s)); }
+  st = bin_correspondences(h, s);
+  if (st != CF_OK) return st;
+  SolveArgs a = make_args(h, w.nodes_cat, (int)Nt, (int)Mt);
+  a.transforms = w.T_cat;
+  st = run_gn(h, a, s);
+  if (st != CF_OK) return st;
+  { Timed t(h, s, kProfOther, 1); CF_TRY(launch_batch_scatter(w, h->tb, s)); }
   if (!stats) return CF_OK;
-  CF_TRY(cudaMemcpyAsync(h->h_stats, w.stats, sizeof(DevStats), cudaMemcpyDeviceToHost, s));
-  int herr = 0;
-  CF_TRY(cudaMemcpyAsync(&herr, w.err, sizeof(int), cudaMemcpyDeviceToHost, s));
-  CF_TRY(cudaStreamSynchronize(s));
-  const DevStats& d = *h->h_stats;
-  stats->energy_initial = d.energy[0];
-  stats->energy_final = d.energy[G];
-  for (int g = 0; g <= G && g < CF_MAX_GN_ITERS; g++) stats->energy_per_iter[g] = d.energy[g];
-  for (int g = 0; g < G; g++) {
-    stats->pcg_iterations[g] = d.pcg_iters[g];
-    stats->pcg_residual[g] = d.pcg_res[g];
-  }
-  stats->gn_iterations_run = G;
-  stats->num_blocks = h->p.nnzb;
-  stats->precond_fallbacks = d.fallbacks;
-  stats->error_flags = herr;
-  if (herr & kErrTimeoutBit) return CF_ERR_TIMEOUT;
-  if (herr & kErrNonFiniteBit) return CF_ERR_NON_FINITE;
-  return CF_OK;
+  return read_stats(h, stats, slot_of, num_problems, s);
 }
 
 cf_status cf_gn_profile_enable(cf_gn* h, int on) {
@@ -735,7 +1009,7 @@ cf_status cf_gn_check(cf_gn* h, void* stream) {
 cf_status cf_gn_get_system(cf_gn* h, int* num_rows, int* num_blocks, int* h_row_ptr, int* h_col_idx,
                            float* h_values, float* h_rhs, void* stream) {
   if (!h) return CF_ERR_INVALID_ARG;
-  const int N = h->pattern_valid ? h->pattern_N : 0;
+  const int N = h->pattern_valid ? h->p.N : 0;
   const int nnzb = h->pattern_valid ? h->p.nnzb : 0;
   if (num_rows) *num_rows = N;
   if (num_blocks) *num_blocks = nnzb;

@@ -23,9 +23,43 @@ struct DevStats {
   int pad_;
 };
 
+// One problem of a solve as the kernels see it; a single solve is a batch of
+// one.  Correspondences and nodes of all problems live in one concatenated
+// index space (node ids inside the packed records are global).
+struct ProbDesc {
+  const cf_correspondence* corrs;  // the caller's rows, indexed locally
+  const float* canon;              // canonical points (nullptr: linearise at src)
+  const cf_deform_node* nodes;     // the caller's nodes (batched solves gather them)
+  cf_dual_quat* T;                 // the caller's transforms (batched solves gather/scatter)
+  long long cnt_off;               // first histogram word of this problem in Work::cnt
+  int M, N;
+  int corr_off, node_off;          // first correspondence / node in the concatenated space
+  int bin_cta0, bin_ctas, chunk;   // sort CTAs of this problem, correspondences per CTA
+  int e_cta0, e_ctas;              // residual / energy CTAs, one FP64 partial each
+  float max_rot, max_trans, update_scale;
+  int pad_[2];
+};
+static_assert(sizeof(ProbDesc) == 96, "ProbDesc has no padding (compared bytewise)");
+
+// Per-call problem table (device copies of the host arrays).
+struct Table {
+  int P = 0;
+  int n_bin = 0, n_e = 0;    // total sort / energy CTAs
+  int M = 0, N = 0;          // concatenated sizes
+  int max_N = 0;             // largest problem (shared-memory histograms)
+  ProbDesc* desc = nullptr;  // [P]
+  int* bin_prob = nullptr;   // [n_bin] problem of each sort CTA
+  int* e_prob = nullptr;     // [n_e] problem of each energy CTA
+  int* node_prob = nullptr;  // [N] problem of each node
+};
+
 // Block pattern and everything derived from the graph topology.  Built on
 // the host (cold path, kernels/solver_kernels.cu:498-541) and uploaded.
 struct Pattern {
+  int P = 1;               // problems (block-diagonal union for batched solves)
+  int* prob_edge_off = nullptr;  // [P+1] ARAP edges of each problem (edge_ijk order)
+  int* pcg_cta_off = nullptr;    // [P+1] PCG CTA group of each problem
+  int* pcg_prob = nullptr;       // [pcg_ctas] problem of each PCG CTA
   int N = 0;
   int nnzb = 0;
   int n_upper = 0;      // blocks with col >= row (incl. diagonal)
@@ -82,7 +116,8 @@ struct Work {
   float4* pk_ws = nullptr;
   float4* c_srcfw = nullptr;  // skinned src, fw (0 = skipped)
   float4* c_nres = nullptr;   // normal, residual
-  int* cnt = nullptr;         // [bin_ctas_max * max_nodes]
+  int* cnt = nullptr;         // per sort CTA, a histogram over its problem's nodes
+  long long cnt_cap = 0;      // words allocated for cnt
   int* node_total = nullptr;  // [max_nodes]
   int* inc_start = nullptr;   // [max_nodes+1]
   int* inc = nullptr;         // [4*max_corrs]: (c << 2) | a
@@ -95,16 +130,21 @@ struct Work {
   float* p0 = nullptr;
   float* p1 = nullptr;
   double* partials = nullptr;  // [2 bufs][3 slots][max pcg ctas]
-  unsigned* barrier = nullptr;  // [max pcg ctas] generation flags of the grid barrier
+  unsigned* barrier = nullptr;  // [max pcg ctas] one arrival counter per PCG CTA group
   int* err = nullptr;
-  double* e_data_part = nullptr;  // [kEnergyCtas]
-  double* e_arap_part = nullptr;  // [max_nodes] (per row / per energy CTA)
-  DevStats* stats = nullptr;
+  double* e_data_part = nullptr;  // [kEnergyCtas + kMaxProblems] one partial per energy CTA
+  double* e_arap_part = nullptr;  // [max_nodes] per row
+  DevStats* stats = nullptr;      // [kMaxProblems]
+  // batched solves: the problems' nodes and transforms, concatenated
+  cf_deform_node* nodes_cat = nullptr;  // [max_nodes]
+  cf_dual_quat* T_cat = nullptr;        // [max_nodes]
   long long* timers = nullptr;  // [kTimerSlots] phase cycles of the grid PCG (debug)
 };
 
-constexpr int kEnergyCtas = 592;  // fixed grid of the residual/energy kernels
+constexpr int kEnergyCtas = 592;  // residual/energy CTAs of a single solve
 constexpr int kMaxPcgCtas = 1024;
+constexpr int kMaxProblems = 1024;       // problems per batched solve
+constexpr int kMaxProblemNodes = 48000;  // nodes per problem (per-CTA histograms in shared memory)
 
 struct SolveArgs {
   const cf_deform_node* nodes;
@@ -121,18 +161,20 @@ struct SolveArgs {
   float max_rot, max_trans, update_scale;
   unsigned spin_limit;
   long long* timers;  // non-null: CTA 0 of the grid PCG accumulates phase cycles here
+  Table tb;           // the problems of this solve
 };
 constexpr int kTimerSlots = 12;
 
 // ---- launchers (cf_kernels.cu) ----
-cudaError_t launch_pack_count(const Work& w, const cf_correspondence* corrs, const float* canon, int M, int N,
-                              int bin_ctas, int chunk, cudaStream_t s);
-cudaError_t launch_bin_scan(const Work& w, int N, int bin_ctas, cudaStream_t s);
-cudaError_t launch_bin_scatter(const Work& w, int M, int N, int bin_ctas, int chunk, cudaStream_t s);
+cudaError_t launch_pack_count(const Work& w, const Table& tb, cudaStream_t s);
+cudaError_t launch_bin_scan(const Work& w, const Table& tb, cudaStream_t s);
+cudaError_t launch_bin_scatter(const Work& w, const Table& tb, cudaStream_t s);
 cudaError_t launch_expand(const Work& w, const Pattern& p, int N, cudaStream_t s);
 cudaError_t launch_node_plain(const Work& w, const cf_deform_node* nodes, const cf_dual_quat* T, int N,
                               cudaStream_t s);
-cudaError_t launch_residual(const Work& w, int M, int N, bool skin, cudaStream_t s);
+cudaError_t launch_residual(const Work& w, const Table& tb, bool skin, cudaStream_t s);
+cudaError_t launch_batch_gather(const Work& w, const Table& tb, cudaStream_t s);
+cudaError_t launch_batch_scatter(const Work& w, const Table& tb, cudaStream_t s);
 cudaError_t launch_assemble(const Work& w, const Pattern& p, const SolveArgs& a, const cf_dual_quat* T,
                             cudaStream_t s);
 cudaError_t launch_pcg(const Work& w, const Pattern& p, const SolveArgs& a, int gn_slot, cudaStream_t s);

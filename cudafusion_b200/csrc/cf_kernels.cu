@@ -5,12 +5,15 @@
 //   bin_scan_*    deterministic exclusive offsets (node, CTA)
 //   bin_scatter   stable counting sort of incidences (c, slot) by node
 //   expand        (cf_assemble.cu) per block row: incidences -> (c, a, b)
-//                 entries grouped by upper block column, cut into chunks
+//                 entries grouped by upper block column
 // Per GN iteration:
 //   node_plain    node-centred DQ -> plain DQ (once per node, not per point)
 //   residual      DQ skinning + point-to-plane residual + Huber weight
-//   assemble      (cf_assemble.cu) one warp per chunk of a block's entries,
-//                 Kahan-compensated diagonal blocks, ARAP, damping.
+//   assemble      (cf_assemble.cu) a CTA per diagonal block (Kahan), a warp
+//                 per off-diagonal block, ARAP, damping, rhs.
+// Every kernel works on a table of problems (ProbDesc): a single solve is a
+// batch of one; a batched solve concatenates its problems' correspondences
+// and nodes, and each sort / energy CTA belongs to exactly one problem.
 // The PCG kernels live in cf_pcg_grid.cu (grid-wide cooperative) and
 // cf_pcg_cluster.cu (one thread-block cluster).
 // The reference (CUDAFusion kernels/solver_kernels.cu) assembles with float
@@ -47,16 +50,18 @@ __device__ __forceinline__ double block_sum_d(double v, double* red) {
 // ----------------------------------------------------------------------------
 // pack + count
 // ----------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) pack_count_kernel(const cf_correspondence* __restrict__ corrs,
-                                                              const float* __restrict__ canon, int M, int N,
-                                                              int chunk, Work w) {
+__global__ void __launch_bounds__(kThreads) pack_count_kernel(Table tb, Work w) {
   extern __shared__ int hist[];
   __shared__ __align__(16) uint32_t stage[kThreads * kWords];
   const int tid = threadIdx.x;
+  const ProbDesc d = tb.desc[tb.bin_prob[blockIdx.x]];
+  const int N = d.N, lc = blockIdx.x - d.bin_cta0;
   for (int i = tid; i < N; i += kThreads) hist[i] = 0;
+  const cf_correspondence* corrs = d.corrs;
+  const float* canon = d.canon;
   const bool al16 = ((reinterpret_cast<uintptr_t>(corrs) & 15u) == 0);
-  const int cb = blockIdx.x * chunk;
-  const int ce = min(M, cb + chunk);
+  const int cb = lc * d.chunk;
+  const int ce = min(d.M, cb + d.chunk);
   __syncthreads();
   for (int t0 = cb; t0 < ce; t0 += kThreads) {
     const int n = min(kThreads, ce - t0);
@@ -72,17 +77,26 @@ __global__ void __launch_bounds__(kThreads) pack_count_kernel(const cf_correspon
     __syncthreads();
     if (tid < n) {
       const uint32_t* rec = stage + tid * kWords;
-      const int c = t0 + tid;
+      const int cl = t0 + tid;           // row of the caller's array
+      const int c = d.corr_off + cl;     // concatenated index
       float3 p;
       if (canon) {
-        p = f3(__ldg(canon + 3 * (size_t)c), __ldg(canon + 3 * (size_t)c + 1), __ldg(canon + 3 * (size_t)c + 2));
+        p = f3(__ldg(canon + 3 * (size_t)cl), __ldg(canon + 3 * (size_t)cl + 1), __ldg(canon + 3 * (size_t)cl + 2));
       } else {
         p = f3(__uint_as_float(rec[0]), __uint_as_float(rec[1]), __uint_as_float(rec[2]));
       }
       const bool valid = (rec[18] & 0xffu) != 0;
       const float weight = __uint_as_float(rec[17]);
       const float we = valid ? weight : 0.f;  // <= 0 or NaN: never contributes
-      int4 ids = make_int4((int)rec[9], (int)rec[10], (int)rec[11], (int)rec[12]);
+      int lid[kK];
+#pragma unroll
+      for (int k = 0; k < kK; k++) lid[k] = (int)rec[9 + k];
+      // node ids become global; an id outside [0, N) is no node (-1)
+      int4 ids;
+      ids.x = (lid[0] >= 0 && lid[0] < N) ? lid[0] + d.node_off : -1;
+      ids.y = (lid[1] >= 0 && lid[1] < N) ? lid[1] + d.node_off : -1;
+      ids.z = (lid[2] >= 0 && lid[2] < N) ? lid[2] + d.node_off : -1;
+      ids.w = (lid[3] >= 0 && lid[3] < N) ? lid[3] + d.node_off : -1;
       float4 ws = make_float4(__uint_as_float(rec[13]), __uint_as_float(rec[14]), __uint_as_float(rec[15]),
                               __uint_as_float(rec[16]));
       w.pk_src[c] = make_float4(p.x, p.y, p.z, we);
@@ -93,26 +107,26 @@ __global__ void __launch_bounds__(kThreads) pack_count_kernel(const cf_correspon
       if (we > 0.f) {
 #pragma unroll
         for (int k = 0; k < kK; k++) {
-          int id = sel4i(ids, k);
-          float wk = sel4(ws, k);
-          if (id >= 0 && id < N && wk > 1e-8f) atomicAdd(&hist[id], 1);
+          if (lid[k] >= 0 && lid[k] < N && sel4(ws, k) > 1e-8f) atomicAdd(&hist[lid[k]], 1);
         }
       }
     }
     __syncthreads();
   }
-  int* out = w.cnt + (size_t)blockIdx.x * N;
+  int* out = w.cnt + d.cnt_off + (size_t)lc * N;
   for (int i = tid; i < N; i += kThreads) out[i] = hist[i];
 }
 
-// cnt[k][n] -> exclusive prefix over k (in place); node_total[n] = sum.
-__global__ void bin_scan_nodes_kernel(Work w, int N, int bin_ctas) {
-  int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N) return;
+// Per node: exclusive prefix of its counts over its problem's sort CTAs (in
+// place); node_total[n] = sum.
+__global__ void bin_scan_nodes_kernel(Table tb, Work w) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= tb.N) return;
+  const ProbDesc d = tb.desc[tb.node_prob[n]];
+  int* p = w.cnt + d.cnt_off + (n - d.node_off);
   int run = 0;
-  for (int k = 0; k < bin_ctas; k++) {
-    int* p = w.cnt + (size_t)k * N + n;
-    int v = *p;
+  for (int k = 0; k < d.bin_ctas; k++, p += d.N) {
+    const int v = *p;
     *p = run;
     run += v;
   }
@@ -156,16 +170,18 @@ __global__ void __launch_bounds__(1024) bin_scan_total_kernel(Work w, int N) {
 }
 
 // Stable scatter of incidences: order within a node = (tile, slot, corr).
-__global__ void __launch_bounds__(kThreads) bin_scatter_kernel(Work w, int M, int N, int chunk) {
+__global__ void __launch_bounds__(kThreads) bin_scatter_kernel(Table tb, Work w) {
   extern __shared__ int cursor[];
   __shared__ int wkey[kThreads / 32][32];
   __shared__ int wcnt[kThreads / 32][32];
   __shared__ int wlen[kThreads / 32];
   const int tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
-  const int* base = w.cnt + (size_t)blockIdx.x * N;
-  for (int i = tid; i < N; i += kThreads) cursor[i] = w.inc_start[i] + base[i];
-  const int cb = blockIdx.x * chunk;
-  const int ce = min(M, cb + chunk);
+  const ProbDesc d = tb.desc[tb.bin_prob[blockIdx.x]];
+  const int N = d.N, lc = blockIdx.x - d.bin_cta0;
+  const int* base = w.cnt + d.cnt_off + (size_t)lc * N;
+  for (int i = tid; i < N; i += kThreads) cursor[i] = w.inc_start[d.node_off + i] + base[i];
+  const int cb = d.corr_off + lc * d.chunk;
+  const int ce = d.corr_off + min(d.M, lc * d.chunk + d.chunk);
   __syncthreads();
   for (int t0 = cb; t0 < ce; t0 += kThreads) {
     const int c = t0 + tid;
@@ -180,9 +196,10 @@ __global__ void __launch_bounds__(kThreads) bin_scatter_kernel(Work w, int M, in
     }
 #pragma unroll 1
     for (int a = 0; a < kK; a++) {
-      int id = sel4i(ids, a);
-      float wa = sel4(ws, a);
-      int key = (live && we > 0.f && id >= 0 && id < N && wa > 1e-8f) ? id : -1;
+      const int id = sel4i(ids, a);
+      const float wa = sel4(ws, a);
+      // local node of this problem (packed ids are global or -1)
+      const int key = (live && we > 0.f && id >= 0 && wa > 1e-8f) ? id - d.node_off : -1;
       unsigned peers = __match_any_sync(0xffffffffu, key);
       int rank = __popc(peers & lanemask_lt());
       bool leader = (__ffs(peers) - 1) == lane;
@@ -227,19 +244,32 @@ __global__ void node_plain_kernel(const cf_deform_node* __restrict__ nodes, cons
   store_dq(plain + i, dq_centered(load_dq_cg(T + i), node_pos(nodes, i)));
 }
 
+// Correspondences [c0, c1) of energy CTA blockIdx.x (a contiguous share of
+// its problem's rows).
+__device__ __forceinline__ void e_range(const Table& tb, const ProbDesc& d, int& c0, int& c1) {
+  const int lc = blockIdx.x - d.e_cta0;
+  const int per = (d.M + d.e_ctas - 1) / d.e_ctas;
+  c0 = d.corr_off + min(d.M, lc * per);
+  c1 = d.corr_off + min(d.M, lc * per + per);
+}
+
 template <bool SKIN>
-__global__ void __launch_bounds__(kThreads) residual_kernel(Work w, int M, int N) {
+__global__ void __launch_bounds__(kThreads) residual_kernel(Table tb, Work w) {
   __shared__ double red[32];
+  const ProbDesc d = tb.desc[tb.e_prob[blockIdx.x]];
+  int c0, c1;
+  e_range(tb, d, c0, c1);
+  const int N = tb.N;
   double e = 0.0;
-  for (int c = blockIdx.x * kThreads + threadIdx.x; c < M; c += gridDim.x * kThreads) {
+  for (int c = c0 + threadIdx.x; c < c1; c += kThreads) {
     float4 s = w.pk_src[c];
     if (!(s.w > 0.f)) continue;
     float3 src = f3(s.x, s.y, s.z);
     if (SKIN) src = blend_warp(src, w.pk_ids[c], w.pk_ws[c], w.plain, N);
-    float4 d = w.pk_dst[c];
+    float4 dd = w.pk_dst[c];
     float4 n = w.pk_nrm[c];
     // kernels/solver_kernels.cu:76-85
-    float res = n.x * (src.x - d.x) + n.y * (src.y - d.y) + n.z * (src.z - d.z);
+    float res = n.x * (src.x - dd.x) + n.y * (src.y - dd.y) + n.z * (src.z - dd.z);
     float fw = fmaxf(s.w, 0.f) * huber_w(res, 0.2f);
     if (!(fw > 1e-8f)) {
       fw = 0.f;
@@ -254,22 +284,30 @@ __global__ void __launch_bounds__(kThreads) residual_kernel(Work w, int M, int N
 }
 
 // Energy at the current transforms (after the last update): data term with
-// the final skinning, plus the ARAP edges; fixed grid, per-CTA partials.
-__global__ void __launch_bounds__(kThreads) energy_kernel(Work w, Pattern pt, const cf_deform_node* nodes,
-                                                          const cf_dual_quat* T, int M, int N, float lambda) {
+// the final skinning, plus the problem's ARAP edges; per-CTA partials.
+__global__ void __launch_bounds__(kThreads) energy_kernel(Table tb, Work w, Pattern pt, const cf_deform_node* nodes,
+                                                          const cf_dual_quat* T, float lambda) {
   __shared__ double red[32];
+  const int prob = tb.e_prob[blockIdx.x];
+  const ProbDesc d = tb.desc[prob];
+  int c0, c1;
+  e_range(tb, d, c0, c1);
+  const int N = tb.N;
   double e = 0.0;
-  for (int c = blockIdx.x * kThreads + threadIdx.x; c < M; c += gridDim.x * kThreads) {
+  for (int c = c0 + threadIdx.x; c < c1; c += kThreads) {
     float4 s = w.pk_src[c];
     if (!(s.w > 0.f)) continue;
     float3 src = blend_warp(f3(s.x, s.y, s.z), w.pk_ids[c], w.pk_ws[c], w.plain, N);
-    float4 d = w.pk_dst[c];
+    float4 dd = w.pk_dst[c];
     float4 n = w.pk_nrm[c];
-    float res = n.x * (src.x - d.x) + n.y * (src.y - d.y) + n.z * (src.z - d.z);
+    float res = n.x * (src.x - dd.x) + n.y * (src.y - dd.y) + n.z * (src.z - dd.z);
     float fw = fmaxf(s.w, 0.f) * huber_w(res, 0.2f);
     if (fw > 1e-8f) e += (double)fw * (double)res * (double)res;
   }
-  for (int ed = blockIdx.x * kThreads + threadIdx.x; ed < pt.n_edges; ed += gridDim.x * kThreads) {
+  const int e0 = pt.prob_edge_off[prob], ne = pt.prob_edge_off[prob + 1] - e0;
+  const int lc = blockIdx.x - d.e_cta0, per = (ne + d.e_ctas - 1) / d.e_ctas;
+  const int ea = e0 + min(ne, lc * per), eb = e0 + min(ne, lc * per + per);
+  for (int ed = ea + threadIdx.x; ed < eb; ed += kThreads) {
     Edge ev = eval_edge(nodes, T, pt.edge_ijk[3 * ed], pt.edge_ijk[3 * ed + 1], pt.edge_ijk[3 * ed + 2], lambda);
     if (ev.el > 0.f)
       e += (double)ev.el * ((double)ev.r.x * ev.r.x + (double)ev.r.y * ev.r.y + (double)ev.r.z * ev.r.z);
@@ -278,14 +316,41 @@ __global__ void __launch_bounds__(kThreads) energy_kernel(Work w, Pattern pt, co
   if (threadIdx.x == 0) w.e_data_part[blockIdx.x] = t;
 }
 
-__global__ void energy_reduce_kernel(Work w, int slot) {
+// One warp per problem: its energy = the sum of its CTAs' partials.
+__global__ void energy_reduce_kernel(Table tb, Work w, int slot) {
+  const ProbDesc d = tb.desc[blockIdx.x];
   double v = 0.0;
-  for (int k = threadIdx.x; k < kEnergyCtas; k += 32) v += w.e_data_part[k];
+  for (int k = threadIdx.x; k < d.e_ctas; k += 32) v += w.e_data_part[d.e_cta0 + k];
   v = warp_sum_d(v);
   if (threadIdx.x == 0) {
-    w.stats->energy[slot] = v;
+    w.stats[blockIdx.x].energy[slot] = v;
     if (!isfinite(v)) atomicOr(w.err, kErrNonFinite);
   }
+}
+
+// Batched solves: each problem's nodes (neighbour ids made global) and
+// transforms into the concatenated arrays.
+__global__ void batch_gather_kernel(Table tb, Work w) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= tb.N) return;
+  const ProbDesc d = tb.desc[tb.node_prob[n]];
+  const int l = n - d.node_off;
+  cf_deform_node nd = d.nodes[l];
+  const int nn = min(max(nd.num_neighbors, 0), CF_K_GRAPH);
+#pragma unroll
+  for (int k = 0; k < CF_K_GRAPH; k++) {
+    const int j = nd.neighbors[k];
+    nd.neighbors[k] = (k < nn && j >= 0 && j < d.N) ? j + d.node_off : -1;
+  }
+  w.nodes_cat[n] = nd;
+  store_dq(w.T_cat + n, load_dq_cg(d.T + l));
+}
+
+__global__ void batch_scatter_kernel(Table tb, Work w) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= tb.N) return;
+  const ProbDesc d = tb.desc[tb.node_prob[n]];
+  store_dq(d.T + (n - d.node_off), load_dq_cg(w.T_cat + n));
 }
 
 // WarpField::apply_twist_increment (src/warp_field.cu:250-291).
@@ -340,29 +405,28 @@ inline int cdiv(int a, int b) { return (a + b - 1) / b; }
 // ----------------------------------------------------------------------------
 // launchers
 // ----------------------------------------------------------------------------
-cudaError_t launch_pack_count(const Work& w, const cf_correspondence* corrs, const float* canon, int M, int N,
-                              int bin_ctas, int chunk, cudaStream_t s) {
-  if (M <= 0) return cudaSuccess;
-  size_t smem = (size_t)N * sizeof(int);
-  cudaError_t e = cudaFuncSetAttribute(pack_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+cudaError_t launch_pack_count(const Work& w, const Table& tb, cudaStream_t s) {
+  if (tb.n_bin <= 0) return cudaSuccess;
+  const int smem = tb.max_N * (int)sizeof(int);
+  cudaError_t e = cudaFuncSetAttribute(pack_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  pack_count_kernel<<<bin_ctas, kThreads, smem, s>>>(corrs, canon, M, N, chunk, w);
+  pack_count_kernel<<<tb.n_bin, kThreads, smem, s>>>(tb, w);
   return cudaGetLastError();
 }
 
-cudaError_t launch_bin_scan(const Work& w, int N, int bin_ctas, cudaStream_t s) {
-  if (N <= 0) return cudaSuccess;
-  bin_scan_nodes_kernel<<<cdiv(N, 128), 128, 0, s>>>(w, N, bin_ctas);
-  bin_scan_total_kernel<<<1, 1024, 0, s>>>(w, N);
+cudaError_t launch_bin_scan(const Work& w, const Table& tb, cudaStream_t s) {
+  if (tb.N <= 0) return cudaSuccess;
+  bin_scan_nodes_kernel<<<cdiv(tb.N, 128), 128, 0, s>>>(tb, w);
+  bin_scan_total_kernel<<<1, 1024, 0, s>>>(w, tb.N);
   return cudaGetLastError();
 }
 
-cudaError_t launch_bin_scatter(const Work& w, int M, int N, int bin_ctas, int chunk, cudaStream_t s) {
-  if (M <= 0) return cudaSuccess;
-  size_t smem = (size_t)N * sizeof(int);
-  cudaError_t e = cudaFuncSetAttribute(bin_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+cudaError_t launch_bin_scatter(const Work& w, const Table& tb, cudaStream_t s) {
+  if (tb.n_bin <= 0) return cudaSuccess;
+  const int smem = tb.max_N * (int)sizeof(int);
+  cudaError_t e = cudaFuncSetAttribute(bin_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  bin_scatter_kernel<<<bin_ctas, kThreads, smem, s>>>(w, M, N, chunk);
+  bin_scatter_kernel<<<tb.n_bin, kThreads, smem, s>>>(tb, w);
   return cudaGetLastError();
 }
 
@@ -373,17 +437,31 @@ cudaError_t launch_node_plain(const Work& w, const cf_deform_node* nodes, const 
   return cudaGetLastError();
 }
 
-cudaError_t launch_residual(const Work& w, int M, int N, bool skin, cudaStream_t s) {
+cudaError_t launch_residual(const Work& w, const Table& tb, bool skin, cudaStream_t s) {
+  if (tb.n_e <= 0) return cudaSuccess;
   if (skin)
-    residual_kernel<true><<<kEnergyCtas, kThreads, 0, s>>>(w, M, N);
+    residual_kernel<true><<<tb.n_e, kThreads, 0, s>>>(tb, w);
   else
-    residual_kernel<false><<<kEnergyCtas, kThreads, 0, s>>>(w, M, N);
+    residual_kernel<false><<<tb.n_e, kThreads, 0, s>>>(tb, w);
   return cudaGetLastError();
 }
 
 cudaError_t launch_final_energy(const Work& w, const Pattern& p, const SolveArgs& a, int slot, cudaStream_t s) {
-  energy_kernel<<<kEnergyCtas, kThreads, 0, s>>>(w, p, a.nodes, a.transforms, a.M, a.N, a.lambda_smooth);
-  energy_reduce_kernel<<<1, 32, 0, s>>>(w, slot);
+  if (a.tb.n_e <= 0) return cudaSuccess;
+  energy_kernel<<<a.tb.n_e, kThreads, 0, s>>>(a.tb, w, p, a.nodes, a.transforms, a.lambda_smooth);
+  energy_reduce_kernel<<<a.tb.P, 32, 0, s>>>(a.tb, w, slot);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_gather(const Work& w, const Table& tb, cudaStream_t s) {
+  if (tb.N <= 0) return cudaSuccess;
+  batch_gather_kernel<<<cdiv(tb.N, 128), 128, 0, s>>>(tb, w);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_scatter(const Work& w, const Table& tb, cudaStream_t s) {
+  if (tb.N <= 0) return cudaSuccess;
+  batch_scatter_kernel<<<cdiv(tb.N, 128), 128, 0, s>>>(tb, w);
   return cudaGetLastError();
 }
 

@@ -179,7 +179,8 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_cluster_kernel(CluArgs P) {
   }
   if (crank == 0 && tid >= 32 && tid < 64) {  // energy of this linearisation point
     double v = 0.0;
-    for (int k = tid - 32; k < kEnergyCtas; k += 32) v += w.e_data_part[k];
+    const int ne = a.tb.desc[0].e_ctas;  // the cluster path serves single solves
+    for (int k = tid - 32; k < ne; k += 32) v += w.e_data_part[k];
     for (int k = tid - 32; k < a.N; k += 32) v += w.e_arap_part[k];
     v = warp_sum_d(v);
     if (tid == 32) {

@@ -117,11 +117,11 @@ __device__ __forceinline__ void gbar(unsigned* ctr, unsigned gen, int G, int cta
   __syncthreads();
 }
 
-// A warp sums NS consecutive slots of the partials (stride G) in one pass:
-// all loads first, fixed order per lane, xor butterfly, so every CTA gets
-// the same bits; results to red[dst..dst+NS).
+// A warp sums NS slots of the G partials of a CTA group (slot stride
+// `stride`) in one pass: all loads first, fixed order per lane, xor
+// butterfly, so every CTA gets the same bits; results to red[dst..dst+NS).
 template <int NS>
-__device__ __forceinline__ void wsum_parts(const double* parts, int G, double* red, int dst) {
+__device__ __forceinline__ void wsum_parts(const double* parts, int G, int stride, double* red, int dst) {
   const int lane = threadIdx.x & 31;
   double v[NS];
 #pragma unroll
@@ -129,7 +129,7 @@ __device__ __forceinline__ void wsum_parts(const double* parts, int G, double* r
   for (int k = lane; k < G; k += 32) {
     double x[NS];
 #pragma unroll
-    for (int s = 0; s < NS; s++) x[s] = __ldcg(parts + s * G + k);
+    for (int s = 0; s < NS; s++) x[s] = __ldcg(parts + s * stride + k);
 #pragma unroll
     for (int s = 0; s < NS; s++) v[s] += x[s];
   }
@@ -172,7 +172,13 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
   const Pattern& pt = P.pt;
   const SolveArgs& a = P.a;
   const int tid = threadIdx.x;
-  const int cta = blockIdx.x, G = gridDim.x;
+  // CTA groups: each problem of the table has its own CTAs, barrier and partials
+  const int cta = blockIdx.x, GT = gridDim.x;
+  const int prob = pt.pcg_prob[cta];
+  const int gb = pt.pcg_cta_off[prob], G = pt.pcg_cta_off[prob + 1] - gb, gcta = cta - gb;
+  const ProbDesc pd = a.tb.desc[prob];
+  DevStats* st = w.stats + prob;
+  unsigned* bar = w.barrier + prob;
   const int r0 = pt.pcg_row_begin[cta], r1 = pt.pcg_row_begin[cta + 1];
   const int nrows = r1 - r0;
   const int b0 = pt.row_ptr[r0], b1 = pt.row_ptr[r1];
@@ -189,9 +195,10 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
   const float* gA = pt.values + (size_t)b0 * 36;
   const int n6 = nrows * 6, h6 = nhalo * 6;
   int* err = w.err;
-  double* part = w.partials;  // [2 bufs][3 slots][G]
+  double* part = w.partials;  // [2 bufs][3 slots][GT], this group's at [gb, gb + G)
   unsigned gen = 0;
   PhaseClock clk((a.timers && cta == 0 && tid == 0) ? a.timers : nullptr);
+  (void)gcta;
 
   // ---- prologue: A rows, indices, halo list, FP64 block inverses ----
   if (A_SMEM) {
@@ -214,15 +221,15 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
       const float* blk = A_SMEM ? (sA + dl * 36) : (gA + dl * 36);
       nfb += inv6_group(blk, scr, sMinv + (act ? i : 0) * 36, act) && (tid & 7) == 0;
     }
-    if (nfb) atomicAdd(&w.stats->fallbacks, nfb);
+    if (nfb) atomicAdd(&st->fallbacks, nfb);
   }
-  if (cta == 0) {  // energy of this linearisation point (fixed-order tree)
+  if (gcta == 0) {  // energy of this problem's linearisation point (fixed-order tree)
     double v = 0.0;
-    for (int k = tid; k < kEnergyCtas; k += kThreads) v += __ldcg(w.e_data_part + k);
-    for (int k = tid; k < a.N; k += kThreads) v += __ldcg(w.e_arap_part + k);
+    for (int k = tid; k < pd.e_ctas; k += kThreads) v += __ldcg(w.e_data_part + pd.e_cta0 + k);
+    for (int k = tid; k < pd.N; k += kThreads) v += __ldcg(w.e_arap_part + pd.node_off + k);
     v = bsum(v, sRed + 32);
     if (tid == 0) {
-      w.stats->energy[P.slot] = v;
+      st->energy[P.slot] = v;
       if (!isfinite(v)) atomicOr(err, kErrNonFinite);
     }
   }
@@ -279,12 +286,12 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
       const int buf = gen & 1;
       bsum2(prz, pbb, sRed);
       if (tid == 0) {
-        part[(buf * 3 + 0) * G + cta] = prz;
-        part[(buf * 3 + 1) * G + cta] = pbb;
+        part[(buf * 3 + 0) * GT + cta] = prz;
+        part[(buf * 3 + 1) * GT + cta] = pbb;
       }
     }
     clk.mark(0);  // prologue
-    gbar(w.barrier, gen++, G, cta, err, a.spin_limit);
+    gbar(bar, gen++, G, cta, err, a.spin_limit);
     clk.mark(1);  // first barrier
     double rz = 0.0;
     float betaf = 0.f;
@@ -295,7 +302,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
       {
         const int buf = (gen - 1) & 1;
         if (tid < 32) {
-          wsum_parts<2>(part + (buf * 3 + 0) * G, G, sRed, 16);
+          wsum_parts<2>(part + (buf * 3 + 0) * GT + gb, G, GT, sRed, 16);
         } else {
           for (int e = tid - 32; e < h6; e += kThreads - 32) {
             const int col = sHalo[e / 6], c = e % 6;
@@ -337,12 +344,12 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
       clk.mark(4);  // spmv
       {
         const double t1 = bsum(ppap, sRed);
-        if (tid == 0) part[((gen & 1) * 3 + 0) * G + cta] = t1;
+        if (tid == 0) part[((gen & 1) * 3 + 0) * GT + cta] = t1;
       }
       clk.mark(5);  // block sum
-      gbar(w.barrier, gen++, G, cta, err, a.spin_limit);
+      gbar(bar, gen++, G, cta, err, a.spin_limit);
       clk.mark(6);  // barrier A
-      if (tid < 32) wsum_parts<1>(part + (((gen - 1) & 1) * 3 + 0) * G, G, sRed, 18);
+      if (tid < 32) wsum_parts<1>(part + (((gen - 1) & 1) * 3 + 0) * GT + gb, G, GT, sRed, 18);
       __syncthreads();
       clk.mark(7);  // pAp partials
       const double pAp = sRed[18];
@@ -366,12 +373,12 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
         const int buf = gen & 1;
         bsum2(prr, przn, sRed);
         if (tid == 0) {
-          part[(buf * 3 + 0) * G + cta] = prr;
-          part[(buf * 3 + 1) * G + cta] = przn;
+          part[(buf * 3 + 0) * GT + cta] = prr;
+          part[(buf * 3 + 1) * GT + cta] = przn;
         }
       }
       clk.mark(9);  // block sums
-      gbar(w.barrier, gen++, G, cta, err, a.spin_limit);
+      gbar(bar, gen++, G, cta, err, a.spin_limit);
       clk.mark(10);  // barrier B
     }
     // ---- epilogue ----
@@ -383,7 +390,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
     } else {
       for (int i = tid; i < nrows; i += kThreads) {
         const int node = r0 + i;
-        DQ Tn = twist_update(load_dq_cg(a.transforms + node), sX + i * 6, a.max_rot, a.max_trans, a.update_scale);
+        DQ Tn = twist_update(load_dq_cg(a.transforms + node), sX + i * 6, pd.max_rot, pd.max_trans, pd.update_scale);
         store_dq(a.transforms + node, Tn);
         store_dq(w.plain + node, dq_centered(Tn, node_pos(a.nodes, node)));
       }
@@ -414,7 +421,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
       sV[t] = uf;
       xb[gen & 1][r0 * 6 + t] = uf;
     }
-    gbar(w.barrier, gen++, G, cta, err, a.spin_limit);
+    gbar(bar, gen++, G, cta, err, a.spin_limit);
     for (int e = tid; e < h6; e += kThreads) sV[n6 + e] = __ldcg(xb[(gen - 1) & 1] + sHalo[e / 6] * 6 + e % 6);
     __syncthreads();
     // w = A u ; then the first reduction and m = M^-1 w
@@ -433,11 +440,11 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
       const int buf = gen & 1;
       const double t1 = bsum(pg, sRed), t2 = bsum(pd, sRed + 8), t3 = bsum(pr, sRed + 24);
       if (tid == 0) {
-        part[(buf * 3 + 0) * G + cta] = t1;
-        part[(buf * 3 + 1) * G + cta] = t2;
-        part[(buf * 3 + 2) * G + cta] = t3;
+        part[(buf * 3 + 0) * GT + cta] = t1;
+        part[(buf * 3 + 1) * GT + cta] = t2;
+        part[(buf * 3 + 2) * GT + cta] = t3;
       }
-      gbar(w.barrier, gen++, G, cta, err, a.spin_limit);
+      gbar(bar, gen++, G, cta, err, a.spin_limit);
     };
     reduce_and_publish();
     double gamma_prev = 0.0, alpha_prev = 0.0;
@@ -445,7 +452,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
       {
         const int buf = (gen - 1) & 1;
         if (tid < 32) {
-          wsum_parts<3>(part + (buf * 3 + 0) * G, G, sRed, 16);
+          wsum_parts<3>(part + (buf * 3 + 0) * GT + gb, G, GT, sRed, 16);
         } else {
           for (int e = tid - 32; e < h6; e += kThreads - 32)
             sV[n6 + e] = __ldcg(xb[buf] + sHalo[e / 6] * 6 + e % 6);
@@ -485,9 +492,9 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
         double pr = 0.0;
         for (int t = tid; t < n6; t += kThreads) pr += vR[t] * vR[t];
         const double t3 = bsum(pr, sRed);
-        if (tid == 0) part[((gen & 1) * 3 + 2) * G + cta] = t3;
-        gbar(w.barrier, gen++, G, cta, err, a.spin_limit);
-        if (tid < 32) wsum_parts<1>(part + (((gen - 1) & 1) * 3 + 2) * G, G, sRed, 18);
+        if (tid == 0) part[((gen & 1) * 3 + 2) * GT + cta] = t3;
+        gbar(bar, gen++, G, cta, err, a.spin_limit);
+        if (tid < 32) wsum_parts<1>(part + (((gen - 1) & 1) * 3 + 2) * GT + gb, G, GT, sRed, 18);
         __syncthreads();
         rr_last = sRed[18];
         break;
@@ -508,7 +515,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
     } else {
       for (int i = tid; i < nrows; i += kThreads) {
         const int node = r0 + i;
-        DQ Tn = twist_update(load_dq_cg(a.transforms + node), xf + i * 6, a.max_rot, a.max_trans, a.update_scale);
+        DQ Tn = twist_update(load_dq_cg(a.transforms + node), xf + i * 6, pd.max_rot, pd.max_trans, pd.update_scale);
         store_dq(a.transforms + node, Tn);
         store_dq(w.plain + node, dq_centered(Tn, node_pos(a.nodes, node)));
       }
@@ -516,9 +523,9 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
   }
   clk.mark(11);  // epilogue
   clk.flush();
-  if (cta == 0 && tid == 0) {
-    w.stats->pcg_iters[P.slot] = used;
-    w.stats->pcg_res[P.slot] = sqrt(rr_last);
+  if (gcta == 0 && tid == 0) {
+    st->pcg_iters[P.slot] = used;
+    st->pcg_res[P.slot] = sqrt(rr_last);
   }
 }
 
@@ -561,7 +568,7 @@ int pcg_max_active_ctas(int smem, bool a_in_smem, bool pipelined) {
 
 cudaError_t launch_pcg(const Work& w, const Pattern& p, const SolveArgs& a, int gn_slot, cudaStream_t s) {
   if (a.N <= 0) return cudaSuccess;
-  cudaError_t e = cudaMemsetAsync(w.barrier, 0, sizeof(unsigned), s);
+  cudaError_t e = cudaMemsetAsync(w.barrier, 0, sizeof(unsigned) * (size_t)p.P, s);
   if (e != cudaSuccess) return e;
   GridArgs P;
   P.w = w;

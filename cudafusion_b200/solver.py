@@ -173,6 +173,36 @@ class GaussNewtonSolver:
         check(_lib.lib().cf_gn_solve(self._h, ctypes.byref(p), _ptr(d_transforms), None, st), "cf_gn_solve")
         return None
 
+    def gn_solve_batched(self, dproblems, d_transforms, max_rot=0.0, max_trans=0.0, update_scale=1.0, stats=True,
+                         stream=None):
+        """cf_gn_solve_batched: every problem of `dproblems` (DeviceProblem)
+        through G GN iterations in one pass, d_transforms[i] updated in place.
+        With stats=True returns one dict per problem and synchronises."""
+        n = len(dproblems)
+        probs = (_lib.Problem * max(n, 1))(*[d.c(max_rot, max_trans, update_scale) for d in dproblems])
+        ptrs = (ctypes.c_void_p * max(n, 1))(*[t.data_ptr() for t in d_transforms])
+        st = _stream_ptr(stream)
+        if not stats:
+            check(_lib.lib().cf_gn_solve_batched(self._h, probs, n, ptrs, None, st), "cf_gn_solve_batched")
+            return None
+        out = (_lib.SolveStats * max(n, 1))()
+        check(_lib.lib().cf_gn_solve_batched(self._h, probs, n, ptrs, out, st), "cf_gn_solve_batched")
+        res = []
+        for k in range(n):
+            s = out[k]
+            G = s.gn_iterations_run
+            res.append(dict(
+                energy_initial=s.energy_initial,
+                energy_final=s.energy_final,
+                energy=[s.energy_per_iter[g] for g in range(G + 1)],
+                pcg_iterations=[s.pcg_iterations[g] for g in range(G)],
+                pcg_residual=[s.pcg_residual[g] for g in range(G)],
+                num_blocks=s.num_blocks,
+                precond_fallbacks=s.precond_fallbacks,
+                error_flags=s.error_flags,
+            ))
+        return res
+
     def profile_enable(self, on=True):
         """Per-phase CUDA-event timing of every launch (resets totals)."""
         check(_lib.lib().cf_gn_profile_enable(self._h, 1 if on else 0))

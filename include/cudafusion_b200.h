@@ -213,6 +213,20 @@ CF_API cf_status cf_gn_solve(cf_gn* h, const cf_problem* problem,
                       cf_dual_quat* d_transforms, cf_solve_stats* stats,
                       void* stream);
 
+/* Batched solve (no counterpart in the reference, which solves one warp
+ * field per call): num_problems independent problems of uneven size, each
+ * with its own graph, correspondences, clamps and transforms
+ * (d_transforms[p], a host array of device pointers, updated in place), run
+ * through G GN iterations together — one launch per phase for the whole
+ * batch, one PCG CTA group with its own reductions and stopping test per
+ * problem.  The handle's max_nodes / max_corrs bound the batch totals; one
+ * problem holds at most 48000 nodes; at most 1024 problems.  Problems with
+ * no nodes are skipped.  `stats` (may be NULL: no synchronisation) receives
+ * num_problems records, num_blocks being the batch's total. */
+CF_API cf_status cf_gn_solve_batched(cf_gn* h, const cf_problem* problems, int num_problems,
+                                     cf_dual_quat* const* d_transforms, cf_solve_stats* stats,
+                                     void* stream);
+
 /* Per-phase device timing (no reference counterpart; the reference times the
  * whole solve with std::chrono, include/fusion_app.h:386-391).  When enabled,
  * every kernel launch of a solve is bracketed by CUDA events on the launch
