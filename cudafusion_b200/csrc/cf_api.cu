@@ -5,6 +5,7 @@
 // kernels/solver_kernels.cu:498-541), the PCG row partition, and the launch
 // sequence.  Every device computation happens in cf_kernels.cu.
 #include <algorithm>
+#include <set>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -95,6 +96,7 @@ void free_pattern(Pattern& p) {
   dfree(p.clu_row_begin); dfree(p.cta_of_row); dfree(p.ustart); dfree(p.low_ptr); dfree(p.low_pack);
   dfree(p.low_jl); dfree(p.g_vidx); dfree(p.g_halo_ptr); dfree(p.g_halo_col);
   dfree(p.off_upper); dfree(p.pcg_cta_off); dfree(p.pcg_prob); dfree(p.prob_edge_off);
+  dfree(p.st_tile_ptr); dfree(p.st_tile_row);
   p = Pattern();
 }
 
@@ -103,7 +105,7 @@ void free_work(Work& w) {
   dfree(w.c_srcfw); dfree(w.c_nres); dfree(w.cnt); dfree(w.node_total); dfree(w.inc_start);
   dfree(w.inc); dfree(w.trip); dfree(w.ekeys); dfree(w.rhs); dfree(w.plain); dfree(w.x); dfree(w.z); dfree(w.p0); dfree(w.p1);
   dfree(w.partials); dfree(w.barrier); dfree(w.err); dfree(w.e_data_part); dfree(w.e_arap_part); dfree(w.stats); dfree(w.timers);
-  dfree(w.nodes_cat); dfree(w.T_cat);
+  dfree(w.nodes_cat); dfree(w.T_cat); dfree(w.r); dfree(w.ap); dfree(w.minv32);
   w.cnt_cap = 0;
 }
 
@@ -343,16 +345,18 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
   std::vector<int> rb2, g_vidx(std::max(1, nnzb)), g_halo_ptr, g_halo_col, cta_off2, cta_prob2;
   int smem = 0;
   bool a_smem = true;
-  for (int attempt = 0; attempt < 64; attempt++) {
-    // CTAs per problem: one each, the rest by largest share of blocks
+  // G CTAs over the problems (one each, the rest by largest share of
+  // blocks), each problem's rows split into contiguous ranges of balanced
+  // block counts
+  auto split_rows = [&](int G_, std::vector<int>& rb, std::vector<int>& cta_off, std::vector<int>& cta_prob) {
     std::vector<int> gp(P, 1);
     {
       std::vector<std::pair<double, int>> rem;
-      int left = G - P;
+      int left = G_ - P;
       for (int q = 0; q < P; q++) {
-        const double share = (double)(row_ptr[prob_off[q + 1]] - row_ptr[prob_off[q]]) / std::max(1, nnzb) * G;
+        const double share = (double)(row_ptr[prob_off[q + 1]] - row_ptr[prob_off[q]]) / std::max(1, nnzb) * G_;
         int extra = std::min(std::max(0, (int)share - 1), prob_off[q + 1] - prob_off[q] - 1);
-        extra = std::min(extra, left);
+        extra = std::max(0, std::min(extra, left));
         gp[q] += extra;
         left -= extra;
         rem.push_back({share - gp[q], q});
@@ -368,7 +372,9 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
         }
       }
     }
-    std::vector<int> rb(1, 0), cta_off(1, 0), cta_prob;
+    rb.assign(1, 0);
+    cta_off.assign(1, 0);
+    cta_prob.clear();
     for (int q = 0; q < P; q++) {
       const int q0 = prob_off[q], q1 = prob_off[q + 1];
       const long long target = ((long long)(row_ptr[q1] - row_ptr[q0]) + gp[q] - 1) / gp[q];
@@ -392,6 +398,15 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
       rb.back() = q1;
       cta_off.push_back((int)cta_prob.size());
     }
+  };
+  // the shared-memory kernel keeps per row at least the FP64 inverse, the
+  // operand and the state vectors (~410 B) and 4 B per block: skip it when
+  // that cannot fit in the GPU's shared memory
+  const bool grid_fits = (double)N * 410.0 + 4.0 * nnzb < 0.9 * (double)h->sms * 200.0 * 1024.0;
+  std::set<int> tried{G};
+  for (int attempt = 0; attempt < 64 && h->pcg_mode != 3 && grid_fits; attempt++) {
+    std::vector<int> rb, cta_off, cta_prob;
+    split_rows(G, rb, cta_off, cta_prob);
     const int Gc = (int)rb.size() - 1;
     g_halo_ptr.assign(1, 0);
     g_halo_col.clear();
@@ -418,14 +433,16 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
     a_smem = need_a <= limit;
     smem = a_smem ? need_a : need_noa;
     if (smem > limit) {
-      if (G >= std::min(N, kMaxPcgCtas)) return CF_ERR_CAPACITY;
+      if (G >= std::min(N, kMaxPcgCtas)) break;
       G = std::min(std::min(N, kMaxPcgCtas), G * 2);
+      if (!tried.insert(G).second) break;
       continue;
     }
     int cap = pcg_max_active_ctas(smem, a_smem, pipe);
-    if (cap < P) return CF_ERR_CAPACITY;
+    if (cap < P) break;
     if (Gc > cap) {
       G = cap;
+      if (!tried.insert(G).second) break;
       continue;
     }
     rb2 = rb;
@@ -433,7 +450,30 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
     cta_prob2 = cta_prob;
     break;
   }
-  if (rb2.empty()) return CF_ERR_CAPACITY;
+  // systems too large for shared memory (or mode 3): the streaming PCG
+  std::vector<int> tile_ptr, tile_row;
+  const bool stream = rb2.empty();
+  if (stream) {
+    const int cap = pcg_stream_max_active_ctas();
+    if (cap < P) return CF_ERR_CAPACITY;
+    int Gs = h->pcg_ctas_override > 0 ? h->pcg_ctas_override : cap;
+    Gs = std::max(P, std::min({Gs, cap, N, kMaxPcgCtas}));
+    split_rows(Gs, rb2, cta_off2, cta_prob2);
+    const int TB = pcg_stream_tile_blocks();
+    tile_ptr.assign(1, 0);
+    for (size_t c = 0; c + 1 < rb2.size(); c++) {
+      const int r0 = rb2[c], r1 = rb2[c + 1];
+      tile_row.push_back(r0);
+      for (int i = r0; i < r1; i++)
+        if (row_ptr[i + 1] - row_ptr[tile_row.back()] > TB) tile_row.push_back(i);
+      if (r1 > r0) tile_row.push_back(r1);  // end of the last tile
+      tile_ptr.push_back((int)tile_row.size());
+    }
+    g_halo_ptr.assign(rb2.size(), 0);
+    g_halo_col.clear();
+    smem = pcg_stream_smem_bytes();
+    a_smem = false;
+  }
   G = (int)rb2.size() - 1;
   std::vector<int> edge_off(P + 1, 0);
   for (int q = 0, e = 0; q <= P; q++) {
@@ -462,7 +502,7 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
   int clu_C = 0, clu_smem = 0, clu_nup = 0, clu_nlow = 0, clu_rows = 0;
   std::vector<int> clu_rb, cta_of_row(N, 0), low_pack(std::max<size_t>(1, low_u.size())),
       low_jl(std::max<size_t>(1, low_u.size()));
-  if (h->pcg_mode != 1 && P == 1) {
+  if (h->pcg_mode != 1 && h->pcg_mode != 3 && !stream && P == 1) {
     const int cands[2] = {16, 8};
     for (int ci = 0; ci < 2 && !clu_C; ci++) {
       const int C = cands[ci];
@@ -521,6 +561,7 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
   p.pcg_smem = smem;
   p.pcg_a_in_smem = a_smem ? 1 : 0;
   p.pcg_pipelined = pipe ? 1 : 0;
+  p.pcg_stream = stream ? 1 : 0;
   auto up = [](int** d, const std::vector<int>& v) -> cudaError_t {
     cudaError_t e = dalloc(d, v.size());
     if (e != cudaSuccess) return e;
@@ -541,6 +582,16 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
   CF_TRY(up(&p.pcg_cta_off, cta_off2));
   CF_TRY(up(&p.pcg_prob, cta_prob2));
   CF_TRY(up(&p.prob_edge_off, edge_off));
+  if (stream) {
+    CF_TRY(up(&p.st_tile_ptr, tile_ptr));
+    CF_TRY(up(&p.st_tile_row, tile_row));
+    Work& w = h->w;
+    if (!w.minv32) {
+      CF_TRY(dalloc(&w.r, 6 * (size_t)w.max_nodes));
+      CF_TRY(dalloc(&w.ap, 6 * (size_t)w.max_nodes));
+      CF_TRY(dalloc(&w.minv32, 36 * (size_t)w.max_nodes));
+    }
+  }
   CF_TRY(up(&p.g_vidx, g_vidx));
   CF_TRY(up(&p.g_halo_ptr, g_halo_ptr));
   CF_TRY(up(&p.g_halo_col, g_halo_col));
@@ -634,6 +685,7 @@ cf_status bin_correspondences(cf_gn* h, cudaStream_t s) {
 
 cudaError_t launch_pcg_any(cf_gn* h, const SolveArgs& a, int slot, cudaStream_t s) {
   if (h->p.use_cluster) return launch_pcg_cluster(h->w, h->p, a, slot, s);
+  if (h->p.pcg_stream) return launch_pcg_stream(h->w, h->p, a, slot, s);
   return launch_pcg(h->w, h->p, a, slot, s);
 }
 
@@ -822,7 +874,7 @@ cf_status cf_gn_set_option(cf_gn* h, int option, int value) {
       h->pattern_valid = false;
       return CF_OK;
     case CF_OPT_PCG_MODE:
-      if (value < 0 || value > 2) return CF_ERR_INVALID_ARG;
+      if (value < 0 || value > 3) return CF_ERR_INVALID_ARG;
       h->pcg_mode = value;
       h->pattern_valid = false;
       return CF_OK;

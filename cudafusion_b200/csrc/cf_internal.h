@@ -103,6 +103,10 @@ struct Pattern {
   int* g_vidx = nullptr;      // [nnzb] operand slot of each block's column in its CTA ([own | halo])
   int* g_halo_ptr = nullptr;  // [pcg_ctas+1]
   int* g_halo_col = nullptr;  // distinct columns of other CTAs touched by each CTA
+  // streaming PCG (cf_pcg_stream.cu): A streamed from HBM in tiles of whole rows
+  int pcg_stream = 0;
+  int* st_tile_ptr = nullptr;  // [pcg_ctas+1] into st_tile_row
+  int* st_tile_row = nullptr;  // per CTA: its tiles' first rows, then its end row
 };
 
 // Per-handle work buffers sized by (max_nodes, max_corrs).
@@ -135,6 +139,10 @@ struct Work {
   double* e_data_part = nullptr;  // [kEnergyCtas + kMaxProblems] one partial per energy CTA
   double* e_arap_part = nullptr;  // [max_nodes] per row
   DevStats* stats = nullptr;      // [kMaxProblems]
+  // streaming PCG: residual, A p and the FP32 block inverses in global memory
+  float* r = nullptr;       // [6*max_nodes]
+  float* ap = nullptr;      // [6*max_nodes]
+  float* minv32 = nullptr;  // [36*max_nodes]
   // batched solves: the problems' nodes and transforms, concatenated
   cf_deform_node* nodes_cat = nullptr;  // [max_nodes]
   cf_dual_quat* T_cat = nullptr;        // [max_nodes]
@@ -193,5 +201,10 @@ int expand_smem_bytes(int max_upper_row);
 int pcg_cluster_smem_bytes(int nup_max, int nlow_max, int rows_max, int C, bool a_in_smem);
 int pcg_cluster_max_active(int C, int smem, bool a_in_smem);
 cudaError_t launch_pcg_cluster(const Work& w, const Pattern& p, const SolveArgs& a, int gn_slot, cudaStream_t s);
+
+int pcg_stream_smem_bytes();
+int pcg_stream_tile_blocks();
+int pcg_stream_max_active_ctas();
+cudaError_t launch_pcg_stream(const Work& w, const Pattern& p, const SolveArgs& a, int gn_slot, cudaStream_t s);
 
 }  // namespace cf

@@ -147,13 +147,19 @@ CF_API cf_status cf_gn_linearize_solve(cf_gn* h, const cf_correspondence* d_corr
  *                          update.  With 0 the GN energy can rise for large
  *                          lambda_smooth, exactly as in the reference.
  *  CF_OPT_PCG_CTAS         CTAs of the grid-wide PCG kernel (0 = automatic).
- *  CF_OPT_PCG_MODE         0: automatic; 1: grid-wide cooperative PCG;
- *                          2: single-cluster PCG when the system fits the
- *                          cluster's shared memory (else grid-wide).
+ *  CF_OPT_PCG_MODE         0: automatic; 1: grid-wide cooperative PCG with
+ *                          the system in shared memory (streaming when it
+ *                          does not fit); 2: single-cluster PCG when the
+ *                          system fits the cluster's shared memory (else
+ *                          grid-wide); 3: streaming PCG (A re-read from HBM
+ *                          through TMA bulk copies every iteration, vectors
+ *                          in global memory; the automatic choice for systems
+ *                          larger than the GPU's shared memory).
  *  CF_OPT_PCG_PIPELINED    0: the reference's PCG (two reductions per
  *                          iteration); 1: pipelined PCG, the same iterates in
  *                          exact arithmetic with one reduction per iteration
- *                          (FP64 recurrences), grid-wide mode only. */
+ *                          (FP64 recurrences), shared-memory grid-wide mode
+ *                          only. */
 #define CF_OPT_ARAP_CONSISTENT 1
 #define CF_OPT_PCG_CTAS 2
 #define CF_OPT_PCG_MODE 3

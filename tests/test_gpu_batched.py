@@ -24,10 +24,11 @@ def batch():
             for k, (n, m) in enumerate(sizes)]
 
 
-def _solver(batch, **kw):
+def _solver(batch, mode=0, **kw):
     prm = Params(**{**KW, **kw})
-    return GaussNewtonSolver(prm, max_nodes=sum(p.num_nodes for p in batch),
-                             max_corrs=sum(p.num_corrs for p in batch))
+    s = GaussNewtonSolver(prm, max_nodes=sum(p.num_nodes for p in batch), max_corrs=sum(p.num_corrs for p in batch))
+    s.set_option(_lib.CF_OPT_PCG_MODE, mode)
+    return s
 
 
 def _run_batched(s, batch):
@@ -37,8 +38,13 @@ def _run_batched(s, batch):
     return [dq_as_array(T.cpu().numpy().view(DQ_DTYPE)) for T in Ts], st
 
 
-def test_batched_matches_fp64_oracle(batch, oracle):
-    s = _solver(batch)
+# PCG with the system in shared memory (automatic at this size) and streamed
+PCG_MODES = [0, 3]
+
+
+@pytest.mark.parametrize("mode", PCG_MODES)
+def test_batched_matches_fp64_oracle(batch, oracle, mode):
+    s = _solver(batch, mode)
     Tb, st = _run_batched(s, batch)
     prm = oracle.params(**KW)
     for k, p in enumerate(batch):
@@ -54,8 +60,9 @@ def test_batched_matches_fp64_oracle(batch, oracle):
             assert abs(e - Eo[g]) / abs(Eo[g]) < 1e-4, (k, g, e, Eo[g])
 
 
-def test_batched_matches_single_solves(batch):
-    s = _solver(batch)
+@pytest.mark.parametrize("mode", PCG_MODES)
+def test_batched_matches_single_solves(batch, mode):
+    s = _solver(batch, mode)
     Tb, st = _run_batched(s, batch)
     for k, p in enumerate(batch):
         s1 = GaussNewtonSolver(Params(**KW), max_nodes=p.num_nodes, max_corrs=p.num_corrs)
@@ -69,17 +76,19 @@ def test_batched_matches_single_solves(batch):
         assert abs(st[k]["energy_final"] - st1["energy_final"]) / abs(st1["energy_final"]) < 1e-5
 
 
-def test_batched_deterministic(batch):
-    s = _solver(batch)
+@pytest.mark.parametrize("mode", PCG_MODES)
+def test_batched_deterministic(batch, mode):
+    s = _solver(batch, mode)
     a, _ = _run_batched(s, batch)
     b, _ = _run_batched(s, batch)
     assert all(np.array_equal(x, y) for x, y in zip(a, b))
 
 
-def test_batched_per_problem_tolerance_stop(batch):
+@pytest.mark.parametrize("mode", PCG_MODES)
+def test_batched_per_problem_tolerance_stop(batch, mode):
     """Each problem's PCG stops on its own ||r|| < tol test."""
     kw = dict(gn_iterations=1, pcg_iterations=60, pcg_tolerance=2e-3, lambda_damping=1e-2, lambda_smooth=1.0)
-    s = _solver(batch, **kw)
+    s = _solver(batch, mode, **kw)
     _, st = _run_batched(s, batch)
     for k, p in enumerate(batch):
         s1 = GaussNewtonSolver(Params(**{**KW, **kw}), max_nodes=p.num_nodes, max_corrs=p.num_corrs)

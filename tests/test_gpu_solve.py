@@ -19,8 +19,9 @@ from cudafusion_b200.types import CORR_DTYPE, DQ_DTYPE, NODE_DTYPE, dq_as_array,
 
 pytestmark = pytest.mark.gpu
 
-# (PCG mode, pipelined): grid-wide standard, grid-wide pipelined, single cluster
-MODES = [(1, 0), (1, 1), (2, 0)]
+# (PCG mode, pipelined): grid-wide standard, grid-wide pipelined, single
+# cluster, streaming
+MODES = [(1, 0), (1, 1), (2, 0), (3, 0)]
 
 
 def rel(a, b):
@@ -116,6 +117,7 @@ def test_pcg_modes_agree(p1):
         out.append(dq_as_array(T.cpu().numpy().view(DQ_DTYPE)))
     assert np.abs(out[0] - out[2]).max() < 1e-5  # grid-wide vs single cluster (same schedule)
     assert np.abs(out[0] - out[1]).max() < 2e-4  # standard vs pipelined (rounding-amplifying)
+    assert np.abs(out[0] - out[3]).max() < 1e-5  # shared-memory vs streaming (FP32-stored inverses)
 
 
 @pytest.mark.parametrize("mode", MODES)
