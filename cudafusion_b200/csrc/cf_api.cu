@@ -96,7 +96,7 @@ void free_pattern(Pattern& p) {
   dfree(p.clu_row_begin); dfree(p.cta_of_row); dfree(p.ustart); dfree(p.low_ptr); dfree(p.low_pack);
   dfree(p.low_jl); dfree(p.g_vidx); dfree(p.g_halo_ptr); dfree(p.g_halo_col);
   dfree(p.off_upper); dfree(p.pcg_cta_off); dfree(p.pcg_prob); dfree(p.prob_edge_off);
-  dfree(p.st_tile_ptr); dfree(p.st_tile_row);
+  dfree(p.st_tile_ptr); dfree(p.st_tile_row); dfree(p.edge_terms); dfree(p.edge_energy);
   p = Pattern();
 }
 
@@ -578,6 +578,8 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
   CF_TRY(up(&p.arap_blk_ptr, ablk_ptr));
   CF_TRY(up(&p.arap_blk_edge, ablk_edge));
   CF_TRY(up(&p.edge_ijk, eijk));
+  CF_TRY(dalloc(&p.edge_terms, (size_t)kEdgeTerms4 * std::max(1, n_edges)));
+  CF_TRY(dalloc(&p.edge_energy, (size_t)std::max(1, n_edges)));
   CF_TRY(up(&p.pcg_row_begin, rb2));
   CF_TRY(up(&p.pcg_cta_off, cta_off2));
   CF_TRY(up(&p.pcg_prob, cta_prob2));
@@ -732,7 +734,7 @@ cf_status run_gn(cf_gn* h, SolveArgs& a, cudaStream_t s) {
   { Timed t(h, s, kProfNodePlain, 1); CF_TRY(launch_node_plain(w, a.nodes, a.transforms, a.N, s)); }
   const int G = h->params.gn_iterations;
   for (int g = 0; g < G; g++) {
-    { Timed t(h, s, kProfResidual, 1); CF_TRY(launch_residual(w, h->tb, true, s)); }
+    { Timed t(h, s, kProfResidual, 1); CF_TRY(launch_residual(w, h->tb, h->p, a, a.transforms, true, s)); }
     { Timed t(h, s, kProfAssemble, 1); CF_TRY(launch_assemble(w, h->p, a, a.transforms, s)); }
     { Timed t(h, s, kProfPcg, 1); CF_TRY(launch_pcg_any(h, a, g, s)); }
   }
@@ -916,7 +918,7 @@ cf_status cf_gn_linearize_solve(cf_gn* h, const cf_correspondence* d_corrs, int 
   if (st != CF_OK) return st;
   SolveArgs a = make_args(h, d_nodes, num_nodes, num_corrs);
   a.delta_x = d_delta_x;
-  { Timed t(h, s, kProfResidual, 1); CF_TRY(launch_residual(w, h->tb, false, s)); }
+  { Timed t(h, s, kProfResidual, 1); CF_TRY(launch_residual(w, h->tb, h->p, a, d_transforms, false, s)); }
   { Timed t(h, s, kProfAssemble, 1); CF_TRY(launch_assemble(w, h->p, a, d_transforms, s)); }
   { Timed t(h, s, kProfPcg, 1); CF_TRY(launch_pcg_any(h, a, 0, s)); }
   h->last_gn = 1;

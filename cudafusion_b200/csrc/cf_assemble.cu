@@ -2,19 +2,16 @@
 //
 // expand (once per solve): one CTA per block row r turns the row's
 //   incidences (c, a) — correspondence c has node r in slot a — into entries
-//   (c, a, b) for every valid slot b whose node is an upper column of row r
-//   present in the pattern (find_block < 0 drops the term, as in
-//   kernels/solver_kernels.cu:123-125), grouped by column with a stable
-//   counting sort: order within a column = (warp, round, sub-round, slot,
-//   lane), fixed by the incidence order, so the assembly is deterministic.
-// assemble (every GN iteration), one launch:
-//   CTAs [0, N)        the diagonal block of row r: 8 warps share the row's
-//                      segment (4 entries per lane per round, loads issued
-//                      before the arithmetic), Kahan-compensated partials are
-//                      combined in warp order, then the ARAP terms, the
-//                      damping and the rhs.
-//   CTAs [N, ...)      one warp per off-diagonal upper block (r, j), j > r,
-//                      written with its transpose.
+//   (ii, b), ii the incidence's position in the row's list, for every valid
+//   slot b whose node is an upper column of row r present in the pattern
+//   (find_block < 0 drops the term, as in kernels/solver_kernels.cu:123-125),
+//   grouped by column with a stable counting sort: order within a column =
+//   (warp, round, sub-round, slot, lane), fixed by the incidence order, so
+//   the assembly is deterministic.
+// assemble (every GN iteration): one CTA per block row, described at
+//   assemble_kernel.  The ARAP terms of every edge (weight, residual and the
+//   two rotated offsets of kernels/solver_kernels.cu:202-352) are evaluated
+//   once per GN iteration by the residual launch (cf_kernels.cu).
 #include "cf_device.cuh"
 #include "cf_internal.h"
 
@@ -24,6 +21,8 @@ namespace {
 
 constexpr int kWarps = kThreads / 32;
 constexpr int kEpl = 4;  // incidences per lane per round of expand
+constexpr int kStageCap = 768;  // incidences of a row staged by the assembly (51 KB with their entries)
+constexpr int kRowEdges = 64;   // ARAP edges of a row / of its upper blocks staged by the assembly
 constexpr int kRound = 32 * kEpl;
 
 __device__ __forceinline__ int find_col(const int* cols, int n, int v) {
@@ -125,13 +124,14 @@ __global__ void __launch_bounds__(kThreads) expand_kernel(Work w, Pattern pt, in
     }
 #pragma unroll
     for (int k = 0; k < kEpl; k++) {
+      const int ii = t + lane + 32 * k - i0;  // the incidence's position in the row's list
 #pragma unroll
       for (int b = 0; b < kK; b++) {
         const int key = e[k] >= 0 ? key_of(kk[k], b) : -1;
         const unsigned peers = __match_any_sync(0xffffffffu, key);
         if (key >= 0) {
           const int pos = mycnt[key] + __popc(peers & lanemask_lt());
-          w.trip[base + pos] = ((e[k] >> 2) << 4) | ((e[k] & 3) << 2) | b;
+          w.trip[base + pos] = (ii << 2) | b;
         }
         __syncwarp();
         if (key >= 0 && (__ffs(peers) - 1) == lane) mycnt[key] += __popc(peers);
@@ -143,21 +143,13 @@ __global__ void __launch_bounds__(kThreads) expand_kernel(Work w, Pattern pt, in
 
 struct AsmArgs {
   const cf_deform_node* nodes;
-  const cf_dual_quat* T;
   int N;
-  float lambda_smooth, lambda_damping, arap_sgn;
+  int stage_cap;  // incidences of a row staged in shared memory
+  float lambda_damping;
 };
 
 // index of (p, q), p <= q, in the packed upper triangle of a 6x6 block
 __host__ __device__ constexpr int tri(int p, int q) { return p * 6 - p * (p - 1) / 2 + (q - p); }
-
-// Per-warp staging of the gathered per-correspondence records: kStages
-// rounds of 32 entries, 3 float4 each (skinned src + fw, normal + residual,
-// skin weights), brought in by cp.async so that a warp keeps up to
-// 3*kStages 16-byte gathers per lane in flight without holding them in
-// registers.  Layout [stage][field][lane]: a lane reads consecutive 16 B.
-constexpr int kStages = 8;
-constexpr int kStageFloats4 = kStages * 3 * 32;  // float4 per warp
 
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
@@ -167,229 +159,293 @@ __device__ __forceinline__ void cp_async_commit_wait_all() {
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
-__device__ __forceinline__ float4* stage_smem() {
-  extern __shared__ float4 stage_buf[];
-  return stage_buf;
-}
+// The row's incidence records (skinned src + fw, normal + residual, skin
+// weights) and entries: the first `ns` / `nt` staged in shared memory, the
+// rest (rows beyond the staging capacity) read from global memory.
+struct RowRecords {
+  const float4* s_sf;
+  const float4* s_nr;
+  const float4* s_ws;
+  const int* s_a;     // slot a of each staged incidence
+  const int* s_trip;  // the row's entries (ii << 2) | b
+  const int* inc;     // the row's incidences (c << 2) | a
+  const int* trip;    // the row's entries in global memory
+  int ns, nt;
+  __device__ __forceinline__ void get(const Work& w, int ii, float4& sf, float4& nr, float4& ws) const {
+    if (ii < ns) {
+      sf = s_sf[ii];
+      nr = s_nr[ii];
+      ws = s_ws[ii];
+    } else {
+      const int c = __ldg(inc + ii) >> 2;
+      sf = __ldcg(w.c_srcfw + c);
+      nr = __ldcg(w.c_nres + c);
+      ws = __ldg(w.pk_ws + c);
+    }
+  }
+  __device__ __forceinline__ int slot(int ii) const { return ii < ns ? s_a[ii] : (__ldg(inc + ii) & 3); }
+  __device__ __forceinline__ int entry(int t) const { return t < nt ? s_trip[t] : __ldg(trip + t); }
+};
 
-// Stages entries t + s*stride + lane (s < kStages) of a segment ending at
-// `end`; tv[s] is the entry word of stage s for this lane (-1 if none).
-__device__ __forceinline__ void stage_entries(const Work& w, int t, int stride, int end, float4* buf, int* tv) {
+// Reduce-scatter of 32 per-lane values: afterwards a[0] of lane l holds the
+// warp's sum of value l (31 exchanges instead of 32 x 5 for a butterfly per
+// value; fixed pairing, so the result is deterministic).
+__device__ __forceinline__ void reduce_scatter32(float* a) {
   const int lane = lane_id();
 #pragma unroll
-  for (int s = 0; s < kStages; s++) {
-    const int e = t + s * stride + lane;
-    tv[s] = e < end ? __ldg(w.trip + e) : -1;
-  }
+  for (int s = 16; s >= 1; s >>= 1) {
+    const bool up = (lane & s) != 0;
 #pragma unroll
-  for (int s = 0; s < kStages; s++) {
-    if (tv[s] >= 0) {
-      const int c = tv[s] >> 4;
-      cp_async16(buf + (s * 3 + 0) * 32 + lane, w.c_srcfw + c);
-      cp_async16(buf + (s * 3 + 1) * 32 + lane, w.c_nres + c);
-      cp_async16(buf + (s * 3 + 2) * 32 + lane, w.pk_ws + c);
+    for (int k = 0; k < s; k++) {
+      const float send = up ? a[k] : a[k + s];
+      const float keep = up ? a[k + s] : a[k];
+      a[k] = keep + __shfl_xor_sync(0xffffffffu, send, s);
     }
   }
-  cp_async_commit_wait_all();
-  __syncwarp();
 }
 
-// diagonal block of row r: CTA-wide, values v[0,21) upper entries, v[21,27) rhs
-__device__ void assemble_diag(const Work& w, const Pattern& pt, const AsmArgs& aa, int r) {
-  __shared__ float sred[kWarps][28];
-  const int lane = lane_id(), wid = threadIdx.x >> 5;
-  const int pos = pt.diag_pos[r];
-  const float3 xr = node_pos(aa.nodes, r);
-  const int off = pt.seg_off[pos], end = off + pt.seg_cnt[pos];
-  float s[27], k[27];
-#pragma unroll
-  for (int q = 0; q < 27; q++) s[q] = k[q] = 0.f;
-  float4* buf = stage_smem() + wid * kStageFloats4;
-  // all 8 warps share every round: stage s of warp w covers entries
-  // t + (s*8 + w)*32 + lane
-  for (int t = off; t < end; t += kWarps * kStages * 32) {
-    int tv[kStages];
-    stage_entries(w, t + wid * 32, kWarps * 32, end, buf, tv);
-#pragma unroll
-    for (int j = 0; j < kStages; j++) {
-      if (tv[j] < 0) continue;
-      const float4 sf = buf[(j * 3 + 0) * 32 + lane];
-      if (sf.w == 0.f) continue;
-      const float4 nr = buf[(j * 3 + 1) * 32 + lane];
-      const float4 w4 = buf[(j * 3 + 2) * 32 + lane];
-      const int a = (tv[j] >> 2) & 3, b = tv[j] & 3;
-      const float3 src = f3(sf.x, sf.y, sf.z), n = f3(nr.x, nr.y, nr.z);
-      float Ja[6], Jb[6], fJa[6];
-      jac_row(src, xr, n, sel4(w4, a), Ja);
-      jac_row(src, xr, n, sel4(w4, b), Jb);
-#pragma unroll
-      for (int p = 0; p < 6; p++) fJa[p] = sf.w * Ja[p];
-#pragma unroll
-      for (int p = 0; p < 6; p++)
-#pragma unroll
-        for (int q = p; q < 6; q++) kahan_add(s[tri(p, q)], k[tri(p, q)], fJa[p] * Jb[q]);
-      if (a == b) {
-#pragma unroll
-        for (int p = 0; p < 6; p++) kahan_add(s[21 + p], k[21 + p], -sf.w * Ja[p] * nr.w);
-      }
-    }
-    __syncwarp();
+constexpr int kPartVals = 42;  // 36 block values + 6 rhs (diagonal block only)
+
+// One CTA per block row r.
+//  1. stage: the row's entry list, its incidences' slots and records
+//     (cp.async, one wait)
+//  2. windows: the row's blocks (diagonal first, then the upper off-diagonal
+//     blocks) are cut into windows of 32 entries; warp w takes a contiguous
+//     run of W/8 windows, accumulates lane-private sums of
+//     fw J_a J_b^T (and -fw J_a r for the diagonal) and, whenever it leaves a
+//     block, reduce-scatters them into a partial slot of that block
+//  3. combine: per block value, the warps' partials in warp order (Kahan on
+//     the diagonal block), the ARAP terms of the block's edges (precomputed
+//     by the residual launch), the damping; blocks written with their
+//     transposes, the rhs and the row's ARAP energy.
+__global__ void __launch_bounds__(kThreads, 2) assemble_kernel(Work w, Pattern pt, AsmArgs aa) {
+  extern __shared__ float4 stage_buf[];
+  const int r = blockIdx.x, lane = lane_id(), wid = threadIdx.x >> 5;
+  const int cap = aa.stage_cap;
+  const int i0 = w.inc_start[r], n_inc = w.inc_start[r + 1] - i0;
+  const int dpos = pt.diag_pos[r], nb = pt.row_ptr[r + 1] - dpos;  // upper blocks of the row, diagonal first
+  const int U = pt.max_upper_row;
+  const int Up = (U + 4) & ~3;
+  float4* s_eterm = stage_buf + 3 * cap;     // [kRowEdges][7]: the row's share of its edges' diagonal terms
+  float4* s_bterm = s_eterm + 7 * kRowEdges; // [kRowEdges][9]: off-diagonal terms of the row's blocks' edges
+  double* s_eng = reinterpret_cast<double*>(s_bterm + 9 * kRowEdges);  // [kRowEdges] energies of the row's edges
+  int* s_a = reinterpret_cast<int*>(s_eng + kRowEdges);
+  int* s_trip = s_a + cap;
+  int* s_wpre = s_trip + 4 * cap;  // [Up] window prefix per block
+  int4* s_blk = reinterpret_cast<int4*>(s_wpre + Up);  // [Up] (segment start, count, column, transpose position)
+  int* s_boff = reinterpret_cast<int*>(s_blk + Up);    // [Up] first block edge of each upper block
+  int* s_erole = s_boff + Up;                          // [kRowEdges] role of each row edge
+  float* s_part = reinterpret_cast<float*>(s_erole + kRowEdges);  // [U+8][42]
+  RowRecords R;
+  R.ns = min(n_inc, cap);
+  R.nt = min(pt.seg_off[dpos + nb - 1] + pt.seg_cnt[dpos + nb - 1] - 4 * i0, 4 * cap);
+  R.s_sf = stage_buf;
+  R.s_nr = stage_buf + cap;
+  R.s_ws = stage_buf + 2 * cap;
+  R.s_a = s_a;
+  R.s_trip = s_trip;
+  R.inc = w.inc + i0;
+  R.trip = w.trip + 4 * (size_t)i0;
+  // block info, ARAP terms of the row's edges and of its blocks' edges
+  const int u0 = pt.ustart[r];
+  const int a0 = pt.arap_row_ptr[r], a1 = pt.arap_row_ptr[r + 1] - a0, na = min(a1, kRowEdges);
+  const int be0 = pt.arap_blk_ptr[u0 + 1];  // the row's off-diagonal upper blocks are u0+1 .. u0+nb-1
+  const int be1 = pt.arap_blk_ptr[u0 + nb] - be0, nbe = min(be1, kRowEdges);
+  for (int k = threadIdx.x; k < nb; k += kThreads) {
+    const int pos = dpos + k;
+    s_blk[k] = make_int4(pt.seg_off[pos] - 4 * i0, pt.seg_cnt[pos], pt.col_idx[pos], pt.trans_pos[pos]);
+    s_boff[k] = k == 0 ? 0 : pt.arap_blk_ptr[u0 + k] - be0;
   }
-  // ARAP edges incident to r, spread over warp 0..7 lanes (kernels/solver_kernels.cu:293-313, 337-350)
-  double earap = 0.0;
-  const int a0 = pt.arap_row_ptr[r], a1 = pt.arap_row_ptr[r + 1];
-  for (int e = a0 + threadIdx.x; e < a1; e += kThreads) {
-    const int inc = pt.arap_row_inc[e];
+  // (threads from the back, so that they overlap the block-info loads)
+  const int te = kThreads - 1 - threadIdx.x;
+  if (te < na) {
+    const int inc = pt.arap_row_inc[a0 + te];
     const int ed = inc >> 1, role = inc & 1;
-    Edge ev = eval_edge(aa.nodes, aa.T, pt.edge_ijk[3 * ed], pt.edge_ijk[3 * ed + 1], pt.edge_ijk[3 * ed + 2],
-                        aa.lambda_smooth);
-    if (ev.el == 0.f) continue;
-    float J[6][3];
-    arap_jac(role == 0 ? ev.qi : ev.qj, aa.arap_sgn, J);
+    s_erole[te] = role;
+    const float4* src = pt.edge_terms + (size_t)kEdgeTerms4 * ed + 7 * role;
 #pragma unroll
-    for (int p = 0; p < 6; p++)
+    for (int k = 0; k < 7; k++) cp_async16(s_eterm + 7 * te + k, src + k);
+    s_eng[te] = role == 0 ? pt.edge_energy[ed] : 0.0;
+  } else if (te >= kRowEdges && te < kRowEdges + nbe) {
+    const int e = te - kRowEdges;
+    const float4* src = pt.edge_terms + (size_t)kEdgeTerms4 * pt.arap_blk_edge[be0 + e] + 14;
 #pragma unroll
-      for (int q = p; q < 6; q++) {
-        float t = 0.f;
-        t += J[p][0] * J[q][0];
-        t += J[p][1] * J[q][1];
-        t += J[p][2] * J[q][2];
-        kahan_add(s[tri(p, q)], k[tri(p, q)], ev.el * t);
-      }
-    const float rr[3] = {ev.r.x, ev.r.y, ev.r.z};
-#pragma unroll
-    for (int p = 0; p < 6; p++) {
-      float t = 0.f;
-      t += J[p][0] * rr[0];
-      t += J[p][1] * rr[1];
-      t += J[p][2] * rr[2];
-      kahan_add(s[21 + p], k[21 + p], role == 0 ? -ev.el * t : ev.el * t);
-    }
-    if (role == 0) earap += (double)ev.el * ((double)rr[0] * rr[0] + (double)rr[1] * rr[1] + (double)rr[2] * rr[2]);
+    for (int k = 0; k < 9; k++) cp_async16(s_bterm + 9 * e + k, src + k);
   }
-  // fold the compensation, reduce each warp, combine warps in order (Kahan)
-#pragma unroll
-  for (int q = 0; q < 27; q++) s[q] = warp_sum_f(s[q] - k[q]);
-  earap = warp_sum_d(earap);
-  if (lane == 0) {
-#pragma unroll
-    for (int q = 0; q < 27; q++) sred[wid][q] = s[q];
+  for (int t = threadIdx.x; t < R.nt; t += kThreads) s_trip[t] = __ldg(R.trip + t);
+  for (int ii = threadIdx.x; ii < R.ns; ii += kThreads) {
+    const int e = __ldg(R.inc + ii);
+    const int c = e >> 2;
+    s_a[ii] = e & 3;
+    cp_async16(stage_buf + ii, w.c_srcfw + c);
+    cp_async16(stage_buf + cap + ii, w.c_nres + c);
+    cp_async16(stage_buf + 2 * cap + ii, w.pk_ws + c);
   }
-  __syncthreads();
-  if (wid == 0) {
-    float tot = 0.f, comp = 0.f;
-    if (lane < 27) {
-      for (int v = 0; v < kWarps; v++) kahan_add(tot, comp, sred[v][lane]);
-      tot -= comp;
-    }
-    // damping on the diagonal entries (solver_kernels.cu:183-193)
-    const int dp = (lane == tri(0, 0)) ? 0 : (lane == tri(1, 1)) ? 1 : (lane == tri(2, 2)) ? 2
-                 : (lane == tri(3, 3)) ? 3 : (lane == tri(4, 4)) ? 4 : (lane == tri(5, 5)) ? 5 : -1;
-    if (dp >= 0) tot = tot + aa.lambda_damping * fmaxf(fabsf(tot), dp < 3 ? 1e-3f : 1e-2f);
-    if (lane < 27) sred[0][lane] = tot;
-  }
-  __syncthreads();
-  float* out = pt.values + (size_t)pos * 36;
-  if (threadIdx.x < 36) {
-    const int p = threadIdx.x / 6, q = threadIdx.x % 6;
-    out[threadIdx.x] = sred[0][tri(min(p, q), max(p, q))];
-  } else if (threadIdx.x >= 64 && threadIdx.x < 70) {
-    w.rhs[r * 6 + threadIdx.x - 64] = sred[0][21 + threadIdx.x - 64];
-  }
-  // energy: per-warp ARAP sums combined in warp order by thread 0
-  __shared__ double swe[kWarps];
-  if (lane == 0) swe[wid] = earap;
+  cp_async_commit_wait_all();
   __syncthreads();
   if (threadIdx.x == 0) {
+    int run = 0;
+    for (int k = 0; k < nb; k++) {
+      s_wpre[k] = run;
+      run += (s_blk[k].y + 31) >> 5;
+    }
+    s_wpre[nb] = run;
+  }
+  __syncthreads();
+
+  // ---- 2. windows ----
+  const int W = s_wpre[nb];
+  const int wa = (int)((long long)W * wid / kWarps), wb = (int)((long long)W * (wid + 1) / kWarps);
+  const float3 xr = node_pos(aa.nodes, r);
+  int k = 0;
+  while (k < nb && s_wpre[k + 1] <= wa) k++;
+  float acc[36], rhs[6];
+#pragma unroll
+  for (int q = 0; q < 36; q++) acc[q] = 0.f;
+#pragma unroll
+  for (int q = 0; q < 6; q++) rhs[q] = 0.f;
+  float3 xc = node_pos(aa.nodes, k < nb ? s_blk[k].z : r);
+  int seg0 = k < nb ? s_blk[k].x : 0, segn = k < nb ? s_blk[k].y : 0;
+  for (int win = wa; win < wb; win++) {
+    const int t = seg0 + (win - s_wpre[k]) * 32 + lane;
+    if (t < seg0 + segn) {
+      const int e = R.entry(t);
+      const int ii = e >> 2, b = e & 3;
+      float4 sf, nr, w4;
+      R.get(w, ii, sf, nr, w4);
+      if (sf.w != 0.f) {
+        const int a = R.slot(ii);
+        const float3 src = f3(sf.x, sf.y, sf.z), n = f3(nr.x, nr.y, nr.z);
+        float Ja[6], Jb[6];
+        jac_row(src, xr, n, sel4(w4, a), Ja);
+        jac_row(src, xc, n, sel4(w4, b), Jb);
+#pragma unroll
+        for (int p = 0; p < 6; p++) {
+          const float f = sf.w * Ja[p];
+#pragma unroll
+          for (int q = 0; q < 6; q++) acc[p * 6 + q] += f * Jb[q];
+        }
+        if (k == 0 && a == b) {
+#pragma unroll
+          for (int p = 0; p < 6; p++) rhs[p] += -sf.w * Ja[p] * nr.w;
+        }
+      }
+    }
+    // leaving block k (next window belongs to another block, or the run ends)
+    if (win + 1 == wb || win + 1 == s_wpre[k + 1]) {
+      float* dst = s_part + (size_t)(k + wid) * kPartVals;
+      float extra[4] = {acc[32], acc[33], acc[34], acc[35]};
+      reduce_scatter32(acc);
+      dst[lane] = acc[0];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const float v = warp_sum_f(extra[q]);
+        if (lane == 0) dst[32 + q] = v;
+      }
+      if (k == 0) {
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+          const float v = warp_sum_f(rhs[q]);
+          if (lane == 0) dst[36 + q] = v;
+          rhs[q] = 0.f;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 36; q++) acc[q] = 0.f;
+      if (win + 1 < wb) {
+        k++;
+        while (k < nb && s_wpre[k + 1] <= win + 1) k++;
+        xc = node_pos(aa.nodes, s_blk[k].z);
+        seg0 = s_blk[k].x;
+        segn = s_blk[k].y;
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- 3. combine ----
+  const int nwork = 27 + 36 * (nb - 1);
+  for (int item = threadIdx.x; item < nwork; item += kThreads) {
+    int kb, v;
+    if (item < 27) {
+      kb = 0;
+      v = item;
+    } else {
+      kb = 1 + (item - 27) / 36;
+      v = (item - 27) % 36;
+    }
+    // warps that touched block kb, in warp order
+    const int w0 = s_wpre[kb], w1 = s_wpre[kb + 1];
+    float tot = 0.f, comp = 0.f;
+    if (w1 > w0) {
+      int idx;
+      if (kb == 0) {
+        int p = 0;
+        while (v >= 21 ? false : (tri(p, 5) < v)) p++;  // row of the upper-triangle index
+        idx = v < 21 ? p * 6 + (v - tri(p, p) + p) : 36 + (v - 21);
+      } else {
+        idx = v;
+      }
+      for (int ww = 0; ww < kWarps; ww++) {  // the warps whose window runs met block kb
+        const int a_w = (int)((long long)W * ww / kWarps), b_w = (int)((long long)W * (ww + 1) / kWarps);
+        if (a_w >= b_w || a_w >= w1 || b_w <= w0) continue;
+        const float x = s_part[(size_t)(kb + ww) * kPartVals + idx];
+        if (kb == 0) kahan_add(tot, comp, x); else tot += x;
+      }
+      tot -= comp;
+      comp = 0.f;
+    }
+    const int pos = dpos + kb;
+    if (kb == 0) {
+      // ARAP edges incident to r (kernels/solver_kernels.cu:293-313, 337-350)
+      for (int e = 0; e < a1; e++) {
+        float x;
+        if (e < na) {
+          x = reinterpret_cast<const float*>(s_eterm + 7 * e)[v];
+        } else {
+          const int inc = pt.arap_row_inc[a0 + e];
+          x = reinterpret_cast<const float*>(pt.edge_terms + (size_t)kEdgeTerms4 * (inc >> 1) + 7 * (inc & 1))[v];
+        }
+        kahan_add(tot, comp, x);
+      }
+      tot -= comp;
+      if (v < 21) {
+        int p = 0;
+        while (tri(p, 5) < v) p++;
+        const int q = v - tri(p, p) + p;
+        // damping on the diagonal entries (solver_kernels.cu:183-193)
+        if (p == q) tot = tot + aa.lambda_damping * fmaxf(fabsf(tot), p < 3 ? 1e-3f : 1e-2f);
+        float* out = pt.values + (size_t)pos * 36;
+        out[p * 6 + q] = tot;
+        out[q * 6 + p] = tot;
+      } else {
+        w.rhs[r * 6 + (v - 21)] = tot;
+      }
+    } else {
+      // ARAP edges (r, j) visited from r (solver_kernels.cu:315-324)
+      const int e0 = s_boff[kb], e1 = kb + 1 < nb ? s_boff[kb + 1] : be1;
+      for (int e = e0; e < e1; e++) {
+        tot += e < nbe ? reinterpret_cast<const float*>(s_bterm + 9 * e)[v]
+                       : reinterpret_cast<const float*>(pt.edge_terms + (size_t)kEdgeTerms4 *
+                                                                          pt.arap_blk_edge[be0 + e] + 14)[v];
+      }
+      pt.values[(size_t)pos * 36 + v] = tot;
+      pt.values[(size_t)s_blk[kb].w * 36 + (v % 6) * 6 + v / 6] = tot;
+    }
+  }
+  if (threadIdx.x == kThreads - 1) {  // the row's ARAP energy: edges owned by r
     double t = 0.0;
-    for (int v = 0; v < kWarps; v++) t += swe[v];
+    for (int e = 0; e < a1; e++) {
+      if (e < na) {
+        t += s_eng[e];
+      } else {
+        const int inc = pt.arap_row_inc[a0 + e];
+        if (!(inc & 1)) t += pt.edge_energy[inc >> 1];
+      }
+    }
     w.e_arap_part[r] = t;
   }
 }
-
-// off-diagonal upper block (r, j), j > r: one warp
-__device__ void assemble_off(const Work& w, const Pattern& pt, const AsmArgs& aa, int u) {
-  const int lane = lane_id();
-  const int pos = pt.upper_pos[u], r = pt.upper_row[u], j = pt.col_idx[pos];
-  const float3 xr = node_pos(aa.nodes, r), xj = node_pos(aa.nodes, j);
-  const int off = pt.seg_off[pos], end = off + pt.seg_cnt[pos];
-  float acc[36];
-#pragma unroll
-  for (int q = 0; q < 36; q++) acc[q] = 0.f;
-  float4* buf = stage_smem() + (threadIdx.x >> 5) * kStageFloats4;
-  for (int t = off; t < end; t += kStages * 32) {
-    int tv[kStages];
-    stage_entries(w, t, 32, end, buf, tv);
-#pragma unroll
-    for (int e = 0; e < kStages; e++) {
-      if (tv[e] < 0) continue;
-      const float4 sf = buf[(e * 3 + 0) * 32 + lane];
-      if (sf.w == 0.f) continue;
-      const float4 nr = buf[(e * 3 + 1) * 32 + lane];
-      const float4 w4 = buf[(e * 3 + 2) * 32 + lane];
-      const int a = (tv[e] >> 2) & 3, b = tv[e] & 3;
-      const float3 src = f3(sf.x, sf.y, sf.z), n = f3(nr.x, nr.y, nr.z);
-      float Ja[6], Jb[6];
-      jac_row(src, xr, n, sel4(w4, a), Ja);
-      jac_row(src, xj, n, sel4(w4, b), Jb);
-#pragma unroll
-      for (int p = 0; p < 6; p++) {
-        const float f = sf.w * Ja[p];
-#pragma unroll
-        for (int q = 0; q < 6; q++) acc[p * 6 + q] += f * Jb[q];
-      }
-    }
-    __syncwarp();
-  }
-  // ARAP edges (r, j) visited from r (solver_kernels.cu:315-324)
-  const int e0 = pt.arap_blk_ptr[u], e1 = pt.arap_blk_ptr[u + 1];
-  for (int e = e0 + lane; e < e1; e += 32) {
-    const int ed = pt.arap_blk_edge[e];
-    Edge ev = eval_edge(aa.nodes, aa.T, pt.edge_ijk[3 * ed], pt.edge_ijk[3 * ed + 1], pt.edge_ijk[3 * ed + 2],
-                        aa.lambda_smooth);
-    if (ev.el == 0.f) continue;
-    float Ji[6][3], Jj[6][3];
-    arap_jac(ev.qi, aa.arap_sgn, Ji);
-    arap_jac(ev.qj, aa.arap_sgn, Jj);
-#pragma unroll
-    for (int p = 0; p < 6; p++)
-#pragma unroll
-      for (int q = 0; q < 6; q++) {
-        float t = 0.f;
-        t += Ji[p][0] * Jj[q][0];
-        t += Ji[p][1] * Jj[q][1];
-        t += Ji[p][2] * Jj[q][2];
-        acc[p * 6 + q] += -ev.el * t;
-      }
-  }
-#pragma unroll
-  for (int q = 0; q < 36; q++) acc[q] = warp_sum_f(acc[q]);
-  float* out = pt.values + (size_t)pos * 36;
-  float* outT = pt.values + (size_t)pt.trans_pos[pos] * 36;
-#pragma unroll
-  for (int h = 0; h < 2; h++) {
-    const int l = lane + 32 * h;
-    if (l < 36) {
-      float val = 0.f;
-#pragma unroll
-      for (int t = 0; t < 36; t++)
-        if (t == l) val = acc[t];
-      out[l] = val;
-      outT[(l % 6) * 6 + (l / 6)] = val;
-    }
-  }
-}
-
-__global__ void __launch_bounds__(kThreads, 2) assemble_kernel(Work w, Pattern pt, AsmArgs aa) {
-  if ((int)blockIdx.x < aa.N) {
-    assemble_diag(w, pt, aa, blockIdx.x);
-  } else {
-    const int k = ((int)blockIdx.x - aa.N) * kWarps + (threadIdx.x >> 5);
-    if (k < pt.n_off) assemble_off(w, pt, aa, pt.off_upper[k]);
-  }
-}
-
-inline int cdiv_(int a, int b) { return (a + b - 1) / b; }
 
 }  // namespace
 
@@ -405,20 +461,25 @@ cudaError_t launch_expand(const Work& w, const Pattern& p, int N, cudaStream_t s
   return cudaGetLastError();
 }
 
+int assemble_smem_bytes(int max_upper_row) {
+  const int Up = (max_upper_row + 4) & ~3;
+  return kStageCap * (3 * (int)sizeof(float4) + 5 * (int)sizeof(int)) + kRowEdges * 16 * (int)sizeof(float4) +
+         kRowEdges * 8 + Up * (4 + 16 + 4) + kRowEdges * 4 + (max_upper_row + kWarps) * kPartVals * 4;
+}
+
 cudaError_t launch_assemble(const Work& w, const Pattern& p, const SolveArgs& a, const cf_dual_quat* T,
                             cudaStream_t s) {
+  (void)T;  // the transforms enter through the ARAP terms of the residual launch
   if (a.N <= 0) return cudaSuccess;
   AsmArgs aa;
   aa.nodes = a.nodes;
-  aa.T = T;
   aa.N = a.N;
-  aa.lambda_smooth = a.lambda_smooth;
+  aa.stage_cap = kStageCap;
   aa.lambda_damping = a.lambda_damping;
-  aa.arap_sgn = a.arap_consistent ? -1.f : 1.f;
-  const int smem = kWarps * kStageFloats4 * (int)sizeof(float4);
+  const int smem = assemble_smem_bytes(p.max_upper_row);
   cudaError_t e = cudaFuncSetAttribute(assemble_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  assemble_kernel<<<a.N + cdiv_(p.n_off, kWarps), kThreads, smem, s>>>(w, p, aa);
+  assemble_kernel<<<a.N, kThreads, smem, s>>>(w, p, aa);
   return cudaGetLastError();
 }
 

@@ -13,6 +13,9 @@ constexpr int kThreads = 256;
 constexpr int kErrTimeoutBit = 1;   // bounded barrier gave up
 constexpr int kErrNonFiniteBit = 2; // NaN/Inf in the solution or energy
 constexpr int kStatsSlots = CF_MAX_GN_ITERS + 1;
+// float4 per ARAP edge in Pattern::edge_terms: diagonal block + rhs of i (7),
+// of j (7), off-diagonal block (9)
+constexpr int kEdgeTerms4 = 23;
 
 // Device-side statistics of one solve (copied to cf_solve_stats on request).
 struct DevStats {
@@ -76,6 +79,8 @@ struct Pattern {
   int* arap_blk_ptr = nullptr;  // [n_upper+1] over upper off-diagonal blocks
   int* arap_blk_edge = nullptr;
   int* edge_ijk = nullptr;      // [3*n_edges] i, j, k (slot in i's list)
+  float4* edge_terms = nullptr; // [kEdgeTerms4*n_edges] per GN iteration: the edge's block contributions
+  double* edge_energy = nullptr; // [n_edges] per GN iteration: el |r|^2
   // per-pattern work arrays
   float* values = nullptr;  // [nnzb*36]
   int* seg_off = nullptr;   // [nnzb]
@@ -180,7 +185,8 @@ cudaError_t launch_bin_scatter(const Work& w, const Table& tb, cudaStream_t s);
 cudaError_t launch_expand(const Work& w, const Pattern& p, int N, cudaStream_t s);
 cudaError_t launch_node_plain(const Work& w, const cf_deform_node* nodes, const cf_dual_quat* T, int N,
                               cudaStream_t s);
-cudaError_t launch_residual(const Work& w, const Table& tb, bool skin, cudaStream_t s);
+cudaError_t launch_residual(const Work& w, const Table& tb, const Pattern& p, const SolveArgs& a,
+                            const cf_dual_quat* T, bool skin, cudaStream_t s);
 cudaError_t launch_batch_gather(const Work& w, const Table& tb, cudaStream_t s);
 cudaError_t launch_batch_scatter(const Work& w, const Table& tb, cudaStream_t s);
 cudaError_t launch_assemble(const Work& w, const Pattern& p, const SolveArgs& a, const cf_dual_quat* T,

@@ -253,9 +253,89 @@ __device__ __forceinline__ void e_range(const Table& tb, const ProbDesc& d, int&
   c1 = d.corr_off + min(d.M, lc * per + per);
 }
 
+struct EdgeArgs {
+  const int* edge_ijk;
+  int n_edges;
+  const cf_deform_node* nodes;
+  const cf_dual_quat* T;
+  float lambda, arap_sgn;
+  float4* out;     // [kEdgeTerms4 * n_edges]
+  double* energy;  // [n_edges]
+};
+
+__device__ __forceinline__ int tri6(int p, int q) { return p * 6 - p * (p - 1) / 2 + (q - p); }
+
+// CTAs after the correspondence ones: every ARAP edge (i, j) at the current
+// transforms (kernels/solver_kernels.cu:202-352: strain and Huber weight,
+// residual r, Jacobians J_i, J_j of both endpoints), written as its complete
+// contributions for the assembly: the diagonal blocks of i and j (upper
+// triangle el J J^T and rhs -+el J r, 27 + pad floats each), the
+// off-diagonal block -el J_i J_j^T (36 floats) and the energy el |r|^2 (FP64).
+__device__ void edge_terms_cta(const EdgeArgs& ea, int cta) {
+  const int ed = cta * kThreads + threadIdx.x;
+  if (ed >= ea.n_edges) return;
+  const Edge ev = eval_edge(ea.nodes, ea.T, ea.edge_ijk[3 * ed], ea.edge_ijk[3 * ed + 1], ea.edge_ijk[3 * ed + 2],
+                            ea.lambda);
+  float Ji[6][3], Jj[6][3];
+  arap_jac(ev.qi, ea.arap_sgn, Ji);
+  arap_jac(ev.qj, ea.arap_sgn, Jj);
+  const float rr[3] = {ev.r.x, ev.r.y, ev.r.z};
+  float di[28], dj[28], o[36];
+#pragma unroll
+  for (int p = 0; p < 6; p++)
+#pragma unroll
+    for (int q = p; q < 6; q++) {
+      float ti = 0.f, tj = 0.f;
+      ti += Ji[p][0] * Ji[q][0];
+      ti += Ji[p][1] * Ji[q][1];
+      ti += Ji[p][2] * Ji[q][2];
+      tj += Jj[p][0] * Jj[q][0];
+      tj += Jj[p][1] * Jj[q][1];
+      tj += Jj[p][2] * Jj[q][2];
+      di[tri6(p, q)] = ev.el * ti;
+      dj[tri6(p, q)] = ev.el * tj;
+    }
+#pragma unroll
+  for (int p = 0; p < 6; p++) {
+    float ti = 0.f, tj = 0.f;
+    ti += Ji[p][0] * rr[0];
+    ti += Ji[p][1] * rr[1];
+    ti += Ji[p][2] * rr[2];
+    tj += Jj[p][0] * rr[0];
+    tj += Jj[p][1] * rr[1];
+    tj += Jj[p][2] * rr[2];
+    di[21 + p] = -ev.el * ti;
+    dj[21 + p] = ev.el * tj;
+  }
+  di[27] = dj[27] = 0.f;
+#pragma unroll
+  for (int p = 0; p < 6; p++)
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+      float t = 0.f;
+      t += Ji[p][0] * Jj[q][0];
+      t += Ji[p][1] * Jj[q][1];
+      t += Ji[p][2] * Jj[q][2];
+      o[p * 6 + q] = -ev.el * t;
+    }
+  float4* out = ea.out + (size_t)kEdgeTerms4 * ed;
+#pragma unroll
+  for (int k = 0; k < 7; k++) out[k] = make_float4(di[4 * k], di[4 * k + 1], di[4 * k + 2], di[4 * k + 3]);
+#pragma unroll
+  for (int k = 0; k < 7; k++) out[7 + k] = make_float4(dj[4 * k], dj[4 * k + 1], dj[4 * k + 2], dj[4 * k + 3]);
+#pragma unroll
+  for (int k = 0; k < 9; k++) out[14 + k] = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
+  ea.energy[ed] =
+      ev.el > 0.f ? (double)ev.el * ((double)rr[0] * rr[0] + (double)rr[1] * rr[1] + (double)rr[2] * rr[2]) : 0.0;
+}
+
 template <bool SKIN>
-__global__ void __launch_bounds__(kThreads) residual_kernel(Table tb, Work w) {
+__global__ void __launch_bounds__(kThreads) residual_kernel(Table tb, Work w, EdgeArgs ea) {
   __shared__ double red[32];
+  if ((int)blockIdx.x >= tb.n_e) {
+    edge_terms_cta(ea, blockIdx.x - tb.n_e);
+    return;
+  }
   const ProbDesc d = tb.desc[tb.e_prob[blockIdx.x]];
   int c0, c1;
   e_range(tb, d, c0, c1);
@@ -437,12 +517,23 @@ cudaError_t launch_node_plain(const Work& w, const cf_deform_node* nodes, const 
   return cudaGetLastError();
 }
 
-cudaError_t launch_residual(const Work& w, const Table& tb, bool skin, cudaStream_t s) {
-  if (tb.n_e <= 0) return cudaSuccess;
+cudaError_t launch_residual(const Work& w, const Table& tb, const Pattern& p, const SolveArgs& a,
+                            const cf_dual_quat* T, bool skin, cudaStream_t s) {
+  EdgeArgs ea;
+  ea.edge_ijk = p.edge_ijk;
+  ea.n_edges = p.n_edges;
+  ea.nodes = a.nodes;
+  ea.T = T;
+  ea.lambda = a.lambda_smooth;
+  ea.arap_sgn = a.arap_consistent ? -1.f : 1.f;
+  ea.out = p.edge_terms;
+  ea.energy = p.edge_energy;
+  const int grid = tb.n_e + cdiv(p.n_edges, kThreads);
+  if (grid <= 0) return cudaSuccess;
   if (skin)
-    residual_kernel<true><<<tb.n_e, kThreads, 0, s>>>(tb, w);
+    residual_kernel<true><<<grid, kThreads, 0, s>>>(tb, w, ea);
   else
-    residual_kernel<false><<<tb.n_e, kThreads, 0, s>>>(tb, w);
+    residual_kernel<false><<<grid, kThreads, 0, s>>>(tb, w, ea);
   return cudaGetLastError();
 }
 
