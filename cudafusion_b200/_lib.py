@@ -22,6 +22,8 @@ CF_OPT_ARAP_CONSISTENT = 1
 CF_OPT_PCG_CTAS = 2
 CF_OPT_PCG_MODE = 3
 CF_OPT_PCG_PIPELINED = 4
+CF_OPT_GRAPH = 5
+CF_OPT_GRAPH_ACTIVE = 6
 CF_MAX_GN_ITERS = 32
 CF_PROF_SLOTS = 12
 CF_NOALLOC_MAX_NODES = 8192
@@ -36,6 +38,7 @@ EXPORTS = [
     "cf_gn_set_params",
     "cf_gn_get_params",
     "cf_gn_set_option",
+    "cf_gn_get_option",
     "cf_gn_check",
     "cf_gn_linearize_solve",
     "cf_gn_invalidate_pattern",
@@ -127,6 +130,7 @@ def lib():
         L.cf_gn_set_params.argtypes = [vp, ctypes.POINTER(GNParams)]
         L.cf_gn_get_params.argtypes = [vp, ctypes.POINTER(GNParams)]
         L.cf_gn_set_option.argtypes = [vp, i, i]
+        L.cf_gn_get_option.argtypes = [vp, i, ctypes.POINTER(i)]
         L.cf_gn_check.argtypes = [vp, vp]
         L.cf_gn_linearize_solve.argtypes = [vp, vp, i, vp, vp, i, vp, vp]
         L.cf_gn_invalidate_pattern.argtypes = [vp]

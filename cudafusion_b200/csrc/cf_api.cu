@@ -43,6 +43,14 @@ struct cf_gn {
   bool pattern_valid = false;
   std::vector<int> h_row_ptr, h_col_idx;
   std::vector<int> pattern_key;  // problem sizes the pattern was built for
+  unsigned pattern_version = 0;  // bumped by every pattern build
+  // the captured launch sequence of the last solve and the arguments it was captured with
+  int use_graph = 1;
+  std::vector<unsigned char> graph_key;
+  cudaGraphExec_t graph_exec = nullptr;
+  long long graph_launches = 0;
+  bool graph_key_failed = false;
+  int graph_last = 0;  // the last solve ran as a graph
   DevStats* h_stats = nullptr;   // pinned, [kMaxProblems]
   // problem table: host copies (to skip unchanged uploads) and device arrays
   std::vector<ProbDesc> h_desc;
@@ -625,6 +633,7 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
   }
   h->h_row_ptr = row_ptr;
   h->h_col_idx = col_idx;
+  h->pattern_version++;
   h->pattern_valid = true;
   return CF_OK;
 }
@@ -775,6 +784,84 @@ cf_status read_stats(cf_gn* h, cf_solve_stats* stats, const std::vector<int>& sl
   return CF_OK;
 }
 
+// The device work of a solve after the host-side preparation: statistics
+// reset, (batched: gather), binning, G GN iterations, final energy,
+// (batched: scatter).  kind 0: single problem, 1: batch.
+cf_status enqueue_solve(cf_gn* h, int kind, SolveArgs& a, cudaStream_t s) {
+  Work& w = h->w;
+  CF_TRY(cudaMemsetAsync(w.stats, 0, sizeof(DevStats) * (size_t)h->tb.P, s));
+  CF_TRY(cudaMemsetAsync(w.err, 0, sizeof(int), s));
+  if (kind == 1) {
+    Timed t(h, s, kProfOther, 1);
+    CF_TRY(launch_batch_gather(w, h->tb, s));
+  }
+  cf_status st = bin_correspondences(h, s);
+  if (st != CF_OK) return st;
+  st = run_gn(h, a, s);
+  if (st != CF_OK) return st;
+  if (kind == 1) {
+    Timed t(h, s, kProfOther, 1);
+    CF_TRY(launch_batch_scatter(w, h->tb, s));
+  }
+  return CF_OK;
+}
+
+// Runs enqueue_solve as a CUDA graph: captured once per distinct set of
+// launch arguments (the problem table itself lives in device memory, so new
+// caller buffers of the same sizes replay the same graph), replayed after.
+// Falls back to direct launches when graphs are off, while profiling, on the
+// legacy default stream, inside a caller's own capture, or if capture fails.
+cf_status solve_graphed(cf_gn* h, int kind, SolveArgs& a, cudaStream_t s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  h->graph_last = 0;
+  if (!h->use_graph || h->profile || s == nullptr || cudaStreamIsCapturing(s, &cs) != cudaSuccess ||
+      cs != cudaStreamCaptureStatusNone)
+    return enqueue_solve(h, kind, a, s);
+  std::vector<unsigned char> key(sizeof(int) * 2 + sizeof(unsigned) + sizeof(cf_gn_params) + sizeof(SolveArgs));
+  unsigned char* k = key.data();
+  memcpy(k, &kind, sizeof(int)); k += sizeof(int);
+  memcpy(k, &h->tb.P, sizeof(int)); k += sizeof(int);
+  memcpy(k, &h->pattern_version, sizeof(unsigned)); k += sizeof(unsigned);
+  memcpy(k, &h->params, sizeof(cf_gn_params)); k += sizeof(cf_gn_params);
+  memcpy(k, &a, sizeof(SolveArgs));
+  if (key == h->graph_key) {
+    if (h->graph_key_failed) return enqueue_solve(h, kind, a, s);
+    h->launches += h->graph_launches;
+    CF_TRY(cudaGraphLaunch(h->graph_exec, s));
+    h->graph_last = 1;
+    return CF_OK;
+  }
+  if (h->graph_exec) {
+    cudaGraphExecDestroy(h->graph_exec);
+    h->graph_exec = nullptr;
+  }
+  h->graph_key = key;
+  h->graph_key_failed = false;
+  const long long before = h->launches;
+  cudaGraph_t g = nullptr;
+  cf_status st = from_cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  if (st == CF_OK) {
+    st = enqueue_solve(h, kind, a, s);
+    const cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (st == CF_OK && e != cudaSuccess) st = from_cuda(e);
+    if (st == CF_OK && cudaGraphInstantiate(&h->graph_exec, g, 0) != cudaSuccess) st = CF_ERR_CUDA;
+  }
+  if (g) cudaGraphDestroy(g);
+  h->graph_launches = h->launches - before;
+  h->launches = before;
+  if (st != CF_OK) {  // not capturable here: remember, and launch directly
+    cudaGetLastError();
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    h->graph_exec = nullptr;
+    h->graph_key_failed = true;
+    return enqueue_solve(h, kind, a, s);
+  }
+  h->launches += h->graph_launches;
+  CF_TRY(cudaGraphLaunch(h->graph_exec, s));
+  h->graph_last = 1;
+  return CF_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -839,6 +926,7 @@ cf_status cf_gn_create(const cf_gn_params* params, int max_nodes, int max_corrs,
 cf_status cf_gn_destroy(cf_gn* h) {
   if (!h) return CF_ERR_INVALID_ARG;
   cudaDeviceSynchronize();
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   free_pattern(h->p);
   free_work(h->w);
   free_table(h->tb);
@@ -880,11 +968,27 @@ cf_status cf_gn_set_option(cf_gn* h, int option, int value) {
       h->pcg_mode = value;
       h->pattern_valid = false;
       return CF_OK;
+    case CF_OPT_GRAPH:
+      h->use_graph = value ? 1 : 0;
+      return CF_OK;
     case CF_OPT_PCG_CTAS:
       if (value < 0 || value > kMaxPcgCtas) return CF_ERR_INVALID_ARG;
       h->pcg_ctas_override = value;
       h->pattern_valid = false;
       return CF_OK;
+  }
+  return CF_ERR_INVALID_ARG;
+}
+
+cf_status cf_gn_get_option(const cf_gn* h, int option, int* value) {
+  if (!h || !value) return CF_ERR_INVALID_ARG;
+  switch (option) {
+    case CF_OPT_ARAP_CONSISTENT: *value = h->arap_consistent; return CF_OK;
+    case CF_OPT_PCG_CTAS: *value = h->pcg_ctas_override; return CF_OK;
+    case CF_OPT_PCG_MODE: *value = h->pcg_mode; return CF_OK;
+    case CF_OPT_PCG_PIPELINED: *value = h->pcg_pipelined; return CF_OK;
+    case CF_OPT_GRAPH: *value = h->use_graph; return CF_OK;
+    case CF_OPT_GRAPH_ACTIVE: *value = h->graph_last; return CF_OK;
   }
   return CF_ERR_INVALID_ARG;
 }
@@ -942,17 +1046,12 @@ cf_status cf_gn_solve(cf_gn* h, const cf_problem* prob, cf_dual_quat* d_transfor
                                    prob->max_trans, prob->update_scale)},
                      true, s);
   if (st != CF_OK) return st;
-  Work& w = h->w;
-  CF_TRY(cudaMemsetAsync(w.stats, 0, sizeof(DevStats), s));
-  CF_TRY(cudaMemsetAsync(w.err, 0, sizeof(int), s));
-  st = bin_correspondences(h, s);
-  if (st != CF_OK) return st;
   SolveArgs a = make_args(h, prob->nodes, N, M);
   a.transforms = d_transforms;
   a.max_rot = prob->max_rot;
   a.max_trans = prob->max_trans;
   a.update_scale = prob->update_scale;
-  st = run_gn(h, a, s);
+  st = solve_graphed(h, 0, a, s);
   if (st != CF_OK || !stats) return st;
   return read_stats(h, stats, {0}, 1, s);
 }
@@ -990,17 +1089,10 @@ cf_status cf_gn_solve_batched(cf_gn* h, const cf_problem* problems, int num_prob
     CF_TRY(dalloc(&w.nodes_cat, (size_t)w.max_nodes));
     CF_TRY(dalloc(&w.T_cat, (size_t)w.max_nodes));
   }
-  CF_TRY(cudaMemsetAsync(w.stats, 0, sizeof(DevStats) * pr.size(), s));
-  CF_TRY(cudaMemsetAsync(w.err, 0, sizeof(int), s));
-  { Timed t(h, s, kProfOther, 1); CF_TRY(launch_batch_gather(w, h->tb, s)); }
-  st = bin_correspondences(h, s);
-  if (st != CF_OK) return st;
   SolveArgs a = make_args(h, w.nodes_cat, (int)Nt, (int)Mt);
   a.transforms = w.T_cat;
-  st = run_gn(h, a, s);
-  if (st != CF_OK) return st;
-  { Timed t(h, s, kProfOther, 1); CF_TRY(launch_batch_scatter(w, h->tb, s)); }
-  if (!stats) return CF_OK;
+  st = solve_graphed(h, 1, a, s);
+  if (st != CF_OK || !stats) return st;
   return read_stats(h, stats, slot_of, num_problems, s);
 }
 

@@ -123,6 +123,11 @@ class GaussNewtonSolver:
     def set_option(self, option, value):
         check(_lib.lib().cf_gn_set_option(self._h, option, int(value)), "cf_gn_set_option")
 
+    def get_option(self, option):
+        v = ctypes.c_int()
+        check(_lib.lib().cf_gn_get_option(self._h, option, ctypes.byref(v)))
+        return v.value
+
     def set_arap_consistent(self, on=True):
         self.set_option(_lib.CF_OPT_ARAP_CONSISTENT, 1 if on else 0)
 

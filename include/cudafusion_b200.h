@@ -159,12 +159,26 @@ CF_API cf_status cf_gn_linearize_solve(cf_gn* h, const cf_correspondence* d_corr
  *                          iteration); 1: pipelined PCG, the same iterates in
  *                          exact arithmetic with one reduction per iteration
  *                          (FP64 recurrences), shared-memory grid-wide mode
- *                          only. */
+ *                          only.
+ *  CF_OPT_GRAPH            1 (default): cf_gn_solve / cf_gn_solve_batched
+ *                          run their launch sequence (binning, G x (residual,
+ *                          assembly, PCG), energy) as a CUDA graph, captured
+ *                          on the first call with given sizes, pointers of the
+ *                          node and transform arrays, parameters and options,
+ *                          replayed on later calls (new correspondence
+ *                          buffers of the same sizes replay it too).  Not used
+ *                          on the legacy default stream, while profiling, or
+ *                          when the caller is capturing `stream` itself.
+ *                          0: direct launches. */
 #define CF_OPT_ARAP_CONSISTENT 1
 #define CF_OPT_PCG_CTAS 2
 #define CF_OPT_PCG_MODE 3
 #define CF_OPT_PCG_PIPELINED 4
+#define CF_OPT_GRAPH 5
+/* read only (cf_gn_get_option): 1 when the last solve ran as a CUDA graph */
+#define CF_OPT_GRAPH_ACTIVE 6
 CF_API cf_status cf_gn_set_option(cf_gn* h, int option, int value);
+CF_API cf_status cf_gn_get_option(const cf_gn* h, int option, int* value);
 
 /* Synchronises `stream` and converts the device error flags of the last
  * solve (bounded-barrier timeout, non-finite result) into a status. */

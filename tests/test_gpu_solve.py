@@ -316,3 +316,33 @@ def test_unaligned_correspondence_array(p1, oracle):
     dxo, *_ = oracle.linearize_solve(p1.corrs, p1.nodes, p1.init_transforms,
                                      oracle.params(pcg_iterations=10, pcg_tolerance=0.0, lambda_smooth=10.0))
     assert rel(dx.cpu().numpy(), dxo) < 2e-4
+
+
+def test_graph_replay_matches_direct_launches(p1):
+    """The captured GN loop (CF_OPT_GRAPH, on a non-default stream) gives the
+    bits of direct launches, on the capturing call, on replay, and with new
+    correspondence buffers of the same sizes (replayed, not re-captured)."""
+    prm = Params(gn_iterations=3, pcg_iterations=10, pcg_tolerance=0.0, lambda_smooth=10.0)
+    side = torch.cuda.Stream()
+    dp = DeviceProblem(p1)
+    out = {}
+    for graph in (0, 1):
+        s = make_solver(prm)
+        s.set_option(_lib.CF_OPT_GRAPH, graph)
+        runs = []
+        with torch.cuda.stream(side):
+            for k in range(3):
+                if k == 2:  # new buffers holding the same correspondences
+                    dp.corrs = dp.corrs.clone()
+                    dp.canon = dp.canon.clone()
+                T = dp.init_transforms.clone()
+                n0 = s.launch_count()
+                st = s.gn_solve(dp, T, max_rot=0.12, max_trans=0.04, stream=side)
+                runs.append((T.cpu().numpy().tobytes(), st["energy_final"], s.launch_count() - n0))
+                assert s.get_option(_lib.CF_OPT_GRAPH_ACTIVE) == graph
+        side.synchronize()
+        out[graph] = runs
+    for k in range(3):
+        assert out[1][k][0] == out[0][k][0]
+        assert out[1][k][1] == out[0][k][1]
+        assert out[1][k][2] == out[0][k][2]  # the launches a replay stands for
