@@ -26,6 +26,13 @@ CF_OPT_GRAPH = 5
 CF_OPT_GRAPH_ACTIVE = 6
 CF_MAX_GN_ITERS = 32
 CF_PROF_SLOTS = 12
+CF_MPNN_IN = 20
+CF_MPNN_HIDDEN = 64
+CF_MPNN_OUT = 6
+CF_MPNN_PARAMS = 19526
+CF_MPNN_ROT_SCALE = 10.0
+CF_MPNN_TRANS_SCALE = 100.0
+CF_MPNN_RES_SCALE = 1000.0
 CF_NOALLOC_MAX_NODES = 8192
 
 # Every symbol the public header declares (the ABI test checks the list
@@ -45,6 +52,18 @@ EXPORTS = [
     "cf_gn_get_system",
     "cf_gn_solve",
     "cf_gn_solve_batched",
+    "cf_gn_last_stats",
+    "cf_mpnn_create",
+    "cf_mpnn_destroy",
+    "cf_mpnn_set_weights",
+    "cf_mpnn_get_weights",
+    "cf_mpnn_set_graph",
+    "cf_mpnn_forward",
+    "cf_mpnn_gradients",
+    "cf_mpnn_train_step",
+    "cf_dq_increments",
+    "cf_gn_features",
+    "cf_gn_solve_learned",
     "cf_energy_noalloc",
     "cf_warp_apply_twist",
     "cf_warp_skin_points",
@@ -95,6 +114,9 @@ class SolveStats(ctypes.Structure):
         ("num_blocks", ctypes.c_int),
         ("precond_fallbacks", ctypes.c_int),
         ("error_flags", ctypes.c_int),
+        ("init_rejected", ctypes.c_int),
+        ("energy_warm_start", ctypes.c_double),
+        ("energy_predicted", ctypes.c_double),
     ]
 
 
@@ -138,6 +160,19 @@ def lib():
         L.cf_gn_solve.argtypes = [vp, ctypes.POINTER(Problem), vp, ctypes.POINTER(SolveStats), vp]
         L.cf_gn_solve_batched.argtypes = [vp, ctypes.POINTER(Problem), i, ctypes.POINTER(vp),
                                           ctypes.POINTER(SolveStats), vp]
+        L.cf_gn_last_stats.argtypes = [vp, ctypes.POINTER(SolveStats), i, vp]
+        pf = ctypes.POINTER(ctypes.c_float)
+        L.cf_mpnn_create.argtypes = [i, ctypes.POINTER(vp)]
+        L.cf_mpnn_destroy.argtypes = [vp]
+        L.cf_mpnn_set_weights.argtypes = [vp, vp, i]
+        L.cf_mpnn_get_weights.argtypes = [vp, vp, i]
+        L.cf_mpnn_set_graph.argtypes = [vp, vp, i, vp]
+        L.cf_mpnn_forward.argtypes = [vp, vp, vp, vp]
+        L.cf_mpnn_gradients.argtypes = [vp, vp, vp, vp, ctypes.POINTER(ctypes.c_double), vp]
+        L.cf_mpnn_train_step.argtypes = [vp, vp, vp, f, ctypes.POINTER(ctypes.c_double), vp]
+        L.cf_dq_increments.argtypes = [vp, vp, i, vp, vp]
+        L.cf_gn_features.argtypes = [vp, ctypes.POINTER(Problem), vp, vp, vp, vp]
+        L.cf_gn_solve_learned.argtypes = [vp, vp, ctypes.POINTER(Problem), vp, vp, ctypes.POINTER(SolveStats), vp]
         L.cf_energy_noalloc.argtypes = [ctypes.POINTER(Problem), vp, f, vp, vp]
         L.cf_warp_apply_twist.argtypes = [vp, vp, i, f, f, f, vp]
         L.cf_warp_skin_points.argtypes = [vp, vp, vp, i, vp, vp, i, vp, vp]

@@ -20,6 +20,7 @@ enum ProfSlot {
   kProfPack = 0, kProfBinScan, kProfScatter, kProfExpand, kProfNodePlain, kProfResidual, kProfAssemble,
   kProfPcg, kProfEnergy, kProfTwist, kProfSkin, kProfOther
 };
+constexpr int kProfLearned = kProfTwist;  // the learned start: features, network, apply, gate
 static const char* kProfNames[CF_PROF_SLOTS] = {"pack_count", "bin_scan", "bin_scatter", "expand",
                                                 "node_plain", "residual", "assemble", "pcg",
                                                 "final_energy", "apply_twist", "skin_points", "other"};
@@ -51,6 +52,9 @@ struct cf_gn {
   long long graph_launches = 0;
   bool graph_key_failed = false;
   int graph_last = 0;  // the last solve ran as a graph
+  // learned solve: the network and the transform history of the call being enqueued
+  Mpnn* learn_net = nullptr;
+  const cf_dual_quat* learn_hist = nullptr;
   DevStats* h_stats = nullptr;   // pinned, [kMaxProblems]
   // problem table: host copies (to skip unchanged uploads) and device arrays
   std::vector<ProbDesc> h_desc;
@@ -778,6 +782,9 @@ cf_status read_stats(cf_gn* h, cf_solve_stats* stats, const std::vector<int>& sl
     out->num_blocks = h->p.nnzb;
     out->precond_fallbacks = d.fallbacks;
     out->error_flags = herr;
+    out->energy_warm_start = d.gate[0];
+    out->energy_predicted = d.gate[1];
+    out->init_rejected = d.init_rejected;
   }
   if (herr & kErrTimeoutBit) return CF_ERR_TIMEOUT;
   if (herr & kErrNonFiniteBit) return CF_ERR_NON_FINITE;
@@ -797,6 +804,23 @@ cf_status enqueue_solve(cf_gn* h, int kind, SolveArgs& a, cudaStream_t s) {
   }
   cf_status st = bin_correspondences(h, s);
   if (st != CF_OK) return st;
+  if (kind == 2) {
+    // learned start: features at the warm start, the network's increment,
+    // kept only if it lowers the energy (the plain warm start otherwise)
+    Mpnn& net = *h->learn_net;
+    { Timed t(h, s, kProfNodePlain, 1); CF_TRY(launch_node_plain(w, a.nodes, a.transforms, a.N, s)); }
+    { Timed t(h, s, kProfResidual, 1); CF_TRY(launch_residual(w, h->tb, h->p, a, a.transforms, true, s)); }
+    {
+      Timed t(h, s, kProfLearned, 6);
+      CF_TRY(launch_features(w, a.transforms, h->learn_hist, a.N, net.feat, s));
+      CF_TRY(mpnn_graph_from_nodes(net, a.nodes, a.N, s));
+      CF_TRY(mpnn_forward(net, net.feat, net.out, s));
+    }
+    { Timed t(h, s, kProfEnergy, 2); CF_TRY(launch_final_energy(w, h->p, a, -1, s)); }
+    { Timed t(h, s, kProfLearned, 1); CF_TRY(launch_apply_prediction(w, a.transforms, a.nodes, net.out, a.N, s)); }
+    { Timed t(h, s, kProfEnergy, 2); CF_TRY(launch_final_energy(w, h->p, a, -2, s)); }
+    { Timed t(h, s, kProfLearned, 1); CF_TRY(launch_gate_prediction(w, a.transforms, a.nodes, a.N, s)); }
+  }
   st = run_gn(h, a, s);
   if (st != CF_OK) return st;
   if (kind == 1) {
@@ -817,8 +841,11 @@ cf_status solve_graphed(cf_gn* h, int kind, SolveArgs& a, cudaStream_t s) {
   if (!h->use_graph || h->profile || s == nullptr || cudaStreamIsCapturing(s, &cs) != cudaSuccess ||
       cs != cudaStreamCaptureStatusNone)
     return enqueue_solve(h, kind, a, s);
-  std::vector<unsigned char> key(sizeof(int) * 2 + sizeof(unsigned) + sizeof(cf_gn_params) + sizeof(SolveArgs));
+  std::vector<unsigned char> key(sizeof(int) * 2 + sizeof(unsigned) + sizeof(cf_gn_params) + sizeof(SolveArgs) +
+                                 2 * sizeof(void*));
   unsigned char* k = key.data();
+  const void* lp[2] = {kind == 2 ? (const void*)h->learn_net : nullptr, kind == 2 ? (const void*)h->learn_hist : nullptr};
+  memcpy(k, lp, sizeof(lp)); k += sizeof(lp);
   memcpy(k, &kind, sizeof(int)); k += sizeof(int);
   memcpy(k, &h->tb.P, sizeof(int)); k += sizeof(int);
   memcpy(k, &h->pattern_version, sizeof(unsigned)); k += sizeof(unsigned);
@@ -1094,6 +1121,209 @@ cf_status cf_gn_solve_batched(cf_gn* h, const cf_problem* problems, int num_prob
   st = solve_graphed(h, 1, a, s);
   if (st != CF_OK || !stats) return st;
   return read_stats(h, stats, slot_of, num_problems, s);
+}
+
+// ---- learned initial increment ------------------------------------------
+
+struct cf_mpnn {
+  Mpnn m;
+};
+
+cf_status cf_mpnn_create(int max_nodes, cf_mpnn** out) {
+  if (!out || max_nodes <= 0) return CF_ERR_INVALID_ARG;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return CF_ERR_NO_DEVICE;
+  cf_mpnn* n = new cf_mpnn();
+  cudaError_t e = mpnn_alloc(n->m, max_nodes);
+  if (e == cudaSuccess) e = cudaMemset(n->m.w, 0, sizeof(float) * CF_MPNN_PARAMS);
+  if (e == cudaSuccess) e = mpnn_refresh_bf16(n->m, nullptr);
+  if (e != cudaSuccess) {
+    mpnn_free(n->m);
+    delete n;
+    return from_cuda(e);
+  }
+  *out = n;
+  return CF_OK;
+}
+
+cf_status cf_mpnn_destroy(cf_mpnn* net) {
+  if (!net) return CF_ERR_INVALID_ARG;
+  cudaDeviceSynchronize();
+  mpnn_free(net->m);
+  delete net;
+  return CF_OK;
+}
+
+cf_status cf_mpnn_set_weights(cf_mpnn* net, const float* h_params, int n) {
+  if (!net || !h_params || n != CF_MPNN_PARAMS) return CF_ERR_INVALID_ARG;
+  Mpnn& m = net->m;
+  CF_TRY(cudaMemcpy(m.w, h_params, sizeof(float) * n, cudaMemcpyHostToDevice));
+  CF_TRY(cudaMemset(m.m, 0, sizeof(float) * n));
+  CF_TRY(cudaMemset(m.v, 0, sizeof(float) * n));
+  m.step = 0;
+  CF_TRY(mpnn_refresh_bf16(m, nullptr));
+  CF_TRY(cudaDeviceSynchronize());
+  return CF_OK;
+}
+
+cf_status cf_mpnn_get_weights(cf_mpnn* net, float* h_params, int n) {
+  if (!net || !h_params || n != CF_MPNN_PARAMS) return CF_ERR_INVALID_ARG;
+  CF_TRY(cudaMemcpy(h_params, net->m.w, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  return CF_OK;
+}
+
+cf_status cf_mpnn_set_graph(cf_mpnn* net, const int* d_nbr, int num_nodes, void* stream) {
+  if (!net || num_nodes < 0 || (num_nodes > 0 && !d_nbr)) return CF_ERR_INVALID_ARG;
+  Mpnn& m = net->m;
+  if (num_nodes > m.max_nodes) return CF_ERR_CAPACITY;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int N = num_nodes;
+  std::vector<int> nbr((size_t)N * CF_K_GRAPH);
+  if (N) CF_TRY(cudaMemcpyAsync(nbr.data(), d_nbr, sizeof(int) * nbr.size(), cudaMemcpyDeviceToHost, s));
+  CF_TRY(cudaStreamSynchronize(s));
+  std::vector<float> inv_deg(std::max(1, N), 0.f);
+  std::vector<int> rev_ptr(N + 1, 0), rev_idx;
+  for (int i = 0; i < N; i++) {
+    int deg = 0;
+    for (int k = 0; k < CF_K_GRAPH; k++) {
+      int& j = nbr[(size_t)i * CF_K_GRAPH + k];
+      if (j < 0 || j >= N) j = -1;
+      if (j >= 0) {
+        deg++;
+        rev_ptr[j + 1]++;
+      }
+    }
+    inv_deg[i] = deg ? 1.f / (float)deg : 0.f;
+  }
+  for (int j = 0; j < N; j++) rev_ptr[j + 1] += rev_ptr[j];
+  rev_idx.assign(std::max(1, rev_ptr[N]), 0);
+  {
+    std::vector<int> fill(rev_ptr.begin(), rev_ptr.end() - 1);
+    for (int i = 0; i < N; i++)
+      for (int k = 0; k < CF_K_GRAPH; k++) {
+        const int j = nbr[(size_t)i * CF_K_GRAPH + k];
+        if (j >= 0) rev_idx[fill[j]++] = i;
+      }
+  }
+  if (N) {
+    CF_TRY(cudaMemcpy(m.nbr, nbr.data(), sizeof(int) * nbr.size(), cudaMemcpyHostToDevice));
+    CF_TRY(cudaMemcpy(m.inv_deg, inv_deg.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
+    CF_TRY(cudaMemcpy(m.rev_ptr, rev_ptr.data(), sizeof(int) * (N + 1), cudaMemcpyHostToDevice));
+    CF_TRY(cudaMemcpy(m.rev_idx, rev_idx.data(), sizeof(int) * rev_idx.size(), cudaMemcpyHostToDevice));
+  }
+  m.N = N;
+  return CF_OK;
+}
+
+cf_status cf_mpnn_forward(cf_mpnn* net, const float* d_features, float* d_out, void* stream) {
+  if (!net || !d_features || !d_out) return CF_ERR_INVALID_ARG;
+  CF_TRY(mpnn_forward(net->m, d_features, d_out, (cudaStream_t)stream));
+  return CF_OK;
+}
+
+cf_status cf_mpnn_gradients(cf_mpnn* net, const float* d_features, const float* d_targets, float* h_grad,
+                            double* h_loss, void* stream) {
+  if (!net || !d_features || !d_targets) return CF_ERR_INVALID_ARG;
+  Mpnn& m = net->m;
+  cudaStream_t s = (cudaStream_t)stream;
+  CF_TRY(mpnn_gradients(m, d_features, d_targets, s));
+  if (h_grad) CF_TRY(cudaMemcpyAsync(h_grad, m.g, sizeof(float) * CF_MPNN_PARAMS, cudaMemcpyDeviceToHost, s));
+  if (h_loss) CF_TRY(cudaMemcpyAsync(h_loss, m.loss, sizeof(double), cudaMemcpyDeviceToHost, s));
+  CF_TRY(cudaStreamSynchronize(s));
+  return CF_OK;
+}
+
+cf_status cf_mpnn_train_step(cf_mpnn* net, const float* d_features, const float* d_targets, float lr,
+                             double* h_loss, void* stream) {
+  if (!net || !d_features || !d_targets || !(lr >= 0.f)) return CF_ERR_INVALID_ARG;
+  Mpnn& m = net->m;
+  cudaStream_t s = (cudaStream_t)stream;
+  CF_TRY(mpnn_gradients(m, d_features, d_targets, s));
+  CF_TRY(mpnn_adam(m, lr, s));
+  if (h_loss) {
+    CF_TRY(cudaMemcpyAsync(h_loss, m.loss, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CF_TRY(cudaStreamSynchronize(s));
+  }
+  return CF_OK;
+}
+
+cf_status cf_dq_increments(const cf_dual_quat* d_to, const cf_dual_quat* d_from, int n, float* d_out, void* stream) {
+  if (n < 0 || (n > 0 && (!d_to || !d_from || !d_out))) return CF_ERR_INVALID_ARG;
+  if ((reinterpret_cast<uintptr_t>(d_to) | reinterpret_cast<uintptr_t>(d_from)) & 15u) return CF_ERR_INVALID_ARG;
+  CF_TRY(launch_increments(d_to, d_from, n, d_out, (cudaStream_t)stream));
+  return CF_OK;
+}
+
+namespace {
+cf_status check_problem(cf_gn* h, const cf_problem* prob, const void* d_T) {
+  if (!h || !prob || prob->num_nodes < 0 || prob->num_corrs < 0) return CF_ERR_INVALID_ARG;
+  if (prob->num_nodes > h->max_nodes || prob->num_corrs > h->max_corrs) return CF_ERR_CAPACITY;
+  if (prob->num_nodes == 0) return CF_OK;
+  if (!prob->nodes || !d_T || (prob->num_corrs > 0 && (!prob->corrs || !prob->canon_points))) return CF_ERR_INVALID_ARG;
+  if ((reinterpret_cast<uintptr_t>(prob->corrs) & 3u) || (reinterpret_cast<uintptr_t>(d_T) & 15u))
+    return CF_ERR_INVALID_ARG;
+  return CF_OK;
+}
+}  // namespace
+
+cf_status cf_gn_features(cf_gn* h, const cf_problem* prob, const cf_dual_quat* d_transforms,
+                         const cf_dual_quat* d_history, float* d_features, void* stream) {
+  cf_status st = check_problem(h, prob, d_transforms);
+  if (st != CF_OK || prob->num_nodes == 0) return st;
+  if (!d_history || !d_features || (reinterpret_cast<uintptr_t>(d_history) & 15u)) return CF_ERR_INVALID_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int N = prob->num_nodes, M = prob->num_corrs;
+  if ((st = ensure_pattern(h, prob->nodes, N, s)) != CF_OK) return st;
+  if ((st = prepare_table(h, {make_desc(prob->corrs, prob->canon_points, prob->nodes,
+                                        const_cast<cf_dual_quat*>(d_transforms), M, N, 0.f, 0.f, 1.f)},
+                          true, s)) != CF_OK)
+    return st;
+  Work& w = h->w;
+  CF_TRY(cudaMemsetAsync(w.err, 0, sizeof(int), s));
+  if ((st = bin_correspondences(h, s)) != CF_OK) return st;
+  SolveArgs a = make_args(h, prob->nodes, N, M);
+  CF_TRY(launch_node_plain(w, prob->nodes, d_transforms, N, s));
+  CF_TRY(launch_residual(w, h->tb, h->p, a, d_transforms, true, s));
+  CF_TRY(launch_features(w, d_transforms, d_history, N, d_features, s));
+  return CF_OK;
+}
+
+cf_status cf_gn_solve_learned(cf_gn* h, cf_mpnn* net, const cf_problem* prob, cf_dual_quat* d_transforms,
+                              const cf_dual_quat* d_history, cf_solve_stats* stats, void* stream) {
+  if (!net) return CF_ERR_INVALID_ARG;
+  if (stats) memset(stats, 0, sizeof(*stats));
+  cf_status st = check_problem(h, prob, d_transforms);
+  if (st != CF_OK || prob->num_nodes == 0) return st;
+  if (!d_history || (reinterpret_cast<uintptr_t>(d_history) & 15u)) return CF_ERR_INVALID_ARG;
+  const int N = prob->num_nodes, M = prob->num_corrs;
+  if (N > net->m.max_nodes) return CF_ERR_CAPACITY;
+  cudaStream_t s = (cudaStream_t)stream;
+  if ((st = ensure_pattern(h, prob->nodes, N, s)) != CF_OK) return st;
+  if ((st = prepare_table(h, {make_desc(prob->corrs, prob->canon_points, prob->nodes, d_transforms, M, N,
+                                        prob->max_rot, prob->max_trans, prob->update_scale)},
+                          true, s)) != CF_OK)
+    return st;
+  Work& w = h->w;
+  if (!w.T_save) CF_TRY(dalloc(&w.T_save, (size_t)w.max_nodes));
+  SolveArgs a = make_args(h, prob->nodes, N, M);
+  a.transforms = d_transforms;
+  a.max_rot = prob->max_rot;
+  a.max_trans = prob->max_trans;
+  a.update_scale = prob->update_scale;
+  h->learn_net = &net->m;
+  h->learn_hist = d_history;
+  net->m.N = N;
+  st = solve_graphed(h, 2, a, s);
+  if (st != CF_OK || !stats) return st;
+  return read_stats(h, stats, {0}, 1, s);
+}
+
+cf_status cf_gn_last_stats(cf_gn* h, cf_solve_stats* stats, int num, void* stream) {
+  if (!h || !stats || num < 1) return CF_ERR_INVALID_ARG;
+  std::vector<int> slots(num, -1);
+  for (int q = 0; q < num && q < h->tb.P; q++) slots[q] = q;
+  return read_stats(h, stats, slots, num, (cudaStream_t)stream);
 }
 
 cf_status cf_gn_profile_enable(cf_gn* h, int on) {

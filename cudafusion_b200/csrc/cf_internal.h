@@ -23,7 +23,8 @@ struct DevStats {
   double pcg_res[CF_MAX_GN_ITERS];     // final ||r|| per GN iteration
   int pcg_iters[CF_MAX_GN_ITERS];
   int fallbacks;                        // Cholesky fallbacks of the last GN iteration
-  int pad_;
+  int init_rejected;                    // learned solve: the predicted start was not kept
+  double gate[2];                       // learned solve: energy at the warm start, at the prediction
 };
 
 // One problem of a solve as the kernels see it; a single solve is a batch of
@@ -148,6 +149,7 @@ struct Work {
   float* r = nullptr;       // [6*max_nodes]
   float* ap = nullptr;      // [6*max_nodes]
   float* minv32 = nullptr;  // [36*max_nodes]
+  cf_dual_quat* T_save = nullptr;  // [max_nodes] learned solve: the warm start
   // batched solves: the problems' nodes and transforms, concatenated
   cf_deform_node* nodes_cat = nullptr;  // [max_nodes]
   cf_dual_quat* T_cat = nullptr;        // [max_nodes]
@@ -207,6 +209,36 @@ int expand_smem_bytes(int max_upper_row);
 int pcg_cluster_smem_bytes(int nup_max, int nlow_max, int rows_max, int C, bool a_in_smem);
 int pcg_cluster_max_active(int C, int smem, bool a_in_smem);
 cudaError_t launch_pcg_cluster(const Work& w, const Pattern& p, const SolveArgs& a, int gn_slot, cudaStream_t s);
+
+// The learned initial increment (cf_mpnn.cu): parameters, graph, activations.
+struct Mpnn {
+  int max_nodes = 0, N = 0;
+  long long step = 0;
+  float *w = nullptr, *m = nullptr, *v = nullptr, *g = nullptr;  // FP32 master, Adam moments, gradient
+  void* wb = nullptr;                                            // BF16 parameters
+  int* nbr = nullptr;       // [N][8] neighbour lists, -1 = none
+  float* inv_deg = nullptr;  // [N]
+  int *rev_ptr = nullptr, *rev_idx = nullptr;  // reverse graph (training)
+  float *feat = nullptr, *tgt = nullptr, *out = nullptr;
+  void *h1 = nullptr, *h2 = nullptr, *h3 = nullptr;  // BF16 activations [N][64]
+  float *dh = nullptr, *dh2 = nullptr, *dcat = nullptr, *part = nullptr;
+  double *loss_part = nullptr, *loss = nullptr;
+};
+int mpnn_param_count();
+cudaError_t mpnn_alloc(Mpnn& m, int max_nodes);
+void mpnn_free(Mpnn& m);
+cudaError_t mpnn_refresh_bf16(const Mpnn& m, cudaStream_t s);
+cudaError_t mpnn_graph_from_nodes(Mpnn& m, const cf_deform_node* nodes, int N, cudaStream_t s);
+cudaError_t mpnn_forward(const Mpnn& m, const float* feat, float* out, cudaStream_t s);
+cudaError_t mpnn_gradients(Mpnn& m, const float* feat, const float* tgt, cudaStream_t s);
+cudaError_t mpnn_adam(Mpnn& m, float lr, cudaStream_t s);
+cudaError_t launch_increments(const cf_dual_quat* to, const cf_dual_quat* from, int n, float* out, cudaStream_t s);
+cudaError_t launch_features(const Work& w, const cf_dual_quat* T, const cf_dual_quat* hist, int N, float* feat,
+                            cudaStream_t s);
+cudaError_t launch_apply_prediction(const Work& w, cf_dual_quat* T, const cf_deform_node* nodes, const float* pred,
+                                    int N, cudaStream_t s);
+cudaError_t launch_gate_prediction(const Work& w, cf_dual_quat* T, const cf_deform_node* nodes, int N,
+                                   cudaStream_t s);
 
 int pcg_stream_smem_bytes();
 int pcg_stream_tile_blocks();

@@ -403,8 +403,12 @@ __global__ void energy_reduce_kernel(Table tb, Work w, int slot) {
   for (int k = threadIdx.x; k < d.e_ctas; k += 32) v += w.e_data_part[d.e_cta0 + k];
   v = warp_sum_d(v);
   if (threadIdx.x == 0) {
-    w.stats[blockIdx.x].energy[slot] = v;
-    if (!isfinite(v)) atomicOr(w.err, kErrNonFinite);
+    if (slot >= 0) {
+      w.stats[blockIdx.x].energy[slot] = v;
+      if (!isfinite(v)) atomicOr(w.err, kErrNonFinite);
+    } else {
+      w.stats[blockIdx.x].gate[-slot - 1] = v;  // energies compared by the learned solve's gate
+    }
   }
 }
 

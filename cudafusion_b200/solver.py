@@ -208,6 +208,16 @@ class GaussNewtonSolver:
             ))
         return res
 
+    def last_stats(self, stream=None):
+        """Statistics of the handle's last solve (cf_gn_last_stats)."""
+        s = _lib.SolveStats()
+        check(_lib.lib().cf_gn_last_stats(self._h, ctypes.byref(s), 1, _stream_ptr(stream)), "cf_gn_last_stats")
+        G = s.gn_iterations_run
+        return dict(energy_initial=s.energy_initial, energy_final=s.energy_final,
+                    energy=[s.energy_per_iter[g] for g in range(G + 1)], init_rejected=s.init_rejected,
+                    energy_warm_start=s.energy_warm_start, energy_predicted=s.energy_predicted,
+                    pcg_iterations=[s.pcg_iterations[g] for g in range(G)], error_flags=s.error_flags)
+
     def profile_enable(self, on=True):
         """Per-phase CUDA-event timing of every launch (resets totals)."""
         check(_lib.lib().cf_gn_profile_enable(self._h, 1 if on else 0))

@@ -41,6 +41,14 @@ extern "C" {
 #define CF_BLOCK_SIZE 36 /* include/types.h:213 */
 #define CF_MAX_GN_ITERS 32
 #define CF_MAX_NODES_DEFAULT 8192 /* WarpField::MAX_NODES, include/warp_field.h:14 */
+/* learned initial increment (no reference counterpart) */
+#define CF_MPNN_IN 20
+#define CF_MPNN_HIDDEN 64
+#define CF_MPNN_OUT 6
+#define CF_MPNN_PARAMS 19526
+#define CF_MPNN_ROT_SCALE 10.0f     /* rotation-vector features: rad x 10 */
+#define CF_MPNN_TRANS_SCALE 100.0f  /* translation features: m x 100 (cm) */
+#define CF_MPNN_RES_SCALE 1000.0f   /* residual features: m x 1000 (mm) */
 
 /* ------------------------------------------------------------------------ */
 /* Byte-compatible mirrors of the reference structs (include/types.h).       */
@@ -207,6 +215,9 @@ typedef struct cf_solve_stats {
   int num_blocks;          /* nnzb of the block pattern */
   int precond_fallbacks;   /* diagonal blocks whose Cholesky failed (last GN it.) */
   int error_flags;         /* bit 0: barrier timeout, bit 1: non-finite */
+  int init_rejected;       /* learned solve: 1 when the predicted start was not kept */
+  double energy_warm_start; /* learned solve: E at the warm start */
+  double energy_predicted;  /* learned solve: E at the network's predicted start */
 } cf_solve_stats;
 
 /* One problem of the multi-iteration solve.  The correspondences carry the
@@ -233,6 +244,11 @@ CF_API cf_status cf_gn_solve(cf_gn* h, const cf_problem* problem,
                       cf_dual_quat* d_transforms, cf_solve_stats* stats,
                       void* stream);
 
+/* Statistics of the handle's last solve, read without running it again
+ * (for a caller that ran it with stats = NULL): `num` records in the order of
+ * the solve's non-empty problems.  Synchronises `stream`. */
+CF_API cf_status cf_gn_last_stats(cf_gn* h, cf_solve_stats* stats, int num, void* stream);
+
 /* Batched solve (no counterpart in the reference, which solves one warp
  * field per call): num_problems independent problems of uneven size, each
  * with its own graph, correspondences, clamps and transforms
@@ -258,6 +274,59 @@ CF_API cf_status cf_gn_profile_enable(cf_gn* h, int on);
 CF_API cf_status cf_gn_profile_read(cf_gn* h, double* ms, int* launches, int n_slots);
 CF_API const char* cf_gn_profile_name(int slot);
 CF_API cf_status cf_gn_launch_count(const cf_gn* h, long long* launches);
+
+/* ------------------------------------------------------------------------ */
+/* Learned initial increment (no counterpart in the reference, whose every   */
+/* frame starts GN from a zero increment).                                    */
+/* ------------------------------------------------------------------------ */
+
+/* A message-passing network over the deformation graph that predicts each
+ * node's increment for the coming frame: 3 layers (each node's features with
+ * the mean of its graph neighbours'), hidden 64, BF16 parameters and
+ * activations, FP32 accumulation; output = the last frame's increment plus a
+ * learned correction.  Features per node (CF_MPNN_IN = 20): the increments
+ * (rotation vector x CF_MPNN_ROT_SCALE, translation x CF_MPNN_TRANS_SCALE) of
+ * the last three frames, and the mean and max |residual| (x CF_MPNN_RES_SCALE)
+ * of the node's correspondences at the warm start.  Parameters: a flat FP32
+ * vector of CF_MPNN_PARAMS (W0 [64][40], b0, W1 [64][128], b1, W2 [64][128],
+ * b2, Wo [6][64], bo).  Created with zero parameters (the prediction is then
+ * the last frame's increment). */
+typedef struct cf_mpnn cf_mpnn;
+CF_API cf_status cf_mpnn_create(int max_nodes, cf_mpnn** out);
+CF_API cf_status cf_mpnn_destroy(cf_mpnn* net);
+/* Sets the FP32 parameters (n = CF_MPNN_PARAMS) and resets the optimiser. */
+CF_API cf_status cf_mpnn_set_weights(cf_mpnn* net, const float* h_params, int n);
+CF_API cf_status cf_mpnn_get_weights(cf_mpnn* net, float* h_params, int n);
+/* The graph for forward / training: d_nbr [num_nodes][CF_K_GRAPH] neighbour
+ * indices, -1 = none (synchronises; builds the reverse graph on the host). */
+CF_API cf_status cf_mpnn_set_graph(cf_mpnn* net, const int* d_nbr, int num_nodes, void* stream);
+/* d_out [N][6] = the predicted increments in feature units. */
+CF_API cf_status cf_mpnn_forward(cf_mpnn* net, const float* d_features, float* d_out, void* stream);
+/* Loss = mean squared error against d_targets [N][6] (feature units), its
+ * gradient into h_grad [CF_MPNN_PARAMS] (either may be NULL); synchronises. */
+CF_API cf_status cf_mpnn_gradients(cf_mpnn* net, const float* d_features, const float* d_targets,
+                                   float* h_grad, double* h_loss, void* stream);
+/* One Adam step (learning rate lr) on the loss above; h_loss may be NULL
+ * (then no synchronisation). */
+CF_API cf_status cf_mpnn_train_step(cf_mpnn* net, const float* d_features, const float* d_targets,
+                                    float lr, double* h_loss, void* stream);
+/* Per node the increment (rotation vector, translation) taking d_from to
+ * d_to: d_to = D (x) d_from, as centred DQs of the same node; d_out [n][6]. */
+CF_API cf_status cf_dq_increments(const cf_dual_quat* d_to, const cf_dual_quat* d_from, int n,
+                                  float* d_out, void* stream);
+/* The network's features of `problem` at the warm start d_transforms
+ * (= T_{t-1}) with d_history = [T_{t-2}, T_{t-3}, T_{t-4}] (3 x num_nodes
+ * DQs); d_features [num_nodes][CF_MPNN_IN]. */
+CF_API cf_status cf_gn_features(cf_gn* h, const cf_problem* problem, const cf_dual_quat* d_transforms,
+                                const cf_dual_quat* d_history, float* d_features, void* stream);
+/* cf_gn_solve from a learned start: features, the network's increment
+ * applied to the warm start, kept only if its energy is below the warm
+ * start's (stats->init_rejected otherwise: the plain warm start is used),
+ * then params.gn_iterations GN iterations.  Runs as one CUDA graph like
+ * cf_gn_solve. */
+CF_API cf_status cf_gn_solve_learned(cf_gn* h, cf_mpnn* net, const cf_problem* problem,
+                                     cf_dual_quat* d_transforms, const cf_dual_quat* d_history,
+                                     cf_solve_stats* stats, void* stream);
 
 /* Allocation-free energy (no counterpart in the reference).
  *
