@@ -82,3 +82,30 @@ def test_live_reference_random(oracle):
         T = oracle.exp_se3(tw)
         o = oracle.mat4_to_dq(T)
         assert np.array_equal(bits(np.array([o], DQ_DTYPE)), bits(r))
+
+
+def test_mpnn_oracle_gradient_matches_finite_differences():
+    """The FP64 network oracle's analytic gradient (the checker of the BF16
+    kernels) against central differences of its own loss."""
+    import mpnn_oracle as O
+
+    rng = np.random.default_rng(0)
+    N = 40
+    nbr = rng.integers(-1, N, size=(N, 8))
+    x = rng.normal(size=(N, O.IN))
+    tgt = rng.normal(size=(N, O.OUT))
+    th = rng.normal(size=O.PARAMS) * 0.2
+    _, g = O.loss_and_grad(th, x, tgt, nbr, rounding=False)
+    idx = rng.choice(O.PARAMS, 40, replace=False)
+    fd = O.finite_differences(th, x, tgt, nbr, idx)
+    assert np.abs(fd - g[idx]).max() < 1e-6 * max(1.0, np.abs(g[idx]).max())
+
+
+def test_mpnn_oracle_bf16_rounding():
+    import mpnn_oracle as O
+
+    v = np.array([1.0, 1.00390625, 1.005859375, -3.14159, 65504.0, 1e-3])
+    r = O.bf16(v)
+    assert r[0] == 1.0 and r[1] == 1.0  # halfway rounds to even
+    assert r[2] == 1.0078125
+    assert np.all(np.abs(r - v) <= np.abs(v) * 2 ** -8)
