@@ -226,6 +226,67 @@ def learned_comparison(frames=300):
     }
 
 
+def precision_study():
+    """The 1280x960 frame (N=8192, M~1.22M): the GPU solve and the FP32
+    reference-order oracle against the FP64 oracle (per node-transform
+    component and per GN energy), and the assembly / PCG bandwidth at that
+    size (event-timed launches, algorithmic bytes of the workload model)."""
+    import numpy as np
+    import torch
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    from cudafusion_b200 import synth
+    from cudafusion_b200.solver import DeviceProblem, GaussNewtonSolver, Params
+    from cudafusion_b200.types import DQ_DTYPE, dq_as_array
+
+    kw = dict(gn_iterations=5, pcg_iterations=20, pcg_tolerance=1e-4, lambda_smooth=10.0, lambda_damping=1.0)
+    p = synth.config3()
+    O.lib().cfo_set_arap_consistent(1)
+    try:
+        T64, E64, _ = O.gn_solve(p, O.params(**kw), MAX_ROT, MAX_TRANS, precision="f64", nthreads=os.cpu_count())
+        T32, E32, _ = O.gn_solve(p, O.params(**kw), MAX_ROT, MAX_TRANS, precision="f32", nthreads=os.cpu_count())
+    finally:
+        O.lib().cfo_set_arap_consistent(0)
+    s = GaussNewtonSolver(Params(**kw), max_nodes=p.num_nodes, max_corrs=p.num_corrs)
+    s.set_arap_consistent(True)
+    dp = DeviceProblem(p)
+    T = dp.init_transforms.clone()
+    st = s.gn_solve(dp, T, MAX_ROT, MAX_TRANS)
+    Tg = dq_as_array(T.cpu().numpy().view(DQ_DTYPE))
+    T64, T32 = dq_as_array(T64), dq_as_array(T32)
+    s.profile_enable(True)
+    for _ in range(5):
+        T.copy_(dp.init_transforms)
+        s.gn_solve(dp, T, MAX_ROT, MAX_TRANS, stats=False)
+    torch.cuda.synchronize()
+    ph = s.profile_read()
+    pcg_used = sum(st["pcg_iterations"]) / len(st["pcg_iterations"])
+    ab = algorithmic_bytes(p.num_nodes, p.num_corrs, st["num_blocks"], pcg_used)
+    asm_ms = ph["assemble"][0] / ph["assemble"][1]
+    pcg_ms = ph["pcg"][0] / ph["pcg"][1]
+    hbm, _ = peaks()
+    e_rel = lambda E: float(max(abs(a - b) / abs(b) for a, b in zip(E, E64)))  # noqa: E731
+    return {
+        "workload": f"two-cylinder 1280x960 frame, N={p.num_nodes}, M={p.num_corrs}, 5 GN x 20 PCG, "
+                    "lambda_smooth 10, lambda_damping 1.0, consistent ARAP Jacobian",
+        "gpu_transform_err_max": float(np.abs(Tg - T64).max()),
+        "gpu_transform_err_rms": float(np.sqrt(np.mean((Tg - T64) ** 2))),
+        "fp32_oracle_transform_err_max": float(np.abs(T32 - T64).max()),
+        "gpu_energy_rel_err_max": e_rel(st["energy"]),
+        "fp32_oracle_energy_rel_err_max": e_rel(E32),
+        "energy_final_fp64": float(E64[-1]),
+        "assembly_gbs": ab["assembly"] / (asm_ms * 1e-3) / 1e9,
+        "pcg_gbs": ab["pcg"] / (pcg_ms * 1e-3) / 1e9,
+        "assembly_frac_of_measured_hbm": ab["assembly"] / (asm_ms * 1e-3) / 1e9 / hbm,
+        "pcg_frac_of_measured_hbm": ab["pcg"] / (pcg_ms * 1e-3) / 1e9 / hbm,
+        "assembly_ms": asm_ms,
+        "pcg_ms_per_launch": pcg_ms,
+        "note": "assembly and the PCG system fit the 126 MB L2 at this size; the fractions use the HBM copy peak",
+    }
+
+
 def run_b200(args, world, rank, local):
     import torch
 
@@ -345,6 +406,7 @@ def run_b200(args, world, rank, local):
     nthreads = os.cpu_count() or 1
     cpu = cpu_baseline(problem, nthreads) if not args.no_cpu_baseline else None
     learned = None if args.no_learned else learned_comparison()
+    precision = None if args.no_precision else precision_study()
     line = {
         "metric": METRIC,
         "value": value,
@@ -374,6 +436,7 @@ def run_b200(args, world, rank, local):
         "gpu_launches_per_step": launches / args.steps,
         "cuda_graph": bool(graphed),
         "learned": learned,
+        "precision": precision,
         "clocks": clocks,
         "energy_initial": stats["energy_initial"],
         "energy_final": stats["energy_final"],
@@ -476,6 +539,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-start comparison")
+    ap.add_argument("--no-precision", action="store_true", help="skip the 8192-node precision study")
     ap.add_argument("--pcg-mode", type=int, default=0, help="0 auto, 1 grid-wide, 2 single cluster")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

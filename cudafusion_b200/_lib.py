@@ -24,6 +24,8 @@ CF_OPT_PCG_MODE = 3
 CF_OPT_PCG_PIPELINED = 4
 CF_OPT_GRAPH = 5
 CF_OPT_GRAPH_ACTIVE = 6
+CF_OPT_SPIN_LIMIT = 7
+CF_OPT_TEST_BARRIER_EXTRA = 8
 CF_MAX_GN_ITERS = 32
 CF_PROF_SLOTS = 12
 CF_MPNN_IN = 20

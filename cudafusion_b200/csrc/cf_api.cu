@@ -39,6 +39,8 @@ struct cf_gn {
   int pcg_mode = 0;  // 0 auto, 1 grid-wide cooperative, 2 single cluster
   int pcg_pipelined = 0;
   int phase_timers = 0;
+  unsigned spin_limit = 1u << 22;
+  unsigned bar_extra = 0;
   Work w;
   Pattern p;
   bool pattern_valid = false;
@@ -715,7 +717,8 @@ SolveArgs make_args(const cf_gn* h, const cf_deform_node* nodes, int N, int M) {
   a.pcg_iterations = std::max(0, h->params.pcg_iterations);
   a.pcg_tolerance = h->params.pcg_tolerance;
   a.arap_consistent = h->arap_consistent;
-  a.spin_limit = 1u << 22;
+  a.spin_limit = h->spin_limit;
+  a.bar_extra = h->bar_extra;
   a.timers = h->phase_timers ? h->w.timers : nullptr;
   a.tb = h->tb;
   return a;
@@ -998,6 +1001,14 @@ cf_status cf_gn_set_option(cf_gn* h, int option, int value) {
     case CF_OPT_GRAPH:
       h->use_graph = value ? 1 : 0;
       return CF_OK;
+    case CF_OPT_SPIN_LIMIT:
+      if (value < 0) return CF_ERR_INVALID_ARG;
+      h->spin_limit = value ? (unsigned)value : (1u << 22);
+      return CF_OK;
+    case CF_OPT_TEST_BARRIER_EXTRA:
+      if (value < 0) return CF_ERR_INVALID_ARG;
+      h->bar_extra = (unsigned)value;
+      return CF_OK;
     case CF_OPT_PCG_CTAS:
       if (value < 0 || value > kMaxPcgCtas) return CF_ERR_INVALID_ARG;
       h->pcg_ctas_override = value;
@@ -1016,6 +1027,8 @@ cf_status cf_gn_get_option(const cf_gn* h, int option, int* value) {
     case CF_OPT_PCG_PIPELINED: *value = h->pcg_pipelined; return CF_OK;
     case CF_OPT_GRAPH: *value = h->use_graph; return CF_OK;
     case CF_OPT_GRAPH_ACTIVE: *value = h->graph_last; return CF_OK;
+    case CF_OPT_SPIN_LIMIT: *value = (int)h->spin_limit; return CF_OK;
+    case CF_OPT_TEST_BARRIER_EXTRA: *value = (int)h->bar_extra; return CF_OK;
   }
   return CF_ERR_INVALID_ARG;
 }

@@ -175,6 +175,7 @@ struct SolveArgs {
   float* delta_x;            // non-null: write dx here and do not update
   float max_rot, max_trans, update_scale;
   unsigned spin_limit;
+  unsigned bar_extra;  // test hook: arrivals every group barrier waits for beyond its CTAs (0)
   long long* timers;  // non-null: CTA 0 of the grid PCG accumulates phase cycles here
   Table tb;           // the problems of this solve
 };

@@ -98,12 +98,13 @@ __device__ __forceinline__ double bsum(double v, double* red) {
 // on B200: G*G acquire loads per round.)  Bounded: gives up after spin_limit
 // polls, records kErrTimeout, and every later barrier of the launch returns
 // at once.
-__device__ __forceinline__ void gbar(unsigned* ctr, unsigned gen, int G, int cta, int* err, unsigned spin_limit) {
+__device__ __forceinline__ void gbar(unsigned* ctr, unsigned gen, int G, int cta, int* err, unsigned spin_limit,
+                                     unsigned extra) {
   (void)cta;
   __syncthreads();
   if (threadIdx.x == 0) {
     red_release_gpu_add(ctr, 1u);
-    const unsigned target = (gen + 1u) * (unsigned)G;
+    const unsigned target = (gen + 1u) * (unsigned)G + extra;
     unsigned polls = 0;
     while (ld_acquire_gpu(ctr) < target) {
       if (*(volatile int*)err != 0) break;
@@ -291,7 +292,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
       }
     }
     clk.mark(0);  // prologue
-    gbar(bar, gen++, G, cta, err, a.spin_limit);
+    gbar(bar, gen++, G, cta, err, a.spin_limit, a.bar_extra);
     clk.mark(1);  // first barrier
     double rz = 0.0;
     float betaf = 0.f;
@@ -347,7 +348,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
         if (tid == 0) part[((gen & 1) * 3 + 0) * GT + cta] = t1;
       }
       clk.mark(5);  // block sum
-      gbar(bar, gen++, G, cta, err, a.spin_limit);
+      gbar(bar, gen++, G, cta, err, a.spin_limit, a.bar_extra);
       clk.mark(6);  // barrier A
       if (tid < 32) wsum_parts<1>(part + (((gen - 1) & 1) * 3 + 0) * GT + gb, G, GT, sRed, 18);
       __syncthreads();
@@ -378,7 +379,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
         }
       }
       clk.mark(9);  // block sums
-      gbar(bar, gen++, G, cta, err, a.spin_limit);
+      gbar(bar, gen++, G, cta, err, a.spin_limit, a.bar_extra);
       clk.mark(10);  // barrier B
     }
     // ---- epilogue ----
@@ -421,7 +422,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
       sV[t] = uf;
       xb[gen & 1][r0 * 6 + t] = uf;
     }
-    gbar(bar, gen++, G, cta, err, a.spin_limit);
+    gbar(bar, gen++, G, cta, err, a.spin_limit, a.bar_extra);
     for (int e = tid; e < h6; e += kThreads) sV[n6 + e] = __ldcg(xb[(gen - 1) & 1] + sHalo[e / 6] * 6 + e % 6);
     __syncthreads();
     // w = A u ; then the first reduction and m = M^-1 w
@@ -444,7 +445,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
         part[(buf * 3 + 1) * GT + cta] = t2;
         part[(buf * 3 + 2) * GT + cta] = t3;
       }
-      gbar(bar, gen++, G, cta, err, a.spin_limit);
+      gbar(bar, gen++, G, cta, err, a.spin_limit, a.bar_extra);
     };
     reduce_and_publish();
     double gamma_prev = 0.0, alpha_prev = 0.0;
@@ -493,7 +494,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
         for (int t = tid; t < n6; t += kThreads) pr += vR[t] * vR[t];
         const double t3 = bsum(pr, sRed);
         if (tid == 0) part[((gen & 1) * 3 + 2) * GT + cta] = t3;
-        gbar(bar, gen++, G, cta, err, a.spin_limit);
+        gbar(bar, gen++, G, cta, err, a.spin_limit, a.bar_extra);
         if (tid < 32) wsum_parts<1>(part + (((gen - 1) & 1) * 3 + 2) * GT + gb, G, GT, sRed, 18);
         __syncthreads();
         rr_last = sRed[18];

@@ -32,6 +32,11 @@ constexpr int kTileBlocks = 256;                 // blocks per tile (one per thr
 constexpr int kTileBytes = kTileBlocks * 36 * 4;  // 36,864 B
 constexpr int kStages = 2;
 constexpr int kPartStride = 7;  // padded 6-float partial row
+// polls of a tile copy's completion before it counts as lost: a copy always
+// completes, so this is far above any real wait and independent of the
+// barrier's (settable) limit; a CTA never exits with its copy in flight
+// unless this runs out
+constexpr unsigned kCopyWaitLimit = 1u << 26;
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -87,11 +92,12 @@ __device__ __forceinline__ double bsum_s(double v, double* red) {
 }
 
 // group barrier: release arrive on the group's counter, bounded acquire poll
-__device__ __forceinline__ void gbar_s(unsigned* ctr, unsigned gen, int G, int* err, unsigned spin_limit) {
+__device__ __forceinline__ void gbar_s(unsigned* ctr, unsigned gen, int G, int* err, unsigned spin_limit,
+                                       unsigned extra) {
   __syncthreads();
   if (threadIdx.x == 0) {
     red_release_gpu_add(ctr, 1u);
-    const unsigned target = (gen + 1u) * (unsigned)G;
+    const unsigned target = (gen + 1u) * (unsigned)G + extra;
     unsigned polls = 0;
     while (ld_acquire_gpu(ctr) < target) {
       if (*(volatile int*)err != 0) break;
@@ -230,7 +236,7 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_stream_kernel(StreamArgs P) {
       part[(0 * 3 + 1) * GT + cta] = t2;
     }
   }
-  gbar_s(bar, gen++, G, err, a.spin_limit);
+  gbar_s(bar, gen++, G, err, a.spin_limit, a.bar_extra);
 
   int used = 0;
   double rz = 0.0, rr_last = 0.0;
@@ -271,7 +277,7 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_stream_kernel(StreamArgs P) {
     double ppap = 0.0;
     for (int t = 0; t < n_tiles; t++) {
       const int s = (int)(consumed % kStages);
-      if (!mbar_wait(&mbar[s], (phase_bits >> s) & 1u, err, a.spin_limit)) ok = false;
+      if (!mbar_wait(&mbar[s], (phase_bits >> s) & 1u, err, kCopyWaitLimit)) ok = false;
       phase_bits ^= 1u << s;
       const float* A = ring + (size_t)s * kTileBlocks * 36;
       const int ra = trow[t], rb_ = trow[t + 1];
@@ -321,7 +327,7 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_stream_kernel(StreamArgs P) {
       const double t1 = bsum_s(ppap, sRed);
       if (tid == 0) part[((gen & 1) * 3 + 0) * GT + cta] = t1;
     }
-    gbar_s(bar, gen++, G, err, a.spin_limit);
+    gbar_s(bar, gen++, G, err, a.spin_limit, a.bar_extra);
     if (tid < 32) {
       double v0 = 0.0;
       for (int k = tid; k < G; k += 32) v0 += __ldcg(part + (((gen - 1) & 1) * 3 + 0) * GT + gb + k);
@@ -371,12 +377,12 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_stream_kernel(StreamArgs P) {
         part[((gen & 1) * 3 + 1) * GT + cta] = t2;
       }
     }
-    gbar_s(bar, gen++, G, err, a.spin_limit);
+    gbar_s(bar, gen++, G, err, a.spin_limit, a.bar_extra);
   }
   // ---- drain the prefetched tiles, then the epilogue ----
   while (consumed < issued) {
     const int s = (int)(consumed % kStages);
-    if (n_tiles > 0) mbar_wait(&mbar[s], (phase_bits >> s) & 1u, err, a.spin_limit);
+    if (n_tiles > 0) mbar_wait(&mbar[s], (phase_bits >> s) & 1u, err, kCopyWaitLimit);
     phase_bits ^= 1u << s;
     consumed++;
   }

@@ -185,6 +185,14 @@ CF_API cf_status cf_gn_linearize_solve(cf_gn* h, const cf_correspondence* d_corr
 #define CF_OPT_GRAPH 5
 /* read only (cf_gn_get_option): 1 when the last solve ran as a CUDA graph */
 #define CF_OPT_GRAPH_ACTIVE 6
+/* Polls of a PCG grid barrier before it gives up (0 = the default, 1<<22):
+ * the kernel then records CF_ERR_TIMEOUT, every later barrier of the launch
+ * returns at once, and the solve returns CF_ERR_TIMEOUT with the context
+ * intact (its transforms are then not a solution). */
+#define CF_OPT_SPIN_LIMIT 7
+/* Test hook for the failure path above: every PCG group barrier also waits
+ * for this many arrivals that never come (0 in normal use). */
+#define CF_OPT_TEST_BARRIER_EXTRA 8
 CF_API cf_status cf_gn_set_option(cf_gn* h, int option, int value);
 CF_API cf_status cf_gn_get_option(const cf_gn* h, int option, int* value);
 

@@ -346,3 +346,28 @@ def test_graph_replay_matches_direct_launches(p1):
         assert out[1][k][0] == out[0][k][0]
         assert out[1][k][1] == out[0][k][1]
         assert out[1][k][2] == out[0][k][2]  # the launches a replay stands for
+
+
+@pytest.mark.parametrize("mode", [1, 3])
+def test_barrier_timeout_is_reported_and_the_context_survives(p1, oracle, mode):
+    """Failure detection without a GPU fault: a PCG barrier that waits for an
+    arrival nobody makes gives up after its (short) poll limit; the solve
+    reports CF_ERR_TIMEOUT, and the next solve on the same handle is exact."""
+    prm = Params(gn_iterations=2, pcg_iterations=10, pcg_tolerance=0.0, lambda_smooth=10.0)
+    s = make_solver(prm, mode=(mode, 0))
+    dp = DeviceProblem(p1)
+    s.set_option(_lib.CF_OPT_SPIN_LIMIT, 20000)
+    s.set_option(_lib.CF_OPT_TEST_BARRIER_EXTRA, 1)
+    T = dp.init_transforms.clone()
+    with pytest.raises(_lib.CFError) as e:
+        s.gn_solve(dp, T, max_rot=0.12, max_trans=0.04)
+    assert e.value.status == _lib.CF_ERR_TIMEOUT
+    s.set_option(_lib.CF_OPT_TEST_BARRIER_EXTRA, 0)
+    s.set_option(_lib.CF_OPT_SPIN_LIMIT, 0)
+    T = dp.init_transforms.clone()
+    st = s.gn_solve(dp, T, max_rot=0.12, max_trans=0.04)
+    assert st["error_flags"] == 0
+    ref = make_solver(prm, mode=(mode, 0))
+    T2 = dp.init_transforms.clone()
+    ref.gn_solve(dp, T2, max_rot=0.12, max_trans=0.04)
+    assert torch.equal(T, T2)
