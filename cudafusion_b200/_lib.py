@@ -26,6 +26,7 @@ CF_OPT_GRAPH = 5
 CF_OPT_GRAPH_ACTIVE = 6
 CF_OPT_SPIN_LIMIT = 7
 CF_OPT_TEST_BARRIER_EXTRA = 8
+CF_OPT_STREAM_TILE = 9
 CF_MAX_GN_ITERS = 32
 CF_PROF_SLOTS = 12
 CF_MPNN_IN = 20
@@ -55,6 +56,7 @@ EXPORTS = [
     "cf_gn_solve",
     "cf_gn_solve_batched",
     "cf_gn_last_stats",
+    "cf_gn_autotune",
     "cf_mpnn_create",
     "cf_mpnn_destroy",
     "cf_mpnn_set_weights",
@@ -122,6 +124,18 @@ class SolveStats(ctypes.Structure):
     ]
 
 
+class TuneResult(ctypes.Structure):
+    _fields_ = [
+        ("pcg_mode", ctypes.c_int),
+        ("pcg_ctas", ctypes.c_int),
+        ("stream_tile", ctypes.c_int),
+        ("candidates", ctypes.c_int),
+        ("ms_best", ctypes.c_double),
+        ("ms_default", ctypes.c_double),
+        ("from_cache", ctypes.c_int),
+    ]
+
+
 class CFError(RuntimeError):
     def __init__(self, status, where=""):
         self.status = status
@@ -163,6 +177,7 @@ def lib():
         L.cf_gn_solve_batched.argtypes = [vp, ctypes.POINTER(Problem), i, ctypes.POINTER(vp),
                                           ctypes.POINTER(SolveStats), vp]
         L.cf_gn_last_stats.argtypes = [vp, ctypes.POINTER(SolveStats), i, vp]
+        L.cf_gn_autotune.argtypes = [vp, ctypes.POINTER(Problem), i, ctypes.POINTER(vp), ctypes.POINTER(TuneResult), vp]
         pf = ctypes.POINTER(ctypes.c_float)
         L.cf_mpnn_create.argtypes = [i, ctypes.POINTER(vp)]
         L.cf_mpnn_destroy.argtypes = [vp]

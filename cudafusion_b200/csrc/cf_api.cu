@@ -5,7 +5,10 @@
 // kernels/solver_kernels.cu:498-541), the PCG row partition, and the launch
 // sequence.  Every device computation happens in cf_kernels.cu.
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <set>
+#include <string>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -40,6 +43,7 @@ struct cf_gn {
   int pcg_pipelined = 0;
   int phase_timers = 0;
   unsigned spin_limit = 1u << 22;
+  int stream_tile = 256;
   unsigned bar_extra = 0;
   Work w;
   Pattern p;
@@ -468,12 +472,12 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
   std::vector<int> tile_ptr, tile_row;
   const bool stream = rb2.empty();
   if (stream) {
-    const int cap = pcg_stream_max_active_ctas();
+    const int TB = h->stream_tile == 128 ? 128 : 256;
+    const int cap = pcg_stream_max_active_ctas(TB);
     if (cap < P) return CF_ERR_CAPACITY;
     int Gs = h->pcg_ctas_override > 0 ? h->pcg_ctas_override : cap;
     Gs = std::max(P, std::min({Gs, cap, N, kMaxPcgCtas}));
     split_rows(Gs, rb2, cta_off2, cta_prob2);
-    const int TB = pcg_stream_tile_blocks();
     tile_ptr.assign(1, 0);
     for (size_t c = 0; c + 1 < rb2.size(); c++) {
       const int r0 = rb2[c], r1 = rb2[c + 1];
@@ -485,7 +489,7 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
     }
     g_halo_ptr.assign(rb2.size(), 0);
     g_halo_col.clear();
-    smem = pcg_stream_smem_bytes();
+    smem = pcg_stream_smem_bytes(TB);
     a_smem = false;
   }
   G = (int)rb2.size() - 1;
@@ -576,6 +580,7 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
   p.pcg_a_in_smem = a_smem ? 1 : 0;
   p.pcg_pipelined = pipe ? 1 : 0;
   p.pcg_stream = stream ? 1 : 0;
+  p.st_tile_blocks = h->stream_tile == 128 ? 128 : 256;
   auto up = [](int** d, const std::vector<int>& v) -> cudaError_t {
     cudaError_t e = dalloc(d, v.size());
     if (e != cudaSuccess) return e;
@@ -1009,6 +1014,11 @@ cf_status cf_gn_set_option(cf_gn* h, int option, int value) {
       if (value < 0) return CF_ERR_INVALID_ARG;
       h->bar_extra = (unsigned)value;
       return CF_OK;
+    case CF_OPT_STREAM_TILE:
+      if (value != 0 && value != 128 && value != 256) return CF_ERR_INVALID_ARG;
+      h->stream_tile = value ? value : 256;
+      h->pattern_valid = false;
+      return CF_OK;
     case CF_OPT_PCG_CTAS:
       if (value < 0 || value > kMaxPcgCtas) return CF_ERR_INVALID_ARG;
       h->pcg_ctas_override = value;
@@ -1029,6 +1039,7 @@ cf_status cf_gn_get_option(const cf_gn* h, int option, int* value) {
     case CF_OPT_GRAPH_ACTIVE: *value = h->graph_last; return CF_OK;
     case CF_OPT_SPIN_LIMIT: *value = (int)h->spin_limit; return CF_OK;
     case CF_OPT_TEST_BARRIER_EXTRA: *value = (int)h->bar_extra; return CF_OK;
+    case CF_OPT_STREAM_TILE: *value = h->stream_tile; return CF_OK;
   }
   return CF_ERR_INVALID_ARG;
 }
@@ -1134,6 +1145,164 @@ cf_status cf_gn_solve_batched(cf_gn* h, const cf_problem* problems, int num_prob
   st = solve_graphed(h, 1, a, s);
   if (st != CF_OK || !stats) return st;
   return read_stats(h, stats, slot_of, num_problems, s);
+}
+
+// ---- autotuner ------------------------------------------------------------
+
+namespace {
+
+struct TuneChoice {
+  int pcg_mode, pcg_ctas, stream_tile;
+  double ms_best, ms_default;
+};
+
+std::mutex g_tune_mu;
+std::map<std::string, TuneChoice> g_tune_cache;
+bool g_tune_loaded = false;
+
+const char* tune_file() { return getenv("CF_AUTOTUNE_CACHE"); }
+
+void tune_load_locked() {
+  if (g_tune_loaded) return;
+  g_tune_loaded = true;
+  const char* path = tune_file();
+  if (!path) return;
+  FILE* f = fopen(path, "r");
+  if (!f) return;
+  char key[512];
+  TuneChoice c;
+  while (fscanf(f, "%511s %d %d %d %lf %lf", key, &c.pcg_mode, &c.pcg_ctas, &c.stream_tile, &c.ms_best,
+                &c.ms_default) == 6)
+    g_tune_cache[key] = c;
+  fclose(f);
+}
+
+void tune_store_locked(const std::string& key, const TuneChoice& c) {
+  g_tune_cache[key] = c;
+  const char* path = tune_file();
+  if (!path) return;
+  FILE* f = fopen(path, "a");
+  if (!f) return;
+  fprintf(f, "%s %d %d %d %.6f %.6f\n", key.c_str(), c.pcg_mode, c.pcg_ctas, c.stream_tile, c.ms_best,
+          c.ms_default);
+  fclose(f);
+}
+
+// the shape of a tuning problem: device, sizes and the solver settings the
+// PCG's speed depends on
+std::string tune_key(const cf_gn* h, const cf_problem* pr, int num) {
+  long long N = 0, M = 0;
+  for (int q = 0; q < num; q++) {
+    N += pr[q].num_nodes;
+    M += pr[q].num_corrs;
+  }
+  char buf[256];
+  snprintf(buf, sizeof(buf), "sm%d/P%d/N%lld/M%lld/G%d/I%d/pipe%d", h->sms, num, N, M, h->params.gn_iterations,
+           h->params.pcg_iterations, h->pcg_pipelined);
+  return buf;
+}
+
+}  // namespace
+
+cf_status cf_gn_autotune(cf_gn* h, const cf_problem* problems, int num_problems, cf_dual_quat* const* d_transforms,
+                         cf_tune_result* out, void* stream) {
+  if (!h || !problems || !d_transforms || num_problems < 1) return CF_ERR_INVALID_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const std::string key = tune_key(h, problems, num_problems);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    tune_load_locked();
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      const TuneChoice& c = it->second;
+      h->pcg_mode = c.pcg_mode;
+      h->pcg_ctas_override = c.pcg_ctas;
+      h->stream_tile = c.stream_tile;
+      h->pattern_valid = false;
+      if (out) *out = cf_tune_result{c.pcg_mode, c.pcg_ctas, c.stream_tile, 0, c.ms_best, c.ms_default, 1};
+      return CF_OK;
+    }
+  }
+  // scratch copies of the transforms: the candidates never touch the caller's
+  std::vector<cf_dual_quat*> scratch(num_problems, nullptr);
+  cf_status st = CF_OK;
+  for (int q = 0; q < num_problems && st == CF_OK; q++) {
+    const size_t n = (size_t)std::max(problems[q].num_nodes, 1);
+    if (cudaMalloc(&scratch[q], sizeof(cf_dual_quat) * n) != cudaSuccess) st = CF_ERR_OOM;
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (st == CF_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) st = CF_ERR_CUDA;
+  const int mode0 = h->pcg_mode, ctas0 = h->pcg_ctas_override, tile0 = h->stream_tile;
+  struct Cand {
+    int mode, ctas, tile;
+  };
+  std::vector<Cand> cands = {{mode0, ctas0, tile0}};  // the configuration in effect first: the baseline
+  for (int ctas : {0, h->sms, 2 * h->sms}) cands.push_back({1, ctas, 256});
+  for (int tile : {256, 128})
+    for (int ctas : {0, h->sms}) cands.push_back({3, ctas, tile});
+  double best = 1e30, baseline = 0.0;
+  Cand pick = cands[0];
+  int timed = 0;
+  std::set<std::vector<int>> seen;  // effective configurations already timed
+  for (const Cand& c : cands) {
+    if (st != CF_OK) break;
+    h->pcg_mode = c.mode;
+    h->pcg_ctas_override = c.ctas;
+    h->stream_tile = c.tile;
+    h->pattern_valid = false;
+    auto run = [&]() -> cf_status {
+      for (int q = 0; q < num_problems; q++)
+        if (problems[q].num_nodes > 0)
+          CF_TRY(cudaMemcpyAsync(scratch[q], d_transforms[q], sizeof(cf_dual_quat) * problems[q].num_nodes,
+                                 cudaMemcpyDeviceToDevice, s));
+      return num_problems == 1 ? cf_gn_solve(h, problems, scratch[0], nullptr, s)
+                               : cf_gn_solve_batched(h, problems, num_problems, scratch.data(), nullptr, s);
+    };
+    cf_status r = run();  // builds the pattern, captures the graph
+    if (r == CF_ERR_CAPACITY) continue;  // not feasible at this size
+    if (r != CF_OK) {
+      st = r;
+      break;
+    }
+    const std::vector<int> eff{h->p.pcg_stream, h->p.pcg_ctas, h->p.use_cluster, h->p.st_tile_blocks};
+    if (!seen.insert(eff).second && timed > 0) continue;
+    std::vector<float> ms;
+    for (int k = 0; k < 3 && st == CF_OK; k++) {
+      cudaEventRecord(e0, s);
+      st = run();
+      cudaEventRecord(e1, s);
+      if (cudaEventSynchronize(e1) != cudaSuccess) st = CF_ERR_CUDA;
+      float t = 0.f;
+      cudaEventElapsedTime(&t, e0, e1);
+      ms.push_back(t);
+    }
+    if (st != CF_OK) break;
+    std::sort(ms.begin(), ms.end());
+    const double med = ms[ms.size() / 2];
+    if (timed == 0) baseline = med;
+    timed++;
+    if (med < best) {
+      best = med;
+      pick = c;
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaStreamSynchronize(s);
+  for (auto p : scratch)
+    if (p) cudaFree(p);
+  h->pcg_mode = st == CF_OK ? pick.mode : mode0;
+  h->pcg_ctas_override = st == CF_OK ? pick.ctas : ctas0;
+  h->stream_tile = st == CF_OK ? pick.tile : tile0;
+  h->pattern_valid = false;
+  if (st != CF_OK) return st;
+  const TuneChoice choice{pick.mode, pick.ctas, pick.tile, best, baseline};
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    tune_store_locked(key, choice);
+  }
+  if (out) *out = cf_tune_result{pick.mode, pick.ctas, pick.tile, timed, best, baseline, 0};
+  return CF_OK;
 }
 
 // ---- learned initial increment ------------------------------------------

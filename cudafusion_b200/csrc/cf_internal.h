@@ -111,6 +111,7 @@ struct Pattern {
   int* g_halo_col = nullptr;  // distinct columns of other CTAs touched by each CTA
   // streaming PCG (cf_pcg_stream.cu): A streamed from HBM in tiles of whole rows
   int pcg_stream = 0;
+  int st_tile_blocks = 256;    // blocks per tile (256 or 128)
   int* st_tile_ptr = nullptr;  // [pcg_ctas+1] into st_tile_row
   int* st_tile_row = nullptr;  // per CTA: its tiles' first rows, then its end row
 };
@@ -241,9 +242,8 @@ cudaError_t launch_apply_prediction(const Work& w, cf_dual_quat* T, const cf_def
 cudaError_t launch_gate_prediction(const Work& w, cf_dual_quat* T, const cf_deform_node* nodes, int N,
                                    cudaStream_t s);
 
-int pcg_stream_smem_bytes();
-int pcg_stream_tile_blocks();
-int pcg_stream_max_active_ctas();
+int pcg_stream_smem_bytes(int tile_blocks);
+int pcg_stream_max_active_ctas(int tile_blocks);
 cudaError_t launch_pcg_stream(const Work& w, const Pattern& p, const SolveArgs& a, int gn_slot, cudaStream_t s);
 
 }  // namespace cf

@@ -9,7 +9,7 @@
 // the data lives: every iteration streams the CTA's block rows of A from HBM
 // through a ring of shared-memory stages filled by TMA bulk copies
 // (cp.async.bulk, completion on an mbarrier), and the vectors stay in global
-// memory.  A tile is a run of whole block rows of at most kTileBlocks blocks.
+// memory.  A tile is a run of whole block rows of at most TB blocks.
 //
 // Per iteration, per CTA:
 //   SpMV   thread per block of the tile: y_b = A_b (z_j + beta p_old_j), the
@@ -28,8 +28,8 @@ namespace cf {
 
 namespace {
 
-constexpr int kTileBlocks = 256;                 // blocks per tile (one per thread)
-constexpr int kTileBytes = kTileBlocks * 36 * 4;  // 36,864 B
+// tile: up to TB blocks of whole rows (one thread per block): 256 (36,864 B)
+// or 128, the autotuner's choice
 constexpr int kStages = 2;
 constexpr int kPartStride = 7;  // padded 6-float partial row
 // polls of a tile copy's completion before it counts as lost: a copy always
@@ -130,7 +130,10 @@ struct StreamArgs {
   int slot;
 };
 
+template <int TB>
 __global__ void __launch_bounds__(kThreads, 2) pcg_stream_kernel(StreamArgs P) {
+  static_assert(TB <= kThreads, "one thread per block of a tile");
+  constexpr int kTileBlocks = TB, kTileBytes = TB * 36 * 4;
   extern __shared__ __align__(128) unsigned char smem[];
   float* ring = reinterpret_cast<float*>(smem);                          // [kStages][kTileBlocks*36]
   float* sPart = reinterpret_cast<float*>(smem + kStages * kTileBytes);  // [kTileBlocks][7]
@@ -410,18 +413,21 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_stream_kernel(StreamArgs P) {
 
 }  // namespace
 
-int pcg_stream_smem_bytes() { return kStages * kTileBytes + kTileBlocks * kPartStride * 4 + 64 * 8; }
-static_assert(kStages * kTileBytes >= (kThreads / 8) * 108 * 8, "the ring holds the inversion scratch");
-int pcg_stream_tile_blocks() { return kTileBlocks; }
+int pcg_stream_smem_bytes(int tb) { return kStages * tb * 144 + tb * kPartStride * 4 + 64 * 8; }
+static_assert(kStages * 128 * 144 >= (kThreads / 8) * 108 * 8, "the ring holds the inversion scratch");
 
-int pcg_stream_max_active_ctas() {
-  const int smem = pcg_stream_smem_bytes();
-  if (cudaFuncSetAttribute(pcg_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) {
+namespace {
+void* stream_fn(int tb) { return tb == 128 ? (void*)pcg_stream_kernel<128> : (void*)pcg_stream_kernel<256>; }
+}  // namespace
+
+int pcg_stream_max_active_ctas(int tb) {
+  const int smem = pcg_stream_smem_bytes(tb);
+  if (cudaFuncSetAttribute(stream_fn(tb), cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_stream_kernel, kThreads, smem) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stream_fn(tb), kThreads, smem) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
@@ -441,8 +447,8 @@ cudaError_t launch_pcg_stream(const Work& w, const Pattern& p, const SolveArgs& 
   P.a = a;
   P.slot = gn_slot;
   void* args[] = {&P};
-  return cudaLaunchCooperativeKernel((void*)pcg_stream_kernel, dim3(p.pcg_ctas), dim3(kThreads), args,
-                                     (size_t)pcg_stream_smem_bytes(), s);
+  return cudaLaunchCooperativeKernel(stream_fn(p.st_tile_blocks), dim3(p.pcg_ctas), dim3(kThreads), args,
+                                     (size_t)pcg_stream_smem_bytes(p.st_tile_blocks), s);
 }
 
 }  // namespace cf

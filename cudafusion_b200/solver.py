@@ -208,6 +208,17 @@ class GaussNewtonSolver:
             ))
         return res
 
+    def autotune(self, dproblems, d_transforms, max_rot=0.0, max_trans=0.0, update_scale=1.0, stream=None):
+        """cf_gn_autotune over `dproblems` (one: the single solve; several:
+        the batched solve); returns the choice as a dict."""
+        n = len(dproblems)
+        probs = (_lib.Problem * n)(*[d.c(max_rot, max_trans, update_scale) for d in dproblems])
+        ptrs = (ctypes.c_void_p * n)(*[t.data_ptr() for t in d_transforms])
+        r = _lib.TuneResult()
+        check(_lib.lib().cf_gn_autotune(self._h, probs, n, ptrs, ctypes.byref(r), _stream_ptr(stream)),
+              "cf_gn_autotune")
+        return {k: getattr(r, k) for k, _ in _lib.TuneResult._fields_}
+
     def last_stats(self, stream=None):
         """Statistics of the handle's last solve (cf_gn_last_stats)."""
         s = _lib.SolveStats()

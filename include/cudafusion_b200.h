@@ -193,6 +193,8 @@ CF_API cf_status cf_gn_linearize_solve(cf_gn* h, const cf_correspondence* d_corr
 /* Test hook for the failure path above: every PCG group barrier also waits
  * for this many arrivals that never come (0 in normal use). */
 #define CF_OPT_TEST_BARRIER_EXTRA 8
+/* Blocks per shared-memory tile of the streaming PCG: 256 (default) or 128. */
+#define CF_OPT_STREAM_TILE 9
 CF_API cf_status cf_gn_set_option(cf_gn* h, int option, int value);
 CF_API cf_status cf_gn_get_option(const cf_gn* h, int option, int* value);
 
@@ -251,6 +253,29 @@ typedef struct cf_problem {
 CF_API cf_status cf_gn_solve(cf_gn* h, const cf_problem* problem,
                       cf_dual_quat* d_transforms, cf_solve_stats* stats,
                       void* stream);
+
+/* Autotuner (no reference counterpart).  Times the PCG configurations that
+ * matter for these problems — the system held in shared memory (grid of the
+ * automatic size, one or two CTAs per SM) or streamed through TMA tiles (256
+ * or 128 blocks per tile; automatic or one CTA per SM) — on the actual
+ * problems (the caller's transforms are read, never written; the candidates
+ * run on scratch copies, which this call allocates), leaves the fastest set
+ * on the handle and remembers it per (SM count, problem count, total nodes and
+ * correspondences, GN / PCG iterations): in the process, and in the file named
+ * by the environment variable CF_AUTOTUNE_CACHE when set.  A remembered
+ * shape is applied without timing (from_cache = 1).  One problem: tuned for
+ * cf_gn_solve; several: for cf_gn_solve_batched.  Synchronises `stream`. */
+typedef struct cf_tune_result {
+  int pcg_mode;     /* the chosen CF_OPT_PCG_MODE */
+  int pcg_ctas;     /* the chosen CF_OPT_PCG_CTAS (0 = automatic) */
+  int stream_tile;  /* the chosen CF_OPT_STREAM_TILE */
+  int candidates;   /* distinct configurations timed */
+  double ms_best;   /* median ms of a solve with the choice */
+  double ms_default; /* median ms of a solve with the configuration in effect before */
+  int from_cache;
+} cf_tune_result;
+CF_API cf_status cf_gn_autotune(cf_gn* h, const cf_problem* problems, int num_problems,
+                                cf_dual_quat* const* d_transforms, cf_tune_result* out, void* stream);
 
 /* Statistics of the handle's last solve, read without running it again
  * (for a caller that ran it with stats = NULL): `num` records in the order of

@@ -110,3 +110,23 @@ def test_batched_skips_empty_problem_and_checks_capacity(batch):
     small = GaussNewtonSolver(Params(**KW), max_nodes=100, max_corrs=100000)
     with pytest.raises(_lib.CFError):
         small.gn_solve_batched([DeviceProblem(batch[1])], [DeviceProblem(batch[1]).init_transforms.clone()])
+
+
+def test_autotune_chooses_times_and_remembers(batch):
+    """The autotuner times several PCG configurations on the batch, leaves
+    the fastest on the handle (results still exact), never writes the
+    caller's transforms, and answers the same shape from its cache."""
+    s = _solver(batch)
+    dps = [DeviceProblem(p) for p in batch]
+    Ts = [d.init_transforms.clone() for d in dps]
+    r = s.autotune(dps, Ts, *CLAMPS)
+    assert r["candidates"] >= 2 and r["from_cache"] == 0
+    assert r["ms_best"] <= r["ms_default"]
+    assert all(torch.equal(T, d.init_transforms) for T, d in zip(Ts, dps))
+    assert s.get_option(_lib.CF_OPT_PCG_MODE) == r["pcg_mode"]
+    assert s.get_option(_lib.CF_OPT_PCG_CTAS) == r["pcg_ctas"]
+    st = s.gn_solve_batched(dps, Ts, *CLAMPS)
+    assert all(x["error_flags"] == 0 for x in st)
+    s2 = _solver(batch)
+    r2 = s2.autotune(dps, [d.init_transforms.clone() for d in dps], *CLAMPS)
+    assert r2["from_cache"] == 1 and r2["pcg_mode"] == r["pcg_mode"] and r2["stream_tile"] == r["stream_tile"]
