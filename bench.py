@@ -446,6 +446,70 @@ def run_b200(args, world, rank, local):
     return line
 
 
+def run_batch(args, world, rank, local):
+    """`--workload batch`: `--problems` uneven sphere problems (N ~ U[500, 8000],
+    M = 150 N +- 20 %) solved together by one cf_gn_solve_batched per step
+    (graphed, side stream), against the same problems solved one by one."""
+    import numpy as np
+    import torch
+
+    from cudafusion_b200 import _lib, synth
+    from cudafusion_b200.solver import DeviceProblem, GaussNewtonSolver, Params
+
+    probs = synth.config4(num_problems=args.problems)
+    dps = [DeviceProblem(p) for p in probs]
+    Nt, Mt = sum(p.num_nodes for p in probs), sum(p.num_corrs for p in probs)
+    prm = Params(gn_iterations=GN_ITERS, pcg_iterations=PCG_ITERS, pcg_tolerance=PCG_TOL, lambda_smooth=10.0,
+                 lambda_damping=1.0)
+    s = GaussNewtonSolver(prm, max_nodes=Nt, max_corrs=Mt)
+    if args.pcg_mode:
+        s.set_option(_lib.CF_OPT_PCG_MODE, args.pcg_mode)
+    side = torch.cuda.Stream()
+    Ts = [d.init_transforms.clone() for d in dps]
+
+    def reset():
+        for T, d in zip(Ts, dps):
+            T.copy_(d.init_transforms)
+
+    with torch.cuda.stream(side):
+        tune = s.autotune(dps, Ts, MAX_ROT, MAX_TRANS, stream=side) if not args.pcg_mode else None
+        for _ in range(args.warmup):
+            reset()
+            s.gn_solve_batched(dps, Ts, MAX_ROT, MAX_TRANS, stats=False, stream=side)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps)]
+        ms = []
+        for k in range(args.steps):
+            reset()
+            ev[2 * k].record(side)
+            s.gn_solve_batched(dps, Ts, MAX_ROT, MAX_TRANS, stats=False, stream=side)
+            ev[2 * k + 1].record(side)
+        side.synchronize()
+        ms = [ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(args.steps)]
+        st = s.gn_solve_batched(dps, Ts, MAX_ROT, MAX_TRANS, stream=side)
+        one = GaussNewtonSolver(prm, max_nodes=max(p.num_nodes for p in probs),
+                                max_corrs=max(p.num_corrs for p in probs))
+        seq = []
+        for d in dps:
+            T = d.init_transforms.clone()
+            one.gn_solve(d, T, MAX_ROT, MAX_TRANS, stats=False, stream=side)
+            side.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            T.copy_(d.init_transforms)
+            a.record(side)
+            one.gn_solve(d, T, MAX_ROT, MAX_TRANS, stats=False, stream=side)
+            b.record(side)
+            side.synchronize()
+            seq.append(a.elapsed_time(b))
+    batch_ms = float(np.median(ms))
+    return {"workload": f"batched uneven solves: {len(probs)} sphere problems, N={Nt} nodes, M={Mt} "
+                        f"correspondences in total, {GN_ITERS} GN x {PCG_ITERS} PCG, lambda_smooth 10, damping 1.0",
+            "batched_ms": batch_ms, "solves_per_s": len(probs) / (batch_ms * 1e-3),
+            "per_problem_latency_ms": batch_ms, "sequential_ms": float(sum(seq)),
+            "sequential_per_problem_ms": float(np.mean(seq)), "speedup_vs_sequential": float(sum(seq)) / batch_ms,
+            "autotune": tune, "cuda_graph": bool(s.get_option(_lib.CF_OPT_GRAPH_ACTIVE)),
+            "error_flags": int(max(x["error_flags"] for x in st)), "steps": args.steps, "warmup": args.warmup}
+
+
 def run_reference(args, world, rank, local):
     import torch
 
@@ -540,13 +604,22 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-start comparison")
     ap.add_argument("--no-precision", action="store_true", help="skip the 8192-node precision study")
-    ap.add_argument("--pcg-mode", type=int, default=0, help="0 auto, 1 grid-wide, 2 single cluster")
+    ap.add_argument("--pcg-mode", type=int, default=0, help="0 auto, 1 grid-wide, 2 single cluster, 3 streaming")
+    ap.add_argument("--workload", default="frame", choices=["frame", "batch", "learned"],
+                    help="frame: the headline line; batch / learned: the batched-solve and learned-start "
+                         "measurements alone")
+    ap.add_argument("--problems", type=int, default=64, help="problems of --workload batch")
+    ap.add_argument("--frames", type=int, default=300, help="frames of --workload learned")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
     try:
         if args.impl == "reference":
             line = run_reference(args, world, rank, local)
+        elif args.workload == "batch":
+            line = run_batch(args, world, rank, local) if rank == 0 else None
+        elif args.workload == "learned":
+            line = learned_comparison(args.frames) if rank == 0 else None
         else:
             line = run_b200(args, world, rank, local)
         if rank == 0 and line is not None:

@@ -51,11 +51,12 @@ __global__ void __launch_bounds__(kThreads) layer_fwd(const void* in_, const int
                                                       const float* __restrict__ x_skip, int N) {
   constexpr int CAT = AGG ? 2 * DIN : DIN;
   extern __shared__ float fsm[];
-  float* sW = fsm;                 // [DOUT][CAT]
+  float* sW = fsm;                 // [CAT][DOUT]: transposed, so that the lanes (consecutive
+                                   // output units) read consecutive banks
   float* sB = sW + DOUT * CAT;     // [DOUT]
   float* sX = sB + DOUT;           // [32][CAT]
   const int n0 = blockIdx.x * kTileNodes;
-  for (int k = threadIdx.x; k < DOUT * CAT; k += kThreads) sW[k] = bf(W[k]);
+  for (int q = threadIdx.x; q < DOUT * CAT; q += kThreads) sW[(q % CAT) * DOUT + q / CAT] = bf(W[q]);
   for (int k = threadIdx.x; k < DOUT; k += kThreads) sB[k] = bf(b[k]);
   auto load_in = [&](int i, int k) -> float {
     if (FIRST) return bf(tobf(reinterpret_cast<const float*>(in_)[(size_t)i * DIN + k]));
@@ -83,10 +84,9 @@ __global__ void __launch_bounds__(kThreads) layer_fwd(const void* in_, const int
     const int s = e / DOUT, u = e % DOUT, i = n0 + s;
     if (i >= N) continue;
     float acc = sB[u];
-    const float* w = sW + u * CAT;
     const float* xx = sX + s * CAT;
 #pragma unroll 8
-    for (int k = 0; k < CAT; k++) acc = fmaf(w[k], xx[k], acc);
+    for (int k = 0; k < CAT; k++) acc = fmaf(sW[k * DOUT + u], xx[k], acc);
     if (RELU) acc = fmaxf(acc, 0.f);
     if (AGG) {
       reinterpret_cast<__nv_bfloat16*>(out_)[(size_t)i * DOUT + u] = tobf(acc);
