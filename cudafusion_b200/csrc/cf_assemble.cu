@@ -218,7 +218,9 @@ constexpr int kPartVals = 42;  // 36 block values + 6 rhs (diagonal block only)
 //     the diagonal block), the ARAP terms of the block's edges (precomputed
 //     by the residual launch), the damping; blocks written with their
 //     transposes, the rhs and the row's ARAP energy.
-__global__ void __launch_bounds__(kThreads, 2) assemble_kernel(Work w, Pattern pt, AsmArgs aa) {
+// 3 CTAs per SM (80 registers, 72 KB of shared memory each): the per-row
+// phases are latency chains, so rows in flight matter more than registers
+__global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern pt, AsmArgs aa) {
   extern __shared__ float4 stage_buf[];
   const int r = blockIdx.x, lane = lane_id(), wid = threadIdx.x >> 5;
   const int cap = aa.stage_cap;
