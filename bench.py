@@ -133,18 +133,28 @@ def barrier(world):
         import torch.distributed as dist
 
         dist.barrier()
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
 
 
 def max_over_ranks(v, world):
+    """The largest value over the ranks (the slowest replica's time)."""
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(per_rank_total_ms, steps, world):
+    """ms per solve of the whole job: each of the `world` replicas solves one
+    frame per step, the job's time is the slowest replica's, so the job
+    finishes world*steps solves in max_over_ranks(total) ms."""
+    return max_over_ranks(per_rank_total_ms, world) / (steps * world)
 
 
 def algorithmic_bytes(N, M, nnzb, pcg_iters_used):
@@ -343,8 +353,7 @@ def run_b200(args, world, rank, local):
     launches = solver.launch_count() - launches0
     graphed = solver.get_option(_lib.CF_OPT_GRAPH_ACTIVE)
     per_step = [a.elapsed_time(b) for a, b in evs]
-    total_ms = max_over_ranks(sum(per_step), world)
-    value = total_ms / (args.steps * world)
+    value = replica_value(sum(per_step), args.steps, world)
     # per-kernel event timing (direct launches: the profiler brackets every
     # launch with events, so this pass runs outside the graph)
     solver.profile_enable(True)
@@ -381,7 +390,7 @@ def run_b200(args, world, rank, local):
             b.record(side)
             side.synchronize()
             e2e_times.append(a.elapsed_time(b))
-    e2e_ms = max_over_ranks(sum(e2e_times), world) / (e2e_steps * world)
+    e2e_ms = replica_value(sum(e2e_times), e2e_steps, world)
     h2d = h_nodes.numel() + h_canon.numel() * 4 + h_corrs.numel() + h_T0.numel()
     d2h = h_Tout.numel() + 8 * (2 * 32 + 33) + 4 * 34  # transforms + the stats record + error word
 
