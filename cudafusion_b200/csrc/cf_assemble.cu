@@ -151,14 +151,6 @@ struct AsmArgs {
 // index of (p, q), p <= q, in the packed upper triangle of a 6x6 block
 __host__ __device__ constexpr int tri(int p, int q) { return p * 6 - p * (p - 1) / 2 + (q - p); }
 
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit_wait_all() {
-  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
-}
-
 // The row's incidence records (skinned src + fw, normal + residual, skin
 // weights) and entries: the first `ns` / `nt` staged in shared memory, the
 // rest (rows beyond the staging capacity) read from global memory.

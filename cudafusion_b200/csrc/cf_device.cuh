@@ -273,43 +273,60 @@ __device__ inline bool inv6_chol_d(const double* A, double* Ainv) {
 // warp); `active` is false for groups without a row.  Returns the fallback flag.
 __device__ inline bool inv6_group(const float* blk, double* S, double* Minv, bool active) {
   const int l = threadIdx.x & 7;
-  double* L = S;       // lower factor, reciprocal pivots on the diagonal
+  double* L = S;       // lower factor, reciprocal pivots on the diagonal (row-major, lower triangle)
   double* D = S + 36;  // A + 1e-4 I
   if (active)
     for (int q = l; q < 36; q += 8) D[q] = (double)blk[q] + ((q % 7 == 0) ? (double)1e-4f : 0.0);
   __syncwarp();
   int ok = 1;
   if (active && l == 0) {
-    for (int i = 0; i < 6 && ok; i++)
+    // the factor in registers (fully unrolled): no dependent shared-memory
+    // round trip per multiply-add of the elimination
+    double f[21];  // row i, column j <= i at i*(i+1)/2 + j
+#pragma unroll
+    for (int i = 0; i < 6; i++)
+#pragma unroll
       for (int j = 0; j <= i; j++) {
         double s = D[i * 6 + j];
-        for (int k = 0; k < j; k++) s -= L[i * 6 + k] * L[j * 6 + k];
+#pragma unroll
+        for (int k = 0; k < j; k++) s -= f[i * (i + 1) / 2 + k] * f[j * (j + 1) / 2 + k];
         if (i == j) {
-          if (!(s > 0.0)) {
-            ok = 0;
-            break;
-          }
-          L[i * 6 + i] = 1.0 / sqrt(s);
+          ok &= (s > 0.0) ? 1 : 0;  // a failed pivot leaves NaN behind it, never read (ok == 0)
+          f[i * (i + 1) / 2 + i] = 1.0 / sqrt(s);
         } else {
-          L[i * 6 + j] = s * L[j * 6 + j];
+          f[i * (i + 1) / 2 + j] = s * f[j * (j + 1) / 2 + j];
         }
       }
+#pragma unroll
+    for (int i = 0; i < 6; i++)
+#pragma unroll
+      for (int j = 0; j <= i; j++) L[i * 6 + j] = f[i * (i + 1) / 2 + j];
   }
   ok = __shfl_sync(0xffffffffu, ok, (threadIdx.x & 31) & ~7);
   __syncwarp();
   if (active && l < 6) {
     if (ok) {
+      double f[21];
+#pragma unroll
+      for (int i = 0; i < 6; i++)
+#pragma unroll
+        for (int j = 0; j <= i; j++) f[i * (i + 1) / 2 + j] = L[i * 6 + j];
       double y[6], x[6];
+#pragma unroll
       for (int i = 0; i < 6; i++) {
         double s = (i == l) ? 1.0 : 0.0;
-        for (int k = 0; k < i; k++) s -= L[i * 6 + k] * y[k];
-        y[i] = s * L[i * 6 + i];
+#pragma unroll
+        for (int k = 0; k < i; k++) s -= f[i * (i + 1) / 2 + k] * y[k];
+        y[i] = s * f[i * (i + 1) / 2 + i];
       }
+#pragma unroll
       for (int i = 5; i >= 0; i--) {
         double s = y[i];
-        for (int k = i + 1; k < 6; k++) s -= L[k * 6 + i] * x[k];
-        x[i] = s * L[i * 6 + i];
+#pragma unroll
+        for (int k = i + 1; k < 6; k++) s -= f[k * (k + 1) / 2 + i] * x[k];
+        x[i] = s * f[i * (i + 1) / 2 + i];
       }
+#pragma unroll
       for (int i = 0; i < 6; i++) Minv[i * 6 + l] = x[i];
     } else {
       for (int q = 0; q < 6; q++) Minv[l * 6 + q] = (q == l) ? 1.0 / (D[l * 6 + l] + (double)1e-6f) : 0.0;
@@ -394,6 +411,19 @@ __device__ __forceinline__ float warp_sum_f(float v) {
 }
 
 // ---- memory-order primitives for the bounded grid barrier ----
+// asynchronous global -> shared copies (16 B: both addresses 16-B aligned; 4 B: 4-B aligned)
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem_dst, const void* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
   unsigned v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");

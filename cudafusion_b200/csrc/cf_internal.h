@@ -180,7 +180,7 @@ struct SolveArgs {
   long long* timers;  // non-null: CTA 0 of the grid PCG accumulates phase cycles here
   Table tb;           // the problems of this solve
 };
-constexpr int kTimerSlots = 12;
+constexpr int kTimerSlots = 16;
 
 // ---- launchers (cf_kernels.cu) ----
 cudaError_t launch_pack_count(const Work& w, const Table& tb, cudaStream_t s);

@@ -29,7 +29,7 @@ namespace {
 __host__ __device__ inline int gal16(int x) { return (x + 15) & ~15; }
 
 struct GLayout {
-  int a, vidx, rowptr, halo, v, minv, scr, st, red, total;
+  int a, vidx, rowptr, halo, v, minv, scr, st, red, tn, total;
 };
 
 // v : the SpMV operand, [own rows | halo] x 6 floats.
@@ -48,6 +48,7 @@ __host__ __device__ inline GLayout glayout(int nblk, int nrows, int nhalo, bool 
   L.st = o;
   o += pipe ? gal16(nrows * 6 * 8) * 8 + gal16(nrows * 6 * 4) : gal16(nrows * 6 * 4) * 4 + gal16(nhalo * 6 * 4) * 2;
   L.red = o; o += 64 * 8;
+  L.tn = o; o += gal16(nrows * 48);  // per row: the transform and the node position, read in the prologue
   L.total = o;
   return L;
 }
@@ -58,25 +59,6 @@ struct GridArgs {
   SolveArgs a;
   int slot;
 };
-
-// two values reduced together: one pair of CTA barriers instead of two
-__device__ __forceinline__ void bsum2(double& a, double& b, double* red) {
-  a = warp_sum_d(a);
-  b = warp_sum_d(b);
-  const int wi = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  __syncthreads();
-  if (lane == 0) {
-    red[wi] = a;
-    red[8 + wi] = b;
-  }
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    double x = (lane < (int)(blockDim.x >> 5)) ? red[lane] : 0.0;
-    double y = (lane < (int)(blockDim.x >> 5)) ? red[8 + lane] : 0.0;
-    a = warp_sum_d(x);
-    b = warp_sum_d(y);
-  }
-}
 
 __device__ __forceinline__ double bsum(double v, double* red) {
   v = warp_sum_d(v);
@@ -98,41 +80,82 @@ __device__ __forceinline__ double bsum(double v, double* red) {
 // on B200: G*G acquire loads per round.)  Bounded: gives up after spin_limit
 // polls, records kErrTimeout, and every later barrier of the launch returns
 // at once.
+// The arrive and the bounded wait of the barrier, by one thread.
+__device__ __forceinline__ void arrive_wait(unsigned* ctr, unsigned gen, int G, int* err, unsigned spin_limit,
+                                            unsigned extra) {
+  red_release_gpu_add(ctr, 1u);
+  const unsigned target = (gen + 1u) * (unsigned)G + extra;
+  unsigned polls = 0;
+  while (ld_acquire_gpu(ctr) < target) {
+    if (*(volatile int*)err != 0) break;
+    if (++polls > spin_limit) {
+      atomicOr(err, kErrTimeout);
+      break;
+    }
+    if (polls > 256) __nanosleep(polls > 8192 ? 256 : 20);
+  }
+}
+
 __device__ __forceinline__ void gbar(unsigned* ctr, unsigned gen, int G, int cta, int* err, unsigned spin_limit,
                                      unsigned extra) {
   (void)cta;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    red_release_gpu_add(ctr, 1u);
-    const unsigned target = (gen + 1u) * (unsigned)G + extra;
-    unsigned polls = 0;
-    while (ld_acquire_gpu(ctr) < target) {
-      if (*(volatile int*)err != 0) break;
-      if (++polls > spin_limit) {
-        atomicOr(err, kErrTimeout);
-        break;
-      }
-      if (polls > 256) __nanosleep(polls > 8192 ? 256 : 20);
-    }
-  }
+  if (threadIdx.x == 0) arrive_wait(ctr, gen, G, err, spin_limit, extra);
   __syncthreads();
 }
 
+// CTA sums of NS values stored as this CTA's partials, with ONE CTA barrier:
+// warp sums, then thread 0 adds the eight warp sums in the xor-butterfly
+// order of warp_sum_d (the bits of a second warp-level sum) and stores them.
+// On return only thread 0 has stored; it arrives at the grid barrier next,
+// its release covering every write of the CTA ordered before the bar.sync.
+template <int NS>
+__device__ __forceinline__ void publish_sums(const double (&v)[NS], double* red, double* const (&dst)[NS]) {
+  static_assert(kThreads == 256, "eight warps per CTA");
+  const int wi = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double ws[NS];
+#pragma unroll
+  for (int k = 0; k < NS; k++) ws[k] = warp_sum_d(v[k]);
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < NS; k++) red[k * 8 + wi] = ws[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+      const double* r = red + k * 8;
+      *dst[k] = ((r[0] + r[4]) + (r[2] + r[6])) + ((r[1] + r[5]) + (r[3] + r[7]));
+    }
+  }
+}
+
 // A warp sums NS slots of the G partials of a CTA group (slot stride
-// `stride`) in one pass: all loads first, fixed order per lane, xor
-// butterfly, so every CTA gets the same bits; results to red[dst..dst+NS).
+// `stride`) in one pass: each lane issues all its loads before it adds them
+// (one round trip to L2 for up to 32 * kPartBatch CTAs), in a fixed order
+// per lane, then an xor butterfly, so every CTA gets the same bits; results
+// to red[dst..dst+NS).
+constexpr int kPartBatch = 8;
 template <int NS>
 __device__ __forceinline__ void wsum_parts(const double* parts, int G, int stride, double* red, int dst) {
   const int lane = threadIdx.x & 31;
   double v[NS];
 #pragma unroll
   for (int s = 0; s < NS; s++) v[s] = 0.0;
-  for (int k = lane; k < G; k += 32) {
-    double x[NS];
+  for (int k0 = lane; k0 < G; k0 += 32 * kPartBatch) {
+    double x[kPartBatch][NS];
 #pragma unroll
-    for (int s = 0; s < NS; s++) x[s] = __ldcg(parts + s * stride + k);
+    for (int b = 0; b < kPartBatch; b++) {
+      const int k = k0 + 32 * b;
 #pragma unroll
-    for (int s = 0; s < NS; s++) v[s] += x[s];
+      for (int s = 0; s < NS; s++) x[b][s] = (k < G) ? __ldcg(parts + s * stride + k) : 0.0;
+    }
+#pragma unroll
+    for (int b = 0; b < kPartBatch; b++)
+      if (k0 + 32 * b < G) {
+#pragma unroll
+        for (int s = 0; s < NS; s++) v[s] += x[b][s];
+      }
   }
 #pragma unroll
   for (int s = 0; s < NS; s++) {
@@ -202,15 +225,29 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
   (void)gcta;
 
   // ---- prologue: A rows, indices, halo list, FP64 block inverses ----
-  if (A_SMEM) {
-    const float4* g4 = reinterpret_cast<const float4*>(gA);
-    float4* s4 = reinterpret_cast<float4*>(sA);
-    for (int i = tid; i < nblk * 9; i += kThreads) s4[i] = __ldcg(g4 + i);
-  }
-  for (int i = tid; i < nblk; i += kThreads) sVidx[i] = pt.g_vidx[b0 + i];
+  // staged with cp.async: every copy of the CTA in flight at once, one wait
+  if (A_SMEM)
+    for (int i = tid; i < nblk * 9; i += kThreads) cp_async16(sA + 4 * i, gA + 4 * i);
+  for (int i = tid; i < nblk; i += kThreads) cp_async4(sVidx + i, pt.g_vidx + b0 + i);
+  for (int i = tid; i < nhalo; i += kThreads) cp_async4(sHalo + i, pt.g_halo_col + h0 + i);
+  // the epilogue's operands (transform, node position), loaded now so that
+  // their latency hides behind the solve
+  float4* sTn = reinterpret_cast<float4*>(smem + L.tn);
+  if (!a.delta_x)
+    for (int i = tid; i < nrows; i += kThreads) {
+      const float4* tq = reinterpret_cast<const float4*>(a.transforms + r0 + i);
+      cp_async16(sTn + 3 * i, tq);
+      cp_async16(sTn + 3 * i + 1, tq + 1);
+      const float* np = reinterpret_cast<const float*>(a.nodes + r0 + i);
+      float* sp = reinterpret_cast<float*>(sTn + 3 * i + 2);
+      cp_async4(sp, np);
+      cp_async4(sp + 1, np + 1);
+      cp_async4(sp + 2, np + 2);
+    }
   for (int i = tid; i <= nrows; i += kThreads) sRow[i] = pt.row_ptr[r0 + i] - b0;
-  for (int i = tid; i < nhalo; i += kThreads) sHalo[i] = pt.g_halo_col[h0 + i];
+  cp_async_commit_wait_all();
   __syncthreads();
+  clk.mark(12);  // A, indices
   // block-Jacobi inverses in FP64, one 8-lane group per row
   {
     double* scr = reinterpret_cast<double*>(smem + L.scr) + (tid >> 3) * 72;
@@ -224,17 +261,39 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
     }
     if (nfb) atomicAdd(&st->fallbacks, nfb);
   }
-  if (gcta == 0) {  // energy of this problem's linearisation point (fixed-order tree)
+  clk.mark(13);  // inverses
+  // The energy of this problem's linearisation point, summed by warps 1..7 of
+  // the group's first CTA while thread 0 waits at the first grid barrier:
+  // per thread in a fixed order (loads in flight together), then per warp,
+  // then the seven warp sums in a fixed tree by thread 32 after the barrier.
+  auto energy_warps = [&]() {
+    if (gcta != 0 || tid < 32) return;
+    const int n1 = pd.e_ctas, n = pd.e_ctas + pd.N;
+    const double* p1 = w.e_data_part + pd.e_cta0;
+    const double* p2 = w.e_arap_part + pd.node_off;
     double v = 0.0;
-    for (int k = tid; k < pd.e_ctas; k += kThreads) v += __ldcg(w.e_data_part + pd.e_cta0 + k);
-    for (int k = tid; k < pd.N; k += kThreads) v += __ldcg(w.e_arap_part + pd.node_off + k);
-    v = bsum(v, sRed + 32);
-    if (tid == 0) {
-      st->energy[P.slot] = v;
-      if (!isfinite(v)) atomicOr(err, kErrNonFinite);
+    for (int k0 = tid - 32; k0 < n; k0 += (kThreads - 32) * 8) {
+      double x[8];
+#pragma unroll
+      for (int b = 0; b < 8; b++) {
+        const int k = k0 + (kThreads - 32) * b;
+        x[b] = k < n1 ? __ldcg(p1 + k) : (k < n ? __ldcg(p2 + (k - n1)) : 0.0);
+      }
+#pragma unroll
+      for (int b = 0; b < 8; b++)
+        if (k0 + (kThreads - 32) * b < n) v += x[b];
     }
-  }
-  __syncthreads();
+    v = warp_sum_d(v);
+    if ((tid & 31) == 0) sRed[40 + (tid >> 5)] = v;
+  };
+  auto energy_store = [&]() {  // after a CTA barrier that follows energy_warps
+    if (gcta != 0 || tid != 32) return;
+    const double* r = sRed + 41;
+    const double v = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + r[6]);
+    st->energy[P.slot] = v;
+    if (!isfinite(v)) atomicOr(err, kErrNonFinite);
+  };
+  static_assert(kThreads == 256, "energy_store sums seven warps");
 
   // y = A v over own rows (v = sV, own rows then halo), FP32
   auto spmv_row = [&](int t) -> float {
@@ -269,6 +328,8 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
     float* sAp = sR + vs;
     float* sHz = sAp + vs;
     float* sHp = sHz + hs;
+    // lanes per row element of the SpMV: 4, 2 or 1, as many as the CTA's threads allow
+    const int spl_log = (n6 * 4 <= kThreads) ? 2 : (n6 * 2 <= kThreads) ? 1 : 0, spl = 1 << spl_log;
     double prz = 0.0, pbb = 0.0;
     for (int t = tid; t < n6; t += kThreads) {
       const float rt = __ldcg(w.rhs + r0 * 6 + t);
@@ -285,14 +346,18 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
     }
     {
       const int buf = gen & 1;
-      bsum2(prz, pbb, sRed);
-      if (tid == 0) {
-        part[(buf * 3 + 0) * GT + cta] = prz;
-        part[(buf * 3 + 1) * GT + cta] = pbb;
-      }
+      const double v2[2] = {prz, pbb};
+      double* const d2[2] = {part + (buf * 3 + 0) * GT + cta, part + (buf * 3 + 1) * GT + cta};
+      publish_sums<2>(v2, sRed, d2);
     }
     clk.mark(0);  // prologue
-    gbar(bar, gen++, G, cta, err, a.spin_limit, a.bar_extra);
+    if (tid == 0)
+      arrive_wait(bar, gen, G, err, a.spin_limit, a.bar_extra);
+    else
+      energy_warps();
+    gen++;
+    __syncthreads();
+    energy_store();
     clk.mark(1);  // first barrier
     double rz = 0.0;
     float betaf = 0.f;
@@ -336,21 +401,41 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
       __syncthreads();
       clk.mark(3);  // p update
       // ---- Ap (solver_kernels.cu:406-432) and p.Ap ----
+      // S adjacent lanes per row element, lane k over the row's blocks k, k+S, ...,
+      // combined by an xor butterfly: the CTA's time is its longest row / S
       double ppap = 0.0;
-      for (int t = tid; t < n6; t += kThreads) {
-        const float y = spmv_row(t);
-        sAp[t] = y;
-        ppap += (double)sV[t] * y;
+      for (int u0 = 0; u0 < n6 * spl; u0 += kThreads) {
+        const int u = u0 + tid, t = u >> spl_log, k = u & (spl - 1);
+        float y = 0.f;
+        if (t < n6) {
+          const int i = t / 6, c = t % 6;
+          for (int bl = sRow[i] + k; bl < sRow[i + 1]; bl += spl) {
+            const float* Ab = A_SMEM ? (sA + bl * 36 + c * 6) : (gA + bl * 36 + c * 6);
+            const float* vv = sV + sVidx[bl] * 6;
+#pragma unroll
+            for (int q = 0; q < 6; q++) y = __fmaf_rn(A_SMEM ? Ab[q] : __ldcg(Ab + q), vv[q], y);
+          }
+        }
+        for (int o = spl >> 1; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+        if (k == 0 && t < n6) {
+          sAp[t] = y;
+          ppap += (double)sV[t] * y;
+        }
       }
       clk.mark(4);  // spmv
       {
-        const double t1 = bsum(ppap, sRed);
-        if (tid == 0) part[((gen & 1) * 3 + 0) * GT + cta] = t1;
+        const double v1[1] = {ppap};
+        double* const d1[1] = {part + ((gen & 1) * 3 + 0) * GT + cta};
+        publish_sums<1>(v1, sRed, d1);
       }
       clk.mark(5);  // block sum
-      gbar(bar, gen++, G, cta, err, a.spin_limit, a.bar_extra);
-      clk.mark(6);  // barrier A
-      if (tid < 32) wsum_parts<1>(part + (((gen - 1) & 1) * 3 + 0) * GT + gb, G, GT, sRed, 18);
+      if (tid < 32) {  // warp 0 waits and reads the partials; the others wait at the CTA barrier
+        if (tid == 0) arrive_wait(bar, gen, G, err, a.spin_limit, a.bar_extra);
+        clk.mark(6);  // barrier A
+        __syncwarp();
+        wsum_parts<1>(part + ((gen & 1) * 3 + 0) * GT + gb, G, GT, sRed, 18);
+      }
+      gen++;
       __syncthreads();
       clk.mark(7);  // pAp partials
       const double pAp = sRed[18];
@@ -372,14 +457,14 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
       clk.mark(8);  // x, r, z updates
       {
         const int buf = gen & 1;
-        bsum2(prr, przn, sRed);
-        if (tid == 0) {
-          part[(buf * 3 + 0) * GT + cta] = prr;
-          part[(buf * 3 + 1) * GT + cta] = przn;
-        }
+        const double v2[2] = {prr, przn};
+        double* const d2[2] = {part + (buf * 3 + 0) * GT + cta, part + (buf * 3 + 1) * GT + cta};
+        publish_sums<2>(v2, sRed, d2);
       }
       clk.mark(9);  // block sums
-      gbar(bar, gen++, G, cta, err, a.spin_limit, a.bar_extra);
+      if (tid == 0) arrive_wait(bar, gen, G, err, a.spin_limit, a.bar_extra);
+      gen++;
+      __syncthreads();
       clk.mark(10);  // barrier B
     }
     // ---- epilogue ----
@@ -391,9 +476,13 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
     } else {
       for (int i = tid; i < nrows; i += kThreads) {
         const int node = r0 + i;
-        DQ Tn = twist_update(load_dq_cg(a.transforms + node), sX + i * 6, pd.max_rot, pd.max_trans, pd.update_scale);
+        DQ T0;
+        T0.r = sTn[3 * i];
+        T0.d = sTn[3 * i + 1];
+        const float4 xp = sTn[3 * i + 2];
+        DQ Tn = twist_update(T0, sX + i * 6, pd.max_rot, pd.max_trans, pd.update_scale);
         store_dq(a.transforms + node, Tn);
-        store_dq(w.plain + node, dq_centered(Tn, node_pos(a.nodes, node)));
+        store_dq(w.plain + node, dq_centered(Tn, f3(xp.x, xp.y, xp.z)));
       }
     }
   } else {
@@ -422,7 +511,14 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
       sV[t] = uf;
       xb[gen & 1][r0 * 6 + t] = uf;
     }
-    gbar(bar, gen++, G, cta, err, a.spin_limit, a.bar_extra);
+    __syncthreads();
+    if (tid == 0)
+      arrive_wait(bar, gen, G, err, a.spin_limit, a.bar_extra);
+    else
+      energy_warps();
+    gen++;
+    __syncthreads();
+    energy_store();
     for (int e = tid; e < h6; e += kThreads) sV[n6 + e] = __ldcg(xb[(gen - 1) & 1] + sHalo[e / 6] * 6 + e % 6);
     __syncthreads();
     // w = A u ; then the first reduction and m = M^-1 w
@@ -516,9 +612,13 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
     } else {
       for (int i = tid; i < nrows; i += kThreads) {
         const int node = r0 + i;
-        DQ Tn = twist_update(load_dq_cg(a.transforms + node), xf + i * 6, pd.max_rot, pd.max_trans, pd.update_scale);
+        DQ T0;
+        T0.r = sTn[3 * i];
+        T0.d = sTn[3 * i + 1];
+        const float4 xp = sTn[3 * i + 2];
+        DQ Tn = twist_update(T0, xf + i * 6, pd.max_rot, pd.max_trans, pd.update_scale);
         store_dq(a.transforms + node, Tn);
-        store_dq(w.plain + node, dq_centered(Tn, node_pos(a.nodes, node)));
+        store_dq(w.plain + node, dq_centered(Tn, f3(xp.x, xp.y, xp.z)));
       }
     }
   }
