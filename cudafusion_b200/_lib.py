@@ -27,6 +27,7 @@ CF_OPT_GRAPH_ACTIVE = 6
 CF_OPT_SPIN_LIMIT = 7
 CF_OPT_TEST_BARRIER_EXTRA = 8
 CF_OPT_STREAM_TILE = 9
+CF_OPT_PCG_ACTIVE = 10
 CF_MAX_GN_ITERS = 32
 CF_PROF_SLOTS = 12
 CF_MPNN_IN = 20

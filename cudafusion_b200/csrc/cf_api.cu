@@ -111,8 +111,8 @@ void free_pattern(Pattern& p) {
   dfree(p.upper_pos); dfree(p.upper_row); dfree(p.arap_row_ptr); dfree(p.arap_row_inc);
   dfree(p.arap_blk_ptr); dfree(p.arap_blk_edge); dfree(p.edge_ijk); dfree(p.values);
   dfree(p.seg_off); dfree(p.seg_cnt); dfree(p.pcg_row_begin);
-  dfree(p.clu_row_begin); dfree(p.cta_of_row); dfree(p.ustart); dfree(p.low_ptr); dfree(p.low_pack);
-  dfree(p.low_jl); dfree(p.g_vidx); dfree(p.g_halo_ptr); dfree(p.g_halo_col);
+  dfree(p.clu_row_begin); dfree(p.ustart); dfree(p.low_ptr); dfree(p.clu_opnd); dfree(p.clu_push);
+  dfree(p.clu_halo_ptr); dfree(p.clu_halo); dfree(p.g_vidx); dfree(p.g_halo_ptr); dfree(p.g_halo_col);
   dfree(p.off_upper); dfree(p.pcg_cta_off); dfree(p.pcg_prob); dfree(p.prob_edge_off);
   dfree(p.st_tile_ptr); dfree(p.st_tile_row); dfree(p.edge_terms); dfree(p.edge_energy);
   p = Pattern();
@@ -499,74 +499,92 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
     edge_off[q] = (q < P) ? e : n_edges;
   }
 
-  // single-cluster PCG plan: rows split over C CTAs by block count; the upper
-  // blocks live in the owner's shared memory, lower blocks are read from the
-  // owner of their transpose
-  std::vector<int> ustart(N + 1, 0), low_ptr(N + 1, 0), low_u, low_j;
+  // single-cluster PCG plan: rows split over C CTAs in contiguous ranges of
+  // balanced UPPER block counts (what each CTA keeps in shared memory and
+  // multiplies twice).  Per upper block: the operand slot of its column (own
+  // row, or the CTA's halo) and, off the diagonal, where its transposed
+  // product goes: the owner of the column and the receive slot of the lower
+  // block there (row j's lower blocks in order of their row i).
+  std::vector<int> ustart(N + 1, 0), low_ptr(N + 1, 0), low_of_upper(std::max(1, n_upper), -1);
   for (int i = 0; i < N; i++) ustart[i + 1] = ustart[i] + (row_ptr[i + 1] - diag_pos[i]);
   {
-    std::vector<std::vector<std::pair<int, int>>> lows(N);  // row i: (j, u of (j, i))
+    std::vector<std::vector<std::pair<int, int>>> lows(N);  // row i: (j, u of (j, i)), j < i
     for (int j = 0; j < N; j++)
       for (int q = diag_pos[j] + 1; q < row_ptr[j + 1]; q++) lows[col_idx[q]].push_back({j, upper_of_pos[q]});
     for (int i = 0; i < N; i++) {
       std::sort(lows[i].begin(), lows[i].end());
       low_ptr[i + 1] = low_ptr[i] + (int)lows[i].size();
-      for (auto& pr : lows[i]) {
-        low_j.push_back(pr.first);
-        low_u.push_back(pr.second);
-      }
+      for (size_t k = 0; k < lows[i].size(); k++) low_of_upper[lows[i][k].second] = low_ptr[i] + (int)k;
     }
   }
-  int clu_C = 0, clu_smem = 0, clu_nup = 0, clu_nlow = 0, clu_rows = 0;
-  std::vector<int> clu_rb, cta_of_row(N, 0), low_pack(std::max<size_t>(1, low_u.size())),
-      low_jl(std::max<size_t>(1, low_u.size()));
+  int clu_C = 0, clu_smem = 0, clu_nup = 0, clu_nlow = 0, clu_rows = 0, clu_nhalo = 0;
+  std::vector<int> clu_rb, clu_opnd(std::max(1, n_upper)), clu_push(std::max(1, n_upper)), clu_hptr, clu_halo;
   if (h->pcg_mode != 1 && h->pcg_mode != 3 && !stream && P == 1) {
     const int cands[2] = {16, 8};
     for (int ci = 0; ci < 2 && !clu_C; ci++) {
       const int C = cands[ci];
       if (N < C) continue;
-      // contiguous row ranges balanced by row degree (upper + lower blocks)
+      // automatic choice: the cluster's 16 SMs win while each holds few rows
+      // (measured on B200: 54 vs 62 us per PCG at 16 rows per CTA, 169 vs 107
+      // at 128); past ~32 rows per CTA the grid-wide kernel is faster
+      if (h->pcg_mode == 0 && N > kClusterAutoRows * C) continue;
       std::vector<int> rb(1, 0);
-      long long target = ((long long)nnzb + C - 1) / C;
+      const long long target = ((long long)n_upper + C - 1) / C;
       int start = 0;
       for (int c = 0; c < C; c++) {
-        int rem = C - c;
+        const int rem = C - c;
         int end = start + 1;
         if (rem == 1) {
           end = N;
         } else {
-          while (end < N - (rem - 1) && row_ptr[end] - row_ptr[start] < target) end++;
+          while (end < N - (rem - 1) && ustart[end] - ustart[start] < target) end++;
         }
         rb.push_back(end);
         start = end;
       }
-      int nu = 0, nl = 0, nr = 0;
+      std::vector<int> owner(N);
+      for (int c = 0; c < C; c++)
+        for (int r = rb[c]; r < rb[c + 1]; r++) owner[r] = c;
+      std::vector<int> hptr(1, 0), halo;
+      int nu = 0, nl = 0, nr = 0, nh = 0;
       for (int c = 0; c < C; c++) {
-        nu = std::max(nu, ustart[rb[c + 1]] - ustart[rb[c]]);
-        nl = std::max(nl, low_ptr[rb[c + 1]] - low_ptr[rb[c]]);
-        nr = std::max(nr, rb[c + 1] - rb[c]);
+        const int r0 = rb[c], r1 = rb[c + 1];
+        std::vector<int> cols;  // remote columns of the CTA's upper blocks (all > r1 - 1)
+        for (int u = ustart[r0]; u < ustart[r1]; u++) {
+          const int j = col_idx[upper_pos[u]];
+          if (j >= r1) cols.push_back(j);
+        }
+        std::sort(cols.begin(), cols.end());
+        cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+        for (int u = ustart[r0]; u < ustart[r1]; u++) {
+          const int q = upper_pos[u], j = col_idx[q];
+          clu_opnd[u] = (j < r1) ? j - r0
+                                 : (r1 - r0) + (int)(std::lower_bound(cols.begin(), cols.end(), j) - cols.begin());
+          clu_push[u] = (q == diag_pos[upper_row[u]])
+                            ? -1
+                            : (owner[j] << 24) | (low_of_upper[u] - low_ptr[rb[owner[j]]]);
+        }
+        for (int j : cols) halo.push_back((owner[j] << 24) | (j - rb[owner[j]]));
+        hptr.push_back((int)halo.size());
+        nu = std::max(nu, ustart[r1] - ustart[r0]);
+        nl = std::max(nl, low_ptr[r1] - low_ptr[r0]);
+        nr = std::max(nr, r1 - r0);
+        nh = std::max(nh, (int)cols.size());
       }
-      int sm = pcg_cluster_smem_bytes(nu, nl, nr, C, true);
+      const int sm = pcg_cluster_smem_bytes(nu, nl, nr, nh, C);
       if (sm > 227 * 1024 - 1024) continue;
-      if (pcg_cluster_max_active(C, sm, true) < 1) continue;
+      if (pcg_cluster_max_active(C, sm) < 1) continue;
       clu_C = C;
       clu_smem = sm;
       clu_nup = nu;
       clu_nlow = nl;
       clu_rows = nr;
+      clu_nhalo = nh;
       clu_rb = rb;
-    }
-    if (clu_C) {
-      for (int c = 0; c < clu_C; c++)
-        for (int r = clu_rb[c]; r < clu_rb[c + 1]; r++) cta_of_row[r] = c;
-      for (size_t l = 0; l < low_u.size(); l++) {
-        int j = low_j[l], owner = cta_of_row[j];
-        low_pack[l] = (owner << 24) | (low_u[l] - ustart[clu_rb[owner]]);
-        low_jl[l] = j - clu_rb[owner];
-      }
+      clu_hptr = hptr;
+      clu_halo = halo;
     }
   }
-
   free_pattern(h->p);
   Pattern& p = h->p;
   p.P = P;
@@ -619,17 +637,18 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
   p.use_cluster = clu_C ? 1 : 0;
   p.clu_C = clu_C;
   p.clu_smem = clu_smem;
-  p.clu_a_in_smem = 1;
   p.clu_nup_max = clu_nup;
   p.clu_nlow_max = clu_nlow;
   p.clu_rows_max = clu_rows;
+  p.clu_halo_max = clu_nhalo;
   CF_TRY(up(&p.ustart, ustart));
   CF_TRY(up(&p.low_ptr, low_ptr));
   if (clu_C) {
     CF_TRY(up(&p.clu_row_begin, clu_rb));
-    CF_TRY(up(&p.cta_of_row, cta_of_row));
-    CF_TRY(up(&p.low_pack, low_pack));
-    CF_TRY(up(&p.low_jl, low_jl));
+    CF_TRY(up(&p.clu_opnd, clu_opnd));
+    CF_TRY(up(&p.clu_push, clu_push));
+    CF_TRY(up(&p.clu_halo_ptr, clu_hptr));
+    CF_TRY(up(&p.clu_halo, clu_halo.empty() ? std::vector<int>(1, 0) : clu_halo));
   }
   CF_TRY(dalloc(&p.values, (size_t)nnzb * 36));
   CF_TRY(dalloc(&p.seg_off, (size_t)nnzb));
@@ -1040,6 +1059,9 @@ cf_status cf_gn_get_option(const cf_gn* h, int option, int* value) {
     case CF_OPT_SPIN_LIMIT: *value = (int)h->spin_limit; return CF_OK;
     case CF_OPT_TEST_BARRIER_EXTRA: *value = (int)h->bar_extra; return CF_OK;
     case CF_OPT_STREAM_TILE: *value = h->stream_tile; return CF_OK;
+    case CF_OPT_PCG_ACTIVE:
+      *value = !h->pattern_valid ? 0 : h->p.use_cluster ? 2 : h->p.pcg_stream ? 3 : 1;
+      return CF_OK;
   }
   return CF_ERR_INVALID_ARG;
 }
@@ -1238,6 +1260,7 @@ cf_status cf_gn_autotune(cf_gn* h, const cf_problem* problems, int num_problems,
   };
   std::vector<Cand> cands = {{mode0, ctas0, tile0}};  // the configuration in effect first: the baseline
   for (int ctas : {0, h->sms, 2 * h->sms}) cands.push_back({1, ctas, 256});
+  if (num_problems == 1) cands.push_back({2, 0, 256});
   for (int tile : {256, 128})
     for (int ctas : {0, h->sms}) cands.push_back({3, ctas, tile});
   double best = 1e30, baseline = 0.0;

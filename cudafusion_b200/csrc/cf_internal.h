@@ -92,14 +92,14 @@ struct Pattern {
   int use_cluster = 0;
   int clu_C = 0;
   int clu_smem = 0;
-  int clu_a_in_smem = 0;
-  int clu_nup_max = 0, clu_nlow_max = 0, clu_rows_max = 0;
+  int clu_nup_max = 0, clu_nlow_max = 0, clu_rows_max = 0, clu_halo_max = 0;
   int* clu_row_begin = nullptr;  // [clu_C+1]
-  int* cta_of_row = nullptr;     // [N]
   int* ustart = nullptr;         // [N+1] first upper index of each row
-  int* low_ptr = nullptr;        // [N+1] lower blocks (j, i), j < i, of row i
-  int* low_pack = nullptr;       // (owner CTA << 24) | slot of block (j, i) in the owner's upper blocks
-  int* low_jl = nullptr;         // row j local to its owner CTA
+  int* low_ptr = nullptr;        // [N+1] lower blocks (j, i), j < i, of row i, in order of j
+  int* clu_opnd = nullptr;       // [n_upper] operand slot of the block's column in its CTA: own row, or rows + halo slot
+  int* clu_push = nullptr;       // [n_upper] off-diagonal (i, j): (owner of row j << 24) | receive slot of (j, i) there; -1 diagonal
+  int* clu_halo_ptr = nullptr;   // [clu_C+1]
+  int* clu_halo = nullptr;       // per CTA, its remote columns: (owner << 24) | row local to the owner
   // grid PCG partition
   int pcg_ctas = 0;
   int* pcg_row_begin = nullptr;  // [pcg_ctas+1]
@@ -159,6 +159,7 @@ struct Work {
 
 constexpr int kEnergyCtas = 592;  // residual/energy CTAs of a single solve
 constexpr int kMaxPcgCtas = 1024;
+constexpr int kClusterAutoRows = 32;  // rows per CTA up to which mode 0 picks the single-cluster PCG
 constexpr int kMaxProblems = 1024;       // problems per batched solve
 constexpr int kMaxProblemNodes = 48000;  // nodes per problem (per-CTA histograms in shared memory)
 
@@ -181,6 +182,35 @@ struct SolveArgs {
   Table tb;           // the problems of this solve
 };
 constexpr int kTimerSlots = 16;
+
+#ifdef __CUDACC__
+// clock64 phase timer of one thread of the persistent PCG kernels (debug;
+// a.timers == nullptr disables it)
+struct PhaseClock {
+  long long* out;
+  long long last;
+  long long acc[kTimerSlots];
+  __device__ PhaseClock(long long* o) : out(o), last(0) {
+#ifdef __CUDA_ARCH__
+    last = clock64();
+#endif
+    for (int i = 0; i < kTimerSlots; i++) acc[i] = 0;
+  }
+  __device__ __forceinline__ void mark(int slot) {
+#ifdef __CUDA_ARCH__
+    if (!out) return;
+    const long long t = clock64();
+    acc[slot] += t - last;
+    last = t;
+#endif
+  }
+  __device__ void flush() {
+    if (!out) return;
+    for (int i = 0; i < kTimerSlots; i++) atomicAdd(reinterpret_cast<unsigned long long*>(out + i), (unsigned long long)acc[i]);
+  }
+};
+#endif
+
 
 // ---- launchers (cf_kernels.cu) ----
 cudaError_t launch_pack_count(const Work& w, const Table& tb, cudaStream_t s);
@@ -208,8 +238,8 @@ int pcg_grid_smem_bytes(int nblk, int nrows, int nhalo, bool a_in_smem, bool pip
 int pcg_max_active_ctas(int smem, bool a_in_smem, bool pipelined);
 int expand_smem_bytes(int max_upper_row);
 
-int pcg_cluster_smem_bytes(int nup_max, int nlow_max, int rows_max, int C, bool a_in_smem);
-int pcg_cluster_max_active(int C, int smem, bool a_in_smem);
+int pcg_cluster_smem_bytes(int nup_max, int nlow_max, int rows_max, int nhalo_max, int C);
+int pcg_cluster_max_active(int C, int smem);
 cudaError_t launch_pcg_cluster(const Work& w, const Pattern& p, const SolveArgs& a, int gn_slot, cudaStream_t s);
 
 // The learned initial increment (cf_mpnn.cu): parameters, graph, activations.

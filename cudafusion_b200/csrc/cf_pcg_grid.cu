@@ -164,31 +164,6 @@ __device__ __forceinline__ void wsum_parts(const double* parts, int G, int strid
   }
 }
 
-// phase timer of CTA 0, thread 0 (debug; a.timers == nullptr disables it)
-struct PhaseClock {
-  long long* out;
-  long long last;
-  long long acc[kTimerSlots];
-  __device__ PhaseClock(long long* o) : out(o), last(0) {
-#ifdef __CUDA_ARCH__
-    last = clock64();
-#endif
-    for (int i = 0; i < kTimerSlots; i++) acc[i] = 0;
-  }
-  __device__ __forceinline__ void mark(int slot) {
-#ifdef __CUDA_ARCH__
-    if (!out) return;
-    const long long t = clock64();
-    acc[slot] += t - last;
-    last = t;
-#endif
-  }
-  __device__ void flush() {
-    if (!out) return;
-    for (int i = 0; i < kTimerSlots; i++) atomicAdd(reinterpret_cast<unsigned long long*>(out + i), (unsigned long long)acc[i]);
-  }
-};
-
 template <bool A_SMEM, bool PIPE>
 __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -632,7 +607,13 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
 
 template <bool A, bool PP>
 cudaError_t set_smem(int smem) {
-  return cudaFuncSetAttribute(pcg_grid_kernel<A, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  // the device's opt-in maximum, not this plan's size: another handle's plan
+  // (with more shared memory) launches the same kernel
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (smem > optin) return cudaErrorInvalidValue;
+  return cudaFuncSetAttribute(pcg_grid_kernel<A, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
 }
 
 template <bool A, bool PP>

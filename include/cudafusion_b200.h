@@ -155,11 +155,14 @@ CF_API cf_status cf_gn_linearize_solve(cf_gn* h, const cf_correspondence* d_corr
  *                          update.  With 0 the GN energy can rise for large
  *                          lambda_smooth, exactly as in the reference.
  *  CF_OPT_PCG_CTAS         CTAs of the grid-wide PCG kernel (0 = automatic).
- *  CF_OPT_PCG_MODE         0: automatic; 1: grid-wide cooperative PCG with
- *                          the system in shared memory (streaming when it
- *                          does not fit); 2: single-cluster PCG when the
- *                          system fits the cluster's shared memory (else
- *                          grid-wide); 3: streaming PCG (A re-read from HBM
+ *  CF_OPT_PCG_MODE         0: automatic (single cluster up to 32 rows per
+ *                          CTA of a 16-CTA cluster, else grid-wide or, past
+ *                          the GPU's shared memory, streaming); 1: grid-wide
+ *                          cooperative PCG with the system in shared memory
+ *                          (streaming when it does not fit); 2: single-
+ *                          cluster PCG (upper blocks in distributed shared
+ *                          memory) when the system fits the cluster's shared
+ *                          memory (else grid-wide); 3: streaming PCG (A re-read from HBM
  *                          through TMA bulk copies every iteration, vectors
  *                          in global memory; the automatic choice for systems
  *                          larger than the GPU's shared memory).
@@ -195,6 +198,9 @@ CF_API cf_status cf_gn_linearize_solve(cf_gn* h, const cf_correspondence* d_corr
 #define CF_OPT_TEST_BARRIER_EXTRA 8
 /* Blocks per shared-memory tile of the streaming PCG: 256 (default) or 128. */
 #define CF_OPT_STREAM_TILE 9
+/* read only: the PCG kernel the current pattern runs (0 before the first
+ * solve, 1 grid-wide, 2 single cluster, 3 streaming) */
+#define CF_OPT_PCG_ACTIVE 10
 CF_API cf_status cf_gn_set_option(cf_gn* h, int option, int value);
 CF_API cf_status cf_gn_get_option(const cf_gn* h, int option, int* value);
 

@@ -120,6 +120,30 @@ def test_pcg_modes_agree(p1):
     assert np.abs(out[0] - out[3]).max() < 1e-5  # shared-memory vs streaming (FP32-stored inverses)
 
 
+def test_pcg_kernel_choice_and_full_frame_cluster():
+    """Mode 0 runs the single-cluster PCG on a small problem and the grid-wide
+    one on the full frame; forced onto one 16-CTA cluster, the full frame
+    (2048 nodes, upper blocks in distributed shared memory, transposed
+    products pushed between CTAs) lands on the grid-wide result (well
+    conditioned: consistent ARAP Jacobian, damping 1)."""
+    prm = Params(gn_iterations=2, pcg_iterations=10, pcg_tolerance=0.0, lambda_smooth=10.0, lambda_damping=1.0)
+    p2 = synth.config2()
+    dp = DeviceProblem(p2)
+    out, active = [], []
+    for mode in (0, 1, 2):
+        s = make_solver(prm, max_corrs=p2.num_corrs, mode=(mode, 0), consistent=True)
+        T = dp.init_transforms.clone()
+        st = s.gn_solve(dp, T, max_rot=0.12, max_trans=0.04)
+        assert st["error_flags"] == 0
+        active.append(s.get_option(_lib.CF_OPT_PCG_ACTIVE))
+        out.append(dq_as_array(T.cpu().numpy().view(DQ_DTYPE)))
+    assert active == [1, 1, 2]
+    assert np.abs(out[1] - out[2]).max() < 1e-5
+    s = make_solver(prm, mode=(0, 0))
+    s.gn_solve(DeviceProblem(synth.config1()), DeviceProblem(synth.config1()).init_transforms.clone(), 0.12, 0.04)
+    assert s.get_option(_lib.CF_OPT_PCG_ACTIVE) == 2
+
+
 @pytest.mark.parametrize("mode", MODES)
 def test_deterministic(p1, mode):
     prm = Params(gn_iterations=5, pcg_iterations=10, pcg_tolerance=0.0, lambda_smooth=10.0)
