@@ -273,6 +273,8 @@ cf_status prepare_table(cf_gn* h, std::vector<ProbDesc> in, bool single, cudaStr
   t.M = (int)Mt;
   t.N = (int)Nt;
   t.max_N = maxN;
+  t.max_chunk = 0;
+  for (int p = 0; p < P; p++) t.max_chunk = std::max(t.max_chunk, in[p].chunk);
   return CF_OK;
 }
 

@@ -51,6 +51,7 @@ struct Table {
   int n_bin = 0, n_e = 0;    // total sort / energy CTAs
   int M = 0, N = 0;          // concatenated sizes
   int max_N = 0;             // largest problem (shared-memory histograms)
+  int max_chunk = 0;         // most correspondences of one sort CTA
   ProbDesc* desc = nullptr;  // [P]
   int* bin_prob = nullptr;   // [n_bin] problem of each sort CTA
   int* e_prob = nullptr;     // [n_e] problem of each energy CTA

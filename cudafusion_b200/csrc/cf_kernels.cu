@@ -118,19 +118,48 @@ __global__ void __launch_bounds__(kThreads) pack_count_kernel(Table tb, Work w) 
 }
 
 // Per node: exclusive prefix of its counts over its problem's sort CTAs (in
-// place); node_total[n] = sum.
-__global__ void bin_scan_nodes_kernel(Table tb, Work w) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= tb.N) return;
-  const ProbDesc d = tb.desc[tb.node_prob[n]];
-  int* p = w.cnt + d.cnt_off + (n - d.node_off);
-  int run = 0;
-  for (int k = 0; k < d.bin_ctas; k++, p += d.N) {
-    const int v = *p;
-    *p = run;
-    run += v;
+// place); node_total[n] = sum.  32 nodes per CTA, lane = node (coalesced
+// over the sort-CTA index k); the k range is split over the 8 warps: segment
+// sums with all loads in flight, a prefix over the warps, then each warp
+// rewrites its segment.
+__global__ void __launch_bounds__(kThreads) bin_scan_nodes_kernel(Table tb, Work w) {
+  __shared__ int seg[kThreads / 32][32];
+  const int lane = lane_id(), wid = threadIdx.x >> 5;
+  const int n = blockIdx.x * 32 + lane;
+  int bc = 0, stride = 0;
+  int* p = nullptr;
+  if (n < tb.N) {
+    const ProbDesc& d = tb.desc[tb.node_prob[n]];
+    bc = d.bin_ctas;
+    stride = d.N;
+    p = w.cnt + d.cnt_off + (n - d.node_off);
   }
-  w.node_total[n] = run;
+  const int per = (bc + kThreads / 32 - 1) / (kThreads / 32);
+  const int k0 = min(bc, wid * per), k1 = min(bc, k0 + per);
+  int s = 0;
+  for (int k = k0; k < k1; k += 8) {
+    int v[8];
+#pragma unroll
+    for (int b = 0; b < 8; b++) v[b] = (k + b < k1) ? p[(size_t)(k + b) * stride] : 0;
+#pragma unroll
+    for (int b = 0; b < 8; b++) s += v[b];
+  }
+  seg[wid][lane] = s;
+  __syncthreads();
+  int run = 0;
+  for (int v = 0; v < wid; v++) run += seg[v][lane];
+  if (wid == kThreads / 32 - 1 && n < tb.N) w.node_total[n] = run + s;
+  for (int k = k0; k < k1; k += 8) {
+    int v[8];
+#pragma unroll
+    for (int b = 0; b < 8; b++) v[b] = (k + b < k1) ? p[(size_t)(k + b) * stride] : 0;
+#pragma unroll
+    for (int b = 0; b < 8; b++)
+      if (k + b < k1) {
+        p[(size_t)(k + b) * stride] = run;
+        run += v[b];
+      }
+  }
 }
 
 // inc_start = exclusive scan of node_total (one CTA of 1024 threads).
@@ -230,6 +259,91 @@ __global__ void __launch_bounds__(kThreads) bin_scatter_kernel(Table tb, Work w)
       __syncthreads();
       if (is_last) cursor[key] = pos + 1;
       __syncthreads();
+    }
+  }
+}
+
+// Stable scatter of incidences with per-warp cursors (problems of at most
+// kWarpScatterNodes nodes): the sort CTA's correspondences are split into 8
+// contiguous warp ranges; order within a node = (warp range, round of 32
+// correspondences, slot, lane).  Pass 1 counts per (warp, node) in 16-bit
+// shared counters, pass 2 turns them into offsets below the CTA's base, pass
+// 3 writes; no CTA barrier inside a pass.
+constexpr int kScatterWarps = kThreads / 32;
+constexpr int kWarpScatterSmem = 200 * 1024;
+__device__ __forceinline__ int scatter_key(const ProbDesc& d, bool live, int a, const int4& ids, const float4& ws,
+                                           float we) {
+  if (!live) return -1;
+  const int id = sel4i(ids, a);
+  return (we > 0.f && id >= 0 && sel4(ws, a) > 1e-8f) ? id - d.node_off : -1;
+}
+__global__ void __launch_bounds__(kThreads) bin_scatter_warp_kernel(Table tb, Work w) {
+  extern __shared__ int sbase[];  // [N] CTA base of each node, then [8][N] 16-bit warp offsets
+  const int tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
+  const ProbDesc d = tb.desc[tb.bin_prob[blockIdx.x]];
+  const int N = d.N, lc = blockIdx.x - d.bin_cta0;
+  unsigned short* wcnt = reinterpret_cast<unsigned short*>(sbase + N);
+  unsigned short* mine = wcnt + (size_t)warp * N;
+  const int* base = w.cnt + d.cnt_off + (size_t)lc * N;
+  for (int i = tid; i < N; i += kThreads) sbase[i] = w.inc_start[d.node_off + i] + base[i];
+  for (int i = tid; i < kScatterWarps * N; i += kThreads) wcnt[i] = 0;
+  const int cb = d.corr_off + lc * d.chunk;
+  const int ce = d.corr_off + min(d.M, lc * d.chunk + d.chunk);
+  const int per = (ce - cb + kScatterWarps - 1) / kScatterWarps;
+  const int wb = min(ce, cb + warp * per), we_ = min(ce, wb + per);
+  __syncthreads();
+  // pass 1: counts per (warp, node)
+  for (int t0 = wb; t0 < we_; t0 += 32) {
+    const int c = t0 + lane;
+    const bool live = c < we_;
+    int4 ids = make_int4(-1, -1, -1, -1);
+    float4 ws = make_float4(0.f, 0.f, 0.f, 0.f);
+    float wgt = 0.f;
+    if (live) {
+      ids = w.pk_ids[c];
+      ws = w.pk_ws[c];
+      wgt = w.pk_src[c].w;
+    }
+#pragma unroll
+    for (int a = 0; a < kK; a++) {
+      const int key = scatter_key(d, live, a, ids, ws, wgt);
+      const unsigned peers = __match_any_sync(0xffffffffu, key);
+      if (key >= 0 && (__ffs(peers) - 1) == lane) mine[key] += (unsigned short)__popc(peers);
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  // pass 2: per node, the warps' offsets below the CTA base
+  for (int i = tid; i < N; i += kThreads) {
+    unsigned run = 0;
+#pragma unroll
+    for (int v = 0; v < kScatterWarps; v++) {
+      const unsigned t = wcnt[(size_t)v * N + i];
+      wcnt[(size_t)v * N + i] = (unsigned short)run;
+      run += t;
+    }
+  }
+  __syncthreads();
+  // pass 3: the writes, in the order of pass 1
+  for (int t0 = wb; t0 < we_; t0 += 32) {
+    const int c = t0 + lane;
+    const bool live = c < we_;
+    int4 ids = make_int4(-1, -1, -1, -1);
+    float4 ws = make_float4(0.f, 0.f, 0.f, 0.f);
+    float wgt = 0.f;
+    if (live) {
+      ids = w.pk_ids[c];
+      ws = w.pk_ws[c];
+      wgt = w.pk_src[c].w;
+    }
+#pragma unroll
+    for (int a = 0; a < kK; a++) {
+      const int key = scatter_key(d, live, a, ids, ws, wgt);
+      const unsigned peers = __match_any_sync(0xffffffffu, key);
+      if (key >= 0) w.inc[sbase[key] + mine[key] + __popc(peers & lanemask_lt())] = (c << 2) | a;
+      __syncwarp();
+      if (key >= 0 && (__ffs(peers) - 1) == lane) mine[key] += (unsigned short)__popc(peers);
+      __syncwarp();
     }
   }
 }
@@ -500,13 +614,22 @@ cudaError_t launch_pack_count(const Work& w, const Table& tb, cudaStream_t s) {
 
 cudaError_t launch_bin_scan(const Work& w, const Table& tb, cudaStream_t s) {
   if (tb.N <= 0) return cudaSuccess;
-  bin_scan_nodes_kernel<<<cdiv(tb.N, 128), 128, 0, s>>>(tb, w);
+  bin_scan_nodes_kernel<<<cdiv(tb.N, 32), kThreads, 0, s>>>(tb, w);
   bin_scan_total_kernel<<<1, 1024, 0, s>>>(w, tb.N);
   return cudaGetLastError();
 }
 
 cudaError_t launch_bin_scatter(const Work& w, const Table& tb, cudaStream_t s) {
   if (tb.n_bin <= 0) return cudaSuccess;
+  // per-warp cursors: 20 B of shared memory per node, counts below 2^16
+  const int wsmem = tb.max_N * (int)(sizeof(int) + kScatterWarps * sizeof(unsigned short));
+  if (wsmem <= kWarpScatterSmem && (long long)tb.max_chunk * kK < 65536) {
+    cudaError_t e = cudaFuncSetAttribute(bin_scatter_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kWarpScatterSmem);
+    if (e != cudaSuccess) return e;
+    bin_scatter_warp_kernel<<<tb.n_bin, kThreads, wsmem, s>>>(tb, w);
+    return cudaGetLastError();
+  }
   const int smem = tb.max_N * (int)sizeof(int);
   cudaError_t e = cudaFuncSetAttribute(bin_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
