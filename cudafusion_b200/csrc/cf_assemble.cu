@@ -20,7 +20,8 @@ namespace cf {
 namespace {
 
 constexpr int kWarps = kThreads / 32;
-constexpr int kEpl = 4;  // incidences per lane per round of expand
+constexpr int kEpl = 2;  // incidences per lane per round of expand
+constexpr int kExpandStage = 2048;  // incidences of a row kept in shared memory between the passes of expand
 constexpr int kStageCap = 768;  // incidences of a row staged by the assembly (51 KB with their entries)
 constexpr int kRowEdges = 64;   // ARAP edges of a row / of its upper blocks staged by the assembly
 constexpr int kRound = 32 * kEpl;
@@ -45,10 +46,12 @@ __device__ __forceinline__ int key_of(int2 kk, int b) {
 
 __global__ void __launch_bounds__(kThreads) expand_kernel(Work w, Pattern pt, int N, int U) {
   extern __shared__ int sm[];
-  int* scol = sm;                  // [U]
-  int* wcnt = scol + U;            // [kWarps][U]
+  int2* s_k = reinterpret_cast<int2*>(sm);  // [kExpandStage] keys of the staged incidences
+  int* s_e = sm + 2 * kExpandStage;         // [kExpandStage] the staged incidences
+  int* scol = s_e + kExpandStage;           // [U]
+  int* wcnt = scol + U;                     // [kWarps][U]
   const int lane = lane_id(), wid = threadIdx.x >> 5;
-  const int r = blockIdx.x;
+  const int r = w.row_order[blockIdx.x];  // longest rows first
   const int dpos = pt.diag_pos[r];
   const int nu = pt.row_ptr[r + 1] - dpos;
   for (int l = threadIdx.x; l < nu; l += kThreads) scol[l] = pt.col_idx[dpos + l];
@@ -57,6 +60,7 @@ __global__ void __launch_bounds__(kThreads) expand_kernel(Work w, Pattern pt, in
   int* mycnt = wcnt + wid * U;
   const int i0 = w.inc_start[r], i1 = w.inc_start[r + 1];
   const int base = 4 * i0;
+  const bool staged = i1 - i0 <= kExpandStage;  // else the second pass re-reads global memory
   // ---- pass 1: keys (stored) and per-warp counts ----
   for (int t = i0 + wid * kRound; t < i1; t += kWarps * kRound) {
     int e[kEpl];
@@ -93,22 +97,46 @@ __global__ void __launch_bounds__(kThreads) expand_kernel(Work w, Pattern pt, in
         __syncwarp();
       }
       const int idx = t + lane + 32 * k;
-      if (idx < i1) w.ekeys[idx] = make_int2((int)(kv[0] | (kv[1] << 16)), (int)(kv[2] | (kv[3] << 16)));
+      if (idx < i1) {
+        const int2 kk = make_int2((int)(kv[0] | (kv[1] << 16)), (int)(kv[2] | (kv[3] << 16)));
+        if (staged) {
+          s_k[idx - i0] = kk;
+          s_e[idx - i0] = e[k];
+        } else {
+          w.ekeys[idx] = kk;
+        }
+      }
     }
   }
   __syncthreads();
-  // ---- segments: column-major over (column, warp) ----
-  if (threadIdx.x == 0) {
-    int run = 0;
-    for (int l = 0; l < nu; l++) {
-      pt.seg_off[dpos + l] = base + run;
-      int c0 = run;
+  // ---- segments: column-major over (column, warp); warp 0, lane = column ----
+  if (wid == 0) {
+    int carry = 0;
+    for (int l0 = 0; l0 < nu; l0 += 32) {
+      const int l = l0 + lane;
+      int c[kWarps], tot = 0;
+#pragma unroll
       for (int v = 0; v < kWarps; v++) {
-        const int c = wcnt[v * U + l];
-        wcnt[v * U + l] = run;  // becomes the warp's cursor
-        run += c;
+        c[v] = l < nu ? wcnt[v * U + l] : 0;
+        tot += c[v];
       }
-      pt.seg_cnt[dpos + l] = run - c0;
+      int incl = tot;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int x = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += x;
+      }
+      if (l < nu) {
+        int run = carry + incl - tot;
+        pt.seg_off[dpos + l] = base + run;
+        pt.seg_cnt[dpos + l] = tot;
+#pragma unroll
+        for (int v = 0; v < kWarps; v++) {
+          wcnt[v * U + l] = run;  // becomes the warp's cursor
+          run += c[v];
+        }
+      }
+      carry += __shfl_sync(0xffffffffu, incl, 31);
     }
   }
   __syncthreads();
@@ -119,8 +147,8 @@ __global__ void __launch_bounds__(kThreads) expand_kernel(Work w, Pattern pt, in
 #pragma unroll
     for (int k = 0; k < kEpl; k++) {
       const int idx = t + lane + 32 * k;
-      e[k] = idx < i1 ? w.inc[idx] : -1;
-      kk[k] = idx < i1 ? w.ekeys[idx] : make_int2(-1, -1);
+      e[k] = idx < i1 ? (staged ? s_e[idx - i0] : w.inc[idx]) : -1;
+      kk[k] = idx < i1 ? (staged ? s_k[idx - i0] : w.ekeys[idx]) : make_int2(-1, -1);
     }
 #pragma unroll
     for (int k = 0; k < kEpl; k++) {
@@ -214,7 +242,7 @@ constexpr int kPartVals = 42;  // 36 block values + 6 rhs (diagonal block only)
 // phases are latency chains, so rows in flight matter more than registers
 __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern pt, AsmArgs aa) {
   extern __shared__ float4 stage_buf[];
-  const int r = blockIdx.x, lane = lane_id(), wid = threadIdx.x >> 5;
+  const int r = w.row_order[blockIdx.x], lane = lane_id(), wid = threadIdx.x >> 5;  // longest rows first
   const int cap = aa.stage_cap;
   const int i0 = w.inc_start[r], n_inc = w.inc_start[r + 1] - i0;
   const int dpos = pt.diag_pos[r], nb = pt.row_ptr[r + 1] - dpos;  // upper blocks of the row, diagonal first
@@ -443,7 +471,7 @@ __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern p
 
 }  // namespace
 
-int expand_smem_bytes(int U) { return (1 + kWarps) * U * (int)sizeof(int); }
+int expand_smem_bytes(int U) { return 3 * kExpandStage * (int)sizeof(int) + (1 + kWarps) * U * (int)sizeof(int); }
 
 cudaError_t launch_expand(const Work& w, const Pattern& p, int N, cudaStream_t s) {
   if (N <= 0) return cudaSuccess;

@@ -131,6 +131,7 @@ struct Work {
   int* cnt = nullptr;         // per sort CTA, a histogram over its problem's nodes
   long long cnt_cap = 0;      // words allocated for cnt
   int* node_total = nullptr;  // [max_nodes]
+  int* row_order = nullptr;   // [max_nodes] rows by decreasing incidence count (launch order of the per-row kernels)
   int* inc_start = nullptr;   // [max_nodes+1]
   int* inc = nullptr;         // [4*max_corrs]: (c << 2) | a
   int* trip = nullptr;        // [16*max_corrs]: (c << 4) | (a << 2) | b
@@ -216,6 +217,7 @@ struct PhaseClock {
 // ---- launchers (cf_kernels.cu) ----
 cudaError_t launch_pack_count(const Work& w, const Table& tb, cudaStream_t s);
 cudaError_t launch_bin_scan(const Work& w, const Table& tb, cudaStream_t s);
+cudaError_t launch_row_order(const Work& w, int N, cudaStream_t s);
 cudaError_t launch_bin_scatter(const Work& w, const Table& tb, cudaStream_t s);
 cudaError_t launch_expand(const Work& w, const Pattern& p, int N, cudaStream_t s);
 cudaError_t launch_node_plain(const Work& w, const cf_deform_node* nodes, const cf_dual_quat* T, int N,

@@ -198,6 +198,47 @@ __global__ void __launch_bounds__(1024) bin_scan_total_kernel(Work w, int N) {
   if (tid == 1023) w.inc_start[N] = wsum[31];
 }
 
+// Rows in order of decreasing incidence count (buckets of 16 incidences),
+// so that the per-row kernels (expand, assembly) start their longest rows
+// first and the last wave holds short ones.  The order inside a bucket is
+// whatever the atomics give: it changes the schedule only, never a result.
+constexpr int kOrderBuckets = 1024;
+__global__ void __launch_bounds__(kOrderBuckets) row_order_kernel(Work w, int N) {
+  __shared__ int hist[kOrderBuckets];
+  __shared__ int wsum[kOrderBuckets / 32];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  hist[tid] = 0;
+  __syncthreads();
+  for (int i = tid; i < N; i += kOrderBuckets)
+    atomicAdd(&hist[kOrderBuckets - 1 - min(w.node_total[i] >> 4, kOrderBuckets - 1)], 1);
+  __syncthreads();
+  const int v = hist[tid];
+  int incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int x = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += x;
+  }
+  if (lane == 31) wsum[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    int t = wsum[lane], ti = t;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int x = __shfl_up_sync(0xffffffffu, ti, o);
+      if (lane >= o) ti += x;
+    }
+    wsum[lane] = ti - t;
+  }
+  __syncthreads();
+  hist[tid] = wsum[wid] + incl - v;
+  __syncthreads();
+  for (int i = tid; i < N; i += kOrderBuckets) {
+    const int pos = atomicAdd(&hist[kOrderBuckets - 1 - min(w.node_total[i] >> 4, kOrderBuckets - 1)], 1);
+    w.row_order[pos] = i;
+  }
+}
+
 // Stable scatter of incidences: order within a node = (tile, slot, corr).
 __global__ void __launch_bounds__(kThreads) bin_scatter_kernel(Table tb, Work w) {
   extern __shared__ int cursor[];
@@ -616,6 +657,12 @@ cudaError_t launch_bin_scan(const Work& w, const Table& tb, cudaStream_t s) {
   if (tb.N <= 0) return cudaSuccess;
   bin_scan_nodes_kernel<<<cdiv(tb.N, 32), kThreads, 0, s>>>(tb, w);
   bin_scan_total_kernel<<<1, 1024, 0, s>>>(w, tb.N);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_row_order(const Work& w, int N, cudaStream_t s) {
+  if (N <= 0) return cudaSuccess;
+  row_order_kernel<<<1, kOrderBuckets, 0, s>>>(w, N);
   return cudaGetLastError();
 }
 
