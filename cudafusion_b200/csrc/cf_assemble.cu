@@ -22,6 +22,7 @@ namespace {
 constexpr int kWarps = kThreads / 32;
 constexpr int kEpl = 2;  // incidences per lane per round of expand
 constexpr int kExpandStage = 2048;  // incidences of a row kept in shared memory between the passes of expand
+constexpr int kColMap = 16384;      // nodes up to which expand finds a column through a node -> column map
 constexpr int kStageCap = 768;  // incidences of a row staged by the assembly (51 KB with their entries)
 constexpr int kRowEdges = 64;   // ARAP edges of a row / of its upper blocks staged by the assembly
 constexpr int kRound = 32 * kEpl;
@@ -50,13 +51,27 @@ __global__ void __launch_bounds__(kThreads) expand_kernel(Work w, Pattern pt, in
   int* s_e = sm + 2 * kExpandStage;         // [kExpandStage] the staged incidences
   int* scol = s_e + kExpandStage;           // [U]
   int* wcnt = scol + U;                     // [kWarps][U]
+  int* cmap = wcnt + kWarps * U;            // [N] node -> column (only the row's columns written)
   const int lane = lane_id(), wid = threadIdx.x >> 5;
   const int r = w.row_order[blockIdx.x];  // longest rows first
   const int dpos = pt.diag_pos[r];
   const int nu = pt.row_ptr[r + 1] - dpos;
-  for (int l = threadIdx.x; l < nu; l += kThreads) scol[l] = pt.col_idx[dpos + l];
+  const bool use_map = N <= kColMap;
+  for (int l = threadIdx.x; l < nu; l += kThreads) {
+    const int c = pt.col_idx[dpos + l];
+    scol[l] = c;
+    if (use_map) cmap[c] = l;
+  }
   for (int l = threadIdx.x; l < kWarps * U; l += kThreads) wcnt[l] = 0;
   __syncthreads();
+  // column of node nb in this row, or -1.  The map is written only at the
+  // row's columns: an entry read elsewhere holds whatever shared memory held
+  // and is accepted only if it points at a column equal to nb.
+  auto col_of = [&](int nb) -> int {
+    if (!use_map) return find_col(scol, nu, nb);
+    const int l = cmap[nb];
+    return ((unsigned)l < (unsigned)nu && scol[l] == nb) ? l : -1;
+  };
   int* mycnt = wcnt + wid * U;
   const int i0 = w.inc_start[r], i1 = w.inc_start[r + 1];
   const int base = 4 * i0;
@@ -89,12 +104,10 @@ __global__ void __launch_bounds__(kThreads) expand_kernel(Work w, Pattern pt, in
         int key = -1;
         if (e[k] >= 0) {
           const int nb = sel4i(ids[k], b);
-          if (nb >= r && nb < N && sel4(ws[k], b) > 1e-8f) key = find_col(scol, nu, nb);
+          if (nb >= r && nb < N && sel4(ws[k], b) > 1e-8f) key = col_of(nb);
         }
         kv[b] = key < 0 ? 0xffffu : (unsigned)key;
-        const unsigned peers = __match_any_sync(0xffffffffu, key);
-        if (key >= 0 && (__ffs(peers) - 1) == lane) mycnt[key] += __popc(peers);
-        __syncwarp();
+        if (key >= 0) atomicAdd(&mycnt[key], 1);  // counts only: order comes from pass 2
       }
       const int idx = t + lane + 32 * k;
       if (idx < i1) {
@@ -471,12 +484,15 @@ __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern p
 
 }  // namespace
 
-int expand_smem_bytes(int U) { return 3 * kExpandStage * (int)sizeof(int) + (1 + kWarps) * U * (int)sizeof(int); }
+int expand_smem_bytes(int U, int N) {
+  return 3 * kExpandStage * (int)sizeof(int) + (1 + kWarps) * U * (int)sizeof(int) +
+         (N <= kColMap ? N * (int)sizeof(int) : 0);
+}
 
 cudaError_t launch_expand(const Work& w, const Pattern& p, int N, cudaStream_t s) {
   if (N <= 0) return cudaSuccess;
   const int U = p.max_upper_row;
-  const size_t smem = (size_t)expand_smem_bytes(U);
+  const size_t smem = (size_t)expand_smem_bytes(U, N);
   cudaError_t e = cudaFuncSetAttribute(expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   expand_kernel<<<N, kThreads, smem, s>>>(w, p, N, U);

@@ -239,7 +239,7 @@ cudaError_t launch_energy_noalloc(const cf_problem* pr, const cf_dual_quat* T, f
                                   cudaStream_t s);
 int pcg_grid_smem_bytes(int nblk, int nrows, int nhalo, bool a_in_smem, bool pipelined);
 int pcg_max_active_ctas(int smem, bool a_in_smem, bool pipelined);
-int expand_smem_bytes(int max_upper_row);
+int expand_smem_bytes(int max_upper_row, int N);
 
 int pcg_cluster_smem_bytes(int nup_max, int nlow_max, int rows_max, int nhalo_max, int C);
 int pcg_cluster_max_active(int C, int smem);

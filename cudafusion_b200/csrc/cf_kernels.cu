@@ -52,7 +52,7 @@ __device__ __forceinline__ double block_sum_d(double v, double* red) {
 // ----------------------------------------------------------------------------
 __global__ void __launch_bounds__(kThreads) pack_count_kernel(Table tb, Work w) {
   extern __shared__ int hist[];
-  __shared__ __align__(16) uint32_t stage[kThreads * kWords];
+  __shared__ __align__(16) uint32_t stage2[2][kThreads * kWords];  // double-buffered tiles of records
   const int tid = threadIdx.x;
   const ProbDesc d = tb.desc[tb.bin_prob[blockIdx.x]];
   const int N = d.N, lc = blockIdx.x - d.bin_cta0;
@@ -62,17 +62,27 @@ __global__ void __launch_bounds__(kThreads) pack_count_kernel(Table tb, Work w) 
   const bool al16 = ((reinterpret_cast<uintptr_t>(corrs) & 15u) == 0);
   const int cb = lc * d.chunk;
   const int ce = min(d.M, cb + d.chunk);
-  __syncthreads();
-  for (int t0 = cb; t0 < ce; t0 += kThreads) {
-    const int n = min(kThreads, ce - t0);
+  // the next tile's records are in flight (cp.async) while this one is packed
+  auto issue = [&](int t0, uint32_t* buf) {
+    const int nw = min(kThreads, ce - t0) * kWords;
     const uint32_t* src = reinterpret_cast<const uint32_t*>(corrs) + (size_t)t0 * kWords;
-    const int nw = n * kWords;
     if (al16 && (nw & 3) == 0) {
-      const uint4* s4 = reinterpret_cast<const uint4*>(src);
-      uint4* d4 = reinterpret_cast<uint4*>(stage);
-      for (int i = tid; i < (nw >> 2); i += kThreads) d4[i] = __ldg(s4 + i);
+      for (int i = tid; i < (nw >> 2); i += kThreads) cp_async16(buf + 4 * i, src + 4 * i);
     } else {
-      for (int i = tid; i < nw; i += kThreads) stage[i] = __ldg(src + i);
+      for (int i = tid; i < nw; i += kThreads) cp_async4(buf + i, src + i);
+    }
+    cp_async_commit();
+  };
+  if (cb < ce) issue(cb, stage2[0]);
+  __syncthreads();
+  for (int t0 = cb, it = 0; t0 < ce; t0 += kThreads, it++) {
+    const int n = min(kThreads, ce - t0);
+    const uint32_t* stage = stage2[it & 1];
+    if (t0 + kThreads < ce) {
+      issue(t0 + kThreads, stage2[(it & 1) ^ 1]);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
     if (tid < n) {
