@@ -409,10 +409,10 @@ __global__ void node_plain_kernel(const cf_deform_node* __restrict__ nodes, cons
   store_dq(plain + i, dq_centered(load_dq_cg(T + i), node_pos(nodes, i)));
 }
 
-// Correspondences [c0, c1) of energy CTA blockIdx.x (a contiguous share of
-// its problem's rows).
-__device__ __forceinline__ void e_range(const Table& tb, const ProbDesc& d, int& c0, int& c1) {
-  const int lc = blockIdx.x - d.e_cta0;
+// Correspondences [c0, c1) of energy CTA `cta` (a contiguous share of its
+// problem's rows).
+__device__ __forceinline__ void e_range(const Table& tb, const ProbDesc& d, int cta, int& c0, int& c1) {
+  const int lc = cta - d.e_cta0;
   const int per = (d.M + d.e_ctas - 1) / d.e_ctas;
   c0 = d.corr_off + min(d.M, lc * per);
   c1 = d.corr_off + min(d.M, lc * per + per);
@@ -426,6 +426,7 @@ struct EdgeArgs {
   float lambda, arap_sgn;
   float4* out;     // [kEdgeTerms4 * n_edges]
   double* energy;  // [n_edges]
+  int edge_ctas;   // the launch's first CTAs
 };
 
 __device__ __forceinline__ int tri6(int p, int q) { return p * 6 - p * (p - 1) / 2 + (q - p); }
@@ -494,25 +495,35 @@ __device__ void edge_terms_cta(const EdgeArgs& ea, int cta) {
       ev.el > 0.f ? (double)ev.el * ((double)rr[0] * rr[0] + (double)rr[1] * rr[1] + (double)rr[2] * rr[2]) : 0.0;
 }
 
+// The edge CTAs come first: their per-thread chains are the longest of the
+// launch, so they start while the correspondence CTAs fill the rest.
 template <bool SKIN>
 __global__ void __launch_bounds__(kThreads) residual_kernel(Table tb, Work w, EdgeArgs ea) {
   __shared__ double red[32];
-  if ((int)blockIdx.x >= tb.n_e) {
-    edge_terms_cta(ea, blockIdx.x - tb.n_e);
+  if ((int)blockIdx.x < ea.edge_ctas) {
+    edge_terms_cta(ea, blockIdx.x);
     return;
   }
-  const ProbDesc d = tb.desc[tb.e_prob[blockIdx.x]];
+  const int cta = blockIdx.x - ea.edge_ctas;
+  const ProbDesc d = tb.desc[tb.e_prob[cta]];
   int c0, c1;
-  e_range(tb, d, c0, c1);
+  e_range(tb, d, cta, c0, c1);
   const int N = tb.N;
   double e = 0.0;
   for (int c = c0 + threadIdx.x; c < c1; c += kThreads) {
-    float4 s = w.pk_src[c];
+    // every load of the correspondence issued together, then the skinning gathers
+    const float4 s = w.pk_src[c];
+    const float4 dd = w.pk_dst[c];
+    const float4 n = w.pk_nrm[c];
+    int4 ids = make_int4(-1, -1, -1, -1);
+    float4 ws4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (SKIN) {
+      ids = w.pk_ids[c];
+      ws4 = w.pk_ws[c];
+    }
     if (!(s.w > 0.f)) continue;
     float3 src = f3(s.x, s.y, s.z);
-    if (SKIN) src = blend_warp(src, w.pk_ids[c], w.pk_ws[c], w.plain, N);
-    float4 dd = w.pk_dst[c];
-    float4 n = w.pk_nrm[c];
+    if (SKIN) src = blend_warp(src, ids, ws4, w.plain, N);
     // kernels/solver_kernels.cu:76-85
     float res = n.x * (src.x - dd.x) + n.y * (src.y - dd.y) + n.z * (src.z - dd.z);
     float fw = fmaxf(s.w, 0.f) * huber_w(res, 0.2f);
@@ -525,7 +536,7 @@ __global__ void __launch_bounds__(kThreads) residual_kernel(Table tb, Work w, Ed
     w.c_nres[c] = make_float4(n.x, n.y, n.z, res);
   }
   double t = block_sum_d(e, red);
-  if (threadIdx.x == 0) w.e_data_part[blockIdx.x] = t;
+  if (threadIdx.x == 0) w.e_data_part[cta] = t;
 }
 
 // Energy at the current transforms (after the last update): data term with
@@ -536,7 +547,7 @@ __global__ void __launch_bounds__(kThreads) energy_kernel(Table tb, Work w, Patt
   const int prob = tb.e_prob[blockIdx.x];
   const ProbDesc d = tb.desc[prob];
   int c0, c1;
-  e_range(tb, d, c0, c1);
+  e_range(tb, d, blockIdx.x, c0, c1);
   const int N = tb.N;
   double e = 0.0;
   for (int c = c0 + threadIdx.x; c < c1; c += kThreads) {
@@ -712,7 +723,8 @@ cudaError_t launch_residual(const Work& w, const Table& tb, const Pattern& p, co
   ea.arap_sgn = a.arap_consistent ? -1.f : 1.f;
   ea.out = p.edge_terms;
   ea.energy = p.edge_energy;
-  const int grid = tb.n_e + cdiv(p.n_edges, kThreads);
+  ea.edge_ctas = cdiv(p.n_edges, kThreads);
+  const int grid = tb.n_e + ea.edge_ctas;
   if (grid <= 0) return cudaSuccess;
   if (skin)
     residual_kernel<true><<<grid, kThreads, 0, s>>>(tb, w, ea);
