@@ -218,7 +218,10 @@ cf_status prepare_table(cf_gn* h, std::vector<ProbDesc> in, bool single, cudaStr
     maxN = std::max(maxN, d.N);
   }
   if (Nt > w.max_nodes || Mt > w.max_corrs) return CF_ERR_CAPACITY;
-  const int B = w.bin_ctas_max;
+  // sort CTAs: two per SM for a single solve; a batch gets at least one per
+  // kSortCorrs correspondences, shared out in proportion to the problems' sizes
+  const int B = single ? w.bin_ctas_max
+                       : (int)std::max<long long>(w.bin_ctas_max, std::min<long long>(kMaxSortCtas, (Mt + kSortCorrs - 1) / kSortCorrs));
   std::vector<int> bin_prob, e_prob;
   long long cnt = 0;
   int corr_off = 0, node_off = 0;
@@ -256,9 +259,15 @@ cf_status prepare_table(cf_gn* h, std::vector<ProbDesc> in, bool single, cudaStr
   }
   if (!t.desc) {
     CF_TRY(dalloc(&t.desc, (size_t)kMaxProblems));
-    CF_TRY(dalloc(&t.bin_prob, (size_t)(B + kMaxProblems)));
     CF_TRY(dalloc(&t.e_prob, (size_t)(kEnergyCtas + kMaxProblems)));
     CF_TRY(dalloc(&t.node_prob, (size_t)w.max_nodes));
+  }
+  if ((long long)bin_prob.size() > t.bin_cap) {
+    dfree(t.bin_prob);
+    t.bin_cap = 0;
+    h->h_bin_prob.clear();  // the new buffer holds nothing yet
+    CF_TRY(dalloc(&t.bin_prob, (size_t)B + kMaxProblems));
+    t.bin_cap = (long long)B + kMaxProblems;
   }
   std::vector<int> node_prob;
   node_prob.reserve((size_t)Nt);

@@ -54,6 +54,7 @@ struct Table {
   int max_chunk = 0;         // most correspondences of one sort CTA
   ProbDesc* desc = nullptr;  // [P]
   int* bin_prob = nullptr;   // [n_bin] problem of each sort CTA
+  long long bin_cap = 0;     // capacity of bin_prob
   int* e_prob = nullptr;     // [n_e] problem of each energy CTA
   int* node_prob = nullptr;  // [N] problem of each node
 };
@@ -161,6 +162,8 @@ struct Work {
 
 constexpr int kEnergyCtas = 592;  // residual/energy CTAs of a single solve
 constexpr int kMaxPcgCtas = 1024;
+constexpr int kSortCorrs = 4096;     // correspondences per sort CTA of a batched solve (at least)
+constexpr int kMaxSortCtas = 1 << 16;
 constexpr int kClusterAutoRows = 32;  // rows per CTA up to which mode 0 picks the single-cluster PCG
 constexpr int kMaxProblems = 1024;       // problems per batched solve
 constexpr int kMaxProblemNodes = 48000;  // nodes per problem (per-CTA histograms in shared memory)
