@@ -726,7 +726,7 @@ cf_status bin_correspondences(cf_gn* h, cudaStream_t s) {
   const Table& t = h->tb;
   if (t.n_bin > 0) {
     { Timed tm(h, s, kProfPack, 1); CF_TRY(launch_pack_count(w, t, s)); }
-    { Timed tm(h, s, kProfBinScan, 3); CF_TRY(launch_bin_scan(w, t, s)); CF_TRY(launch_row_order(w, t.N, s)); }
+    { Timed tm(h, s, kProfBinScan, 2); CF_TRY(launch_bin_scan(w, t, s)); }
     { Timed tm(h, s, kProfScatter, 1); CF_TRY(launch_bin_scatter(w, t, s)); }
   } else {
     CF_TRY(cudaMemsetAsync(w.inc_start, 0, sizeof(int) * (size_t)(t.N + 1), s));

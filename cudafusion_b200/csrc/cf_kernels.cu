@@ -172,48 +172,12 @@ __global__ void __launch_bounds__(kThreads) bin_scan_nodes_kernel(Table tb, Work
   }
 }
 
-// inc_start = exclusive scan of node_total (one CTA of 1024 threads).
-__global__ void __launch_bounds__(1024) bin_scan_total_kernel(Work w, int N) {
-  __shared__ int wsum[32];
-  const int tid = threadIdx.x;
-  const int per = (N + 1023) / 1024;
-  const int b = tid * per, e = min(N, b + per);
-  int loc = 0;
-  for (int i = b; i < e; i++) loc += w.node_total[i];
-  // block exclusive scan of loc
-  int v = loc;
-  const int lane = tid & 31, wid = tid >> 5;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int t = __shfl_up_sync(0xffffffffu, v, o);
-    if (lane >= o) v += t;
-  }
-  if (lane == 31) wsum[wid] = v;
-  __syncthreads();
-  if (wid == 0) {
-    int s = wsum[lane];
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int t = __shfl_up_sync(0xffffffffu, s, o);
-      if (lane >= o) s += t;
-    }
-    wsum[lane] = s;
-  }
-  __syncthreads();
-  int excl = v - loc + (wid > 0 ? wsum[wid - 1] : 0);
-  for (int i = b; i < e; i++) {
-    w.inc_start[i] = excl;
-    excl += w.node_total[i];
-  }
-  if (tid == 1023) w.inc_start[N] = wsum[31];
-}
-
 // Rows in order of decreasing incidence count (buckets of 16 incidences),
 // so that the per-row kernels (expand, assembly) start their longest rows
 // first and the last wave holds short ones.  The order inside a bucket is
 // whatever the atomics give: it changes the schedule only, never a result.
 constexpr int kOrderBuckets = 1024;
-__global__ void __launch_bounds__(kOrderBuckets) row_order_kernel(Work w, int N) {
+__device__ __forceinline__ void row_order_body(const Work& w, int N) {
   __shared__ int hist[kOrderBuckets];
   __shared__ int wsum[kOrderBuckets / 32];
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -248,6 +212,47 @@ __global__ void __launch_bounds__(kOrderBuckets) row_order_kernel(Work w, int N)
     w.row_order[pos] = i;
   }
 }
+__global__ void __launch_bounds__(kOrderBuckets) row_order_kernel(Work w, int N) { row_order_body(w, N); }
+
+// inc_start = exclusive scan of node_total (one CTA of 1024 threads), then
+// the rows' launch order.
+__global__ void __launch_bounds__(1024) bin_scan_total_kernel(Work w, int N) {
+  __shared__ int wsum[32];
+  const int tid = threadIdx.x;
+  const int per = (N + 1023) / 1024;
+  const int b = tid * per, e = min(N, b + per);
+  int loc = 0;
+  for (int i = b; i < e; i++) loc += w.node_total[i];
+  // block exclusive scan of loc
+  int v = loc;
+  const int lane = tid & 31, wid = tid >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += t;
+  }
+  if (lane == 31) wsum[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    int s = wsum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += t;
+    }
+    wsum[lane] = s;
+  }
+  __syncthreads();
+  int excl = v - loc + (wid > 0 ? wsum[wid - 1] : 0);
+  for (int i = b; i < e; i++) {
+    w.inc_start[i] = excl;
+    excl += w.node_total[i];
+  }
+  if (tid == 1023) w.inc_start[N] = wsum[31];
+  __syncthreads();
+  row_order_body(w, N);  // the launch order of the per-row kernels, from the same totals
+}
+
 
 // Stable scatter of incidences: order within a node = (tile, slot, corr).
 __global__ void __launch_bounds__(kThreads) bin_scatter_kernel(Table tb, Work w) {
@@ -677,6 +682,7 @@ cudaError_t launch_pack_count(const Work& w, const Table& tb, cudaStream_t s) {
 cudaError_t launch_bin_scan(const Work& w, const Table& tb, cudaStream_t s) {
   if (tb.N <= 0) return cudaSuccess;
   bin_scan_nodes_kernel<<<cdiv(tb.N, 32), kThreads, 0, s>>>(tb, w);
+  static_assert(kOrderBuckets == 1024, "the scan CTA also orders the rows");
   bin_scan_total_kernel<<<1, 1024, 0, s>>>(w, tb.N);
   return cudaGetLastError();
 }
