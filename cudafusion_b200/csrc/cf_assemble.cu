@@ -23,8 +23,12 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kEpl = 2;  // incidences per lane per round of expand
 constexpr int kExpandStage = 2048;  // incidences of a row kept in shared memory between the passes of expand
 constexpr int kColMap = 16384;      // nodes up to which expand finds a column through a node -> column map
-constexpr int kStageCap = 768;  // incidences of a row staged by the assembly (51 KB with their entries)
-constexpr int kRowEdges = 64;   // ARAP edges of a row / of its upper blocks staged by the assembly
+// incidences of a row staged by the assembly (60 KB with their entries; 92 %
+// of the incidences of the full frame), and ARAP edges of a row / of its
+// upper blocks staged (rows have ~16): with them the CTA fits 3 per SM
+// (measured: 64.5 us per GN vs 66.4 at 768 / 64)
+constexpr int kStageCap = 896;
+constexpr int kRowEdges = 32;
 constexpr int kRound = 32 * kEpl;
 
 __device__ __forceinline__ int find_col(const int* cols, int n, int v) {
@@ -251,7 +255,7 @@ constexpr int kPartVals = 42;  // 36 block values + 6 rhs (diagonal block only)
 //     the diagonal block), the ARAP terms of the block's edges (precomputed
 //     by the residual launch), the damping; blocks written with their
 //     transposes, the rhs and the row's ARAP energy.
-// 3 CTAs per SM (80 registers, 72 KB of shared memory each): the per-row
+// 3 CTAs per SM (80 registers, 74 KB of shared memory each): the per-row
 // phases are latency chains, so rows in flight matter more than registers
 __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern pt, AsmArgs aa) {
   extern __shared__ float4 stage_buf[];
