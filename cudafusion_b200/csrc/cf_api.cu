@@ -856,7 +856,8 @@ cf_status enqueue_solve(cf_gn* h, int kind, SolveArgs& a, cudaStream_t s) {
       CF_TRY(mpnn_graph_from_nodes(net, a.nodes, a.N, s));
       CF_TRY(mpnn_forward(net, net.feat, net.out, s));
     }
-    { Timed t(h, s, kProfEnergy, 2); CF_TRY(launch_final_energy(w, h->p, a, -1, s)); }
+    // the warm start's energy from the residual launch above
+    { Timed t(h, s, kProfEnergy, 1); CF_TRY(launch_residual_energy(w, h->p, a, -1, s)); }
     { Timed t(h, s, kProfLearned, 1); CF_TRY(launch_apply_prediction(w, a.transforms, a.nodes, net.out, a.N, s)); }
     { Timed t(h, s, kProfEnergy, 2); CF_TRY(launch_final_energy(w, h->p, a, -2, s)); }
     { Timed t(h, s, kProfLearned, 1); CF_TRY(launch_gate_prediction(w, a.transforms, a.nodes, a.N, s)); }

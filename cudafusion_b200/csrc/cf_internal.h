@@ -232,6 +232,7 @@ cudaError_t launch_batch_scatter(const Work& w, const Table& tb, cudaStream_t s)
 cudaError_t launch_assemble(const Work& w, const Pattern& p, const SolveArgs& a, const cf_dual_quat* T,
                             cudaStream_t s);
 cudaError_t launch_pcg(const Work& w, const Pattern& p, const SolveArgs& a, int gn_slot, cudaStream_t s);
+cudaError_t launch_residual_energy(const Work& w, const Pattern& p, const SolveArgs& a, int slot, cudaStream_t s);
 cudaError_t launch_final_energy(const Work& w, const Pattern& p, const SolveArgs& a, int slot, cudaStream_t s);
 cudaError_t launch_apply_twist(cf_dual_quat* T, const float* dx, int N, float max_rot, float max_trans,
                                float scale, cudaStream_t s);

@@ -593,6 +593,26 @@ __global__ void energy_reduce_kernel(Table tb, Work w, int slot) {
   }
 }
 
+// One warp per problem: the energy at the transforms the residual launch just
+// linearised at, from that launch's own partials (data-term CTA partials and
+// per-edge ARAP energies) -- no second skinning pass.
+__global__ void residual_energy_kernel(Table tb, Work w, Pattern pt, int slot) {
+  const ProbDesc d = tb.desc[blockIdx.x];
+  double v = 0.0;
+  for (int k = threadIdx.x; k < d.e_ctas; k += 32) v += w.e_data_part[d.e_cta0 + k];
+  const int e0 = pt.prob_edge_off[blockIdx.x], e1 = pt.prob_edge_off[blockIdx.x + 1];
+  for (int e = e0 + threadIdx.x; e < e1; e += 32) v += pt.edge_energy[e];
+  v = warp_sum_d(v);
+  if (threadIdx.x == 0) {
+    if (slot >= 0) {
+      w.stats[blockIdx.x].energy[slot] = v;
+      if (!isfinite(v)) atomicOr(w.err, kErrNonFinite);
+    } else {
+      w.stats[blockIdx.x].gate[-slot - 1] = v;
+    }
+  }
+}
+
 // Batched solves: each problem's nodes (neighbour ids made global) and
 // transforms into the concatenated arrays.
 __global__ void batch_gather_kernel(Table tb, Work w) {
@@ -736,6 +756,12 @@ cudaError_t launch_residual(const Work& w, const Table& tb, const Pattern& p, co
     residual_kernel<true><<<grid, kThreads, 0, s>>>(tb, w, ea);
   else
     residual_kernel<false><<<grid, kThreads, 0, s>>>(tb, w, ea);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_residual_energy(const Work& w, const Pattern& p, const SolveArgs& a, int slot, cudaStream_t s) {
+  if (a.tb.P <= 0) return cudaSuccess;
+  residual_energy_kernel<<<a.tb.P, 32, 0, s>>>(a.tb, w, p, slot);
   return cudaGetLastError();
 }
 

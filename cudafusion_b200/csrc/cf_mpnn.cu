@@ -16,8 +16,9 @@
 // Parameters and activations are BF16 (parameters kept in FP32 for Adam and
 // rounded to BF16 after every step); every sum accumulates in FP32, in a
 // fixed order, so forward and gradients are deterministic.  The layers are
-// tiny (N x 128 x 64); each runs on CUDA cores from shared-memory tiles of 32
-// nodes, the weight gradients as per-CTA partial sums reduced in CTA order.
+// tiny (N x 128 x 64); each runs on CUDA cores from shared-memory tiles of 16
+// nodes (forward) or 32 (gradients, as per-CTA partial sums reduced in CTA
+// order).
 #include <cuda_bf16.h>
 
 #include "cf_device.cuh"
@@ -39,10 +40,15 @@ static_assert(kParams == CF_MPNN_PARAMS, "parameter count");
 __device__ __forceinline__ float bf(__nv_bfloat16 v) { return __bfloat162float(v); }
 __device__ __forceinline__ __nv_bfloat16 tobf(float v) { return __float2bfloat16_rn(v); }
 
-// Forward of one message-passing layer over a tile of 32 nodes:
+// Forward of one message-passing layer over a tile of kFwdTile nodes:
 // out = act(W [in_i, mean_j in_j] + b).  FIRST: `in` is the FP32 feature
 // array (rounded to BF16 on load).  AGG=false (output layer): out = W in + b
-// + x[0:6] (FP32 out).
+// + x[0:6] (FP32 out).  Latency-bound at this size, so every phase issues
+// all its loads before it uses them: the weights as 16-B chunks of 8 BF16,
+// the neighbour lists, then the neighbours' features; the products run
+// several nodes per thread in independent chains.  The sums keep the order
+// of a plain loop (bias, then k ascending; neighbours in list order).
+constexpr int kFwdTile = 16;
 template <int DIN, int DOUT, bool FIRST, bool AGG, bool RELU>
 __global__ void __launch_bounds__(kThreads) layer_fwd(const void* in_, const int* __restrict__ nbr,
                                                       const float* __restrict__ inv_deg,
@@ -50,48 +56,108 @@ __global__ void __launch_bounds__(kThreads) layer_fwd(const void* in_, const int
                                                       const __nv_bfloat16* __restrict__ b, void* out_,
                                                       const float* __restrict__ x_skip, int N) {
   constexpr int CAT = AGG ? 2 * DIN : DIN;
+  static_assert(CAT % 8 == 0, "weight rows in 16-B chunks");
   extern __shared__ float fsm[];
   float* sW = fsm;                 // [CAT][DOUT]: transposed, so that the lanes (consecutive
                                    // output units) read consecutive banks
   float* sB = sW + DOUT * CAT;     // [DOUT]
-  float* sX = sB + DOUT;           // [32][CAT]
-  const int n0 = blockIdx.x * kTileNodes;
-  for (int q = threadIdx.x; q < DOUT * CAT; q += kThreads) sW[(q % CAT) * DOUT + q / CAT] = bf(W[q]);
-  for (int k = threadIdx.x; k < DOUT; k += kThreads) sB[k] = bf(b[k]);
+  float* sX = sB + DOUT;           // [kFwdTile][CAT]
+  const int tid = threadIdx.x;
+  const int n0 = blockIdx.x * kFwdTile;
+  {
+    constexpr int NCH = DOUT * CAT / 8, PER = (NCH + kThreads - 1) / kThreads;
+    uint4 wv[PER];
+#pragma unroll
+    for (int j = 0; j < PER; j++) {
+      const int q = tid + j * kThreads;
+      if (q < NCH) wv[j] = __ldg(reinterpret_cast<const uint4*>(W) + q);
+    }
+#pragma unroll
+    for (int j = 0; j < PER; j++) {
+      const int q = tid + j * kThreads;
+      if (q < NCH) {
+        const __nv_bfloat16* h = reinterpret_cast<const __nv_bfloat16*>(&wv[j]);
+#pragma unroll
+        for (int t = 0; t < 8; t++) {
+          const int idx = 8 * q + t, u = idx / CAT, k = idx % CAT;
+          sW[k * DOUT + u] = bf(h[t]);
+        }
+      }
+    }
+  }
+  for (int k = tid; k < DOUT; k += kThreads) sB[k] = bf(b[k]);
   auto load_in = [&](int i, int k) -> float {
     if (FIRST) return bf(tobf(reinterpret_cast<const float*>(in_)[(size_t)i * DIN + k]));
     return bf(reinterpret_cast<const __nv_bfloat16*>(in_)[(size_t)i * DIN + k]);
   };
-  for (int e = threadIdx.x; e < kTileNodes * DIN; e += kThreads) {
-    const int s = e / DIN, k = e % DIN, i = n0 + s;
-    float v = 0.f, a = 0.f;
-    if (i < N) {
-      v = load_in(i, k);
-      if (AGG) {
+  {
+    constexpr int NE = kFwdTile * DIN, EPT = (NE + kThreads - 1) / kThreads;
+    int jn[EPT][CF_K_GRAPH];
 #pragma unroll
-        for (int q = 0; q < CF_K_GRAPH; q++) {
-          const int j = nbr[(size_t)i * CF_K_GRAPH + q];
-          if (j >= 0) a += load_in(j, k);
-        }
-        a *= inv_deg[i];
-      }
+    for (int j = 0; j < EPT; j++) {
+      const int e = tid + j * kThreads, i = n0 + e / DIN;
+      const bool ok = e < NE && i < N;
+#pragma unroll
+      for (int q = 0; q < CF_K_GRAPH; q++) jn[j][q] = (AGG && ok) ? nbr[(size_t)i * CF_K_GRAPH + q] : -1;
     }
-    sX[s * CAT + k] = v;
-    if (AGG) sX[s * CAT + DIN + k] = a;
+#pragma unroll
+    for (int j = 0; j < EPT; j++) {
+      const int e = tid + j * kThreads, s = e / DIN, k = e % DIN, i = n0 + s;
+      if (e >= NE) continue;
+      float v = 0.f, a = 0.f;
+      if (i < N) {
+        v = load_in(i, k);
+        if (AGG) {
+          float x[CF_K_GRAPH];
+#pragma unroll
+          for (int q = 0; q < CF_K_GRAPH; q++) x[q] = jn[j][q] >= 0 ? load_in(jn[j][q], k) : 0.f;
+#pragma unroll
+          for (int q = 0; q < CF_K_GRAPH; q++)
+            if (jn[j][q] >= 0) a += x[q];
+          a *= inv_deg[i];
+        }
+      }
+      sX[s * CAT + k] = v;
+      if (AGG) sX[s * CAT + DIN + k] = a;
+    }
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < kTileNodes * DOUT; e += kThreads) {
-    const int s = e / DOUT, u = e % DOUT, i = n0 + s;
-    if (i >= N) continue;
-    float acc = sB[u];
-    const float* xx = sX + s * CAT;
-#pragma unroll 8
-    for (int k = 0; k < CAT; k++) acc = fmaf(sW[k * DOUT + u], xx[k], acc);
+  auto store = [&](int i, int u, float acc) {
     if (RELU) acc = fmaxf(acc, 0.f);
     if (AGG) {
       reinterpret_cast<__nv_bfloat16*>(out_)[(size_t)i * DOUT + u] = tobf(acc);
     } else {
       reinterpret_cast<float*>(out_)[(size_t)i * DOUT + u] = acc + x_skip[(size_t)i * kIn + u];
+    }
+  };
+  if constexpr (kFwdTile * DOUT >= kThreads && kThreads % DOUT == 0) {
+    // unit u = tid % DOUT, nodes tid / DOUT + r * (kThreads / DOUT): NR chains per thread
+    constexpr int SPR = kThreads / DOUT, NR = kFwdTile / SPR;
+    static_assert(kFwdTile % SPR == 0, "whole rounds of nodes");
+    const int u = tid % DOUT, s0 = tid / DOUT;
+    float acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) acc[r] = sB[u];
+#pragma unroll 8
+    for (int k = 0; k < CAT; k++) {
+      const float wk = sW[k * DOUT + u];
+#pragma unroll
+      for (int r = 0; r < NR; r++) acc[r] = fmaf(wk, sX[(s0 + r * SPR) * CAT + k], acc[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+      const int i = n0 + s0 + r * SPR;
+      if (i < N) store(i, u, acc[r]);
+    }
+  } else {
+    for (int e = tid; e < kFwdTile * DOUT; e += kThreads) {
+      const int s = e / DOUT, u = e % DOUT, i = n0 + s;
+      if (i >= N) continue;
+      float acc = sB[u];
+      const float* xx = sX + s * CAT;
+#pragma unroll 8
+      for (int k = 0; k < CAT; k++) acc = fmaf(sW[k * DOUT + u], xx[k], acc);
+      store(i, u, acc);
     }
   }
 }
@@ -432,7 +498,7 @@ inline int cdiv(int a, int b) { return (a + b - 1) / b; }
 int mpnn_param_count() { return kParams; }
 
 static int layer_bwd_smem(int din) { return (kHid * 2 * din + kTileNodes * 2 * din + kTileNodes * kHid) * 4; }
-static int layer_fwd_smem(int cat, int dout) { return (dout * cat + dout + kTileNodes * cat) * 4; }
+static int layer_fwd_smem(int cat, int dout) { return (dout * cat + dout + kFwdTile * cat) * 4; }
 
 template <typename T>
 static cudaError_t alloc_n(T** p, size_t n) {
@@ -484,7 +550,7 @@ cudaError_t mpnn_graph_from_nodes(Mpnn& m, const cf_deform_node* nodes, int N, c
 cudaError_t mpnn_forward(const Mpnn& m, const float* feat, float* out, cudaStream_t s) {
   const int N = m.N;
   if (N <= 0) return cudaSuccess;
-  const int g = cdiv(N, kTileNodes);
+  const int g = cdiv(N, kFwdTile);
   const __nv_bfloat16* wb = reinterpret_cast<const __nv_bfloat16*>(m.wb);
   const int s0 = layer_fwd_smem(2 * kIn, kHid), s1 = layer_fwd_smem(2 * kHid, kHid), so = layer_fwd_smem(kHid, kOut);
   cudaError_t e = cudaFuncSetAttribute(layer_fwd<kHid, kHid, false, true, true>,
