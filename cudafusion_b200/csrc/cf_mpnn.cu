@@ -421,14 +421,29 @@ __global__ void features_kernel(const cf_dual_quat* __restrict__ T, const cf_dua
   if (i >= N) return;
   float s = 0.f, mx = 0.f;
   int cnt = 0;
-  for (int q = inc_start[i] + lane; q < inc_start[i + 1]; q += 32) {
-    const int c = inc[q] >> 2;
-    if (c_srcfw[c].w > 0.f) {
-      const float r = fabsf(c_nres[c].w);
-      s += r;
-      mx = fmaxf(mx, r);
-      cnt++;
+  // 4 incidences per lane in flight: their ids, then the weight and the
+  // residual of each (the .w of the two records), summed in incidence order
+  const int q1 = inc_start[i + 1];
+  const float* fw = reinterpret_cast<const float*>(c_srcfw) + 3;
+  const float* rs = reinterpret_cast<const float*>(c_nres) + 3;
+  for (int q0 = inc_start[i] + lane; q0 < q1; q0 += 4 * 32) {
+    int c[4];
+#pragma unroll
+    for (int b = 0; b < 4; b++) c[b] = q0 + 32 * b < q1 ? (inc[q0 + 32 * b] >> 2) : -1;
+    float f[4], r[4];
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      f[b] = c[b] >= 0 ? __ldg(fw + 4 * (size_t)c[b]) : 0.f;
+      r[b] = c[b] >= 0 ? __ldg(rs + 4 * (size_t)c[b]) : 0.f;
     }
+#pragma unroll
+    for (int b = 0; b < 4; b++)
+      if (f[b] > 0.f) {
+        const float ra = fabsf(r[b]);
+        s += ra;
+        mx = fmaxf(mx, ra);
+        cnt++;
+      }
   }
   s = warp_sum_f(s);
 #pragma unroll
