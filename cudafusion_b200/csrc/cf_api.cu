@@ -120,7 +120,7 @@ void free_pattern(Pattern& p) {
 
 void free_work(Work& w) {
   dfree(w.pk_src); dfree(w.pk_dst); dfree(w.pk_nrm); dfree(w.pk_ids); dfree(w.pk_ws);
-  dfree(w.c_srcfw); dfree(w.c_nres); dfree(w.cnt); dfree(w.node_total); dfree(w.row_order); dfree(w.inc_start);
+  dfree(w.c_srcfw); dfree(w.c_nres); dfree(w.c_fr); dfree(w.cnt); dfree(w.node_total); dfree(w.row_order); dfree(w.inc_start);
   dfree(w.inc); dfree(w.trip); dfree(w.ekeys); dfree(w.rhs); dfree(w.plain); dfree(w.x); dfree(w.z); dfree(w.p0); dfree(w.p1);
   dfree(w.partials); dfree(w.barrier); dfree(w.err); dfree(w.e_data_part); dfree(w.e_arap_part); dfree(w.stats); dfree(w.timers);
   dfree(w.nodes_cat); dfree(w.T_cat); dfree(w.r); dfree(w.ap); dfree(w.minv32);
@@ -140,7 +140,7 @@ cudaError_t alloc_work(Work& w, int max_nodes, int max_corrs, int bin_ctas_max) 
   cudaError_t e;
 #define A_(ptr, n) if ((e = dalloc(&(ptr), (n))) != cudaSuccess) return e
   A_(w.pk_src, M); A_(w.pk_dst, M); A_(w.pk_nrm, M); A_(w.pk_ids, M); A_(w.pk_ws, M);
-  A_(w.c_srcfw, M); A_(w.c_nres, M);
+  A_(w.c_srcfw, M); A_(w.c_nres, M); A_(w.c_fr, M);
   A_(w.node_total, N); A_(w.row_order, N); A_(w.inc_start, N + 1);
   A_(w.inc, 4 * M); A_(w.trip, 16 * M); A_(w.ekeys, 4 * M);
   A_(w.rhs, 6 * N); A_(w.plain, N); A_(w.x, 6 * N); A_(w.z, 6 * N); A_(w.p0, 6 * N); A_(w.p1, 6 * N);
@@ -849,7 +849,7 @@ cf_status enqueue_solve(cf_gn* h, int kind, SolveArgs& a, cudaStream_t s) {
     // kept only if it lowers the energy (the plain warm start otherwise)
     Mpnn& net = *h->learn_net;
     { Timed t(h, s, kProfNodePlain, 1); CF_TRY(launch_node_plain(w, a.nodes, a.transforms, a.N, s)); }
-    { Timed t(h, s, kProfResidual, 1); CF_TRY(launch_residual(w, h->tb, h->p, a, a.transforms, true, s)); }
+    { Timed t(h, s, kProfResidual, 1); CF_TRY(launch_residual(w, h->tb, h->p, a, a.transforms, true, s, true)); }
     {
       Timed t(h, s, kProfLearned, 6);
       CF_TRY(launch_features(w, a.transforms, h->learn_hist, a.N, net.feat, s));
@@ -1503,7 +1503,7 @@ cf_status cf_gn_features(cf_gn* h, const cf_problem* prob, const cf_dual_quat* d
   if ((st = bin_correspondences(h, s)) != CF_OK) return st;
   SolveArgs a = make_args(h, prob->nodes, N, M);
   CF_TRY(launch_node_plain(w, prob->nodes, d_transforms, N, s));
-  CF_TRY(launch_residual(w, h->tb, h->p, a, d_transforms, true, s));
+  CF_TRY(launch_residual(w, h->tb, h->p, a, d_transforms, true, s, true));
   CF_TRY(launch_features(w, d_transforms, d_history, N, d_features, s));
   return CF_OK;
 }

@@ -129,6 +129,7 @@ struct Work {
   float4* pk_ws = nullptr;
   float4* c_srcfw = nullptr;  // skinned src, fw (0 = skipped)
   float4* c_nres = nullptr;   // normal, residual
+  float2* c_fr = nullptr;     // (weight, residual) per correspondence, for the learned start's features
   int* cnt = nullptr;         // per sort CTA, a histogram over its problem's nodes
   long long cnt_cap = 0;      // words allocated for cnt
   int* node_total = nullptr;  // [max_nodes]
@@ -226,7 +227,7 @@ cudaError_t launch_expand(const Work& w, const Pattern& p, int N, cudaStream_t s
 cudaError_t launch_node_plain(const Work& w, const cf_deform_node* nodes, const cf_dual_quat* T, int N,
                               cudaStream_t s);
 cudaError_t launch_residual(const Work& w, const Table& tb, const Pattern& p, const SolveArgs& a,
-                            const cf_dual_quat* T, bool skin, cudaStream_t s);
+                            const cf_dual_quat* T, bool skin, cudaStream_t s, bool fr = false);
 cudaError_t launch_batch_gather(const Work& w, const Table& tb, cudaStream_t s);
 cudaError_t launch_batch_scatter(const Work& w, const Table& tb, cudaStream_t s);
 cudaError_t launch_assemble(const Work& w, const Pattern& p, const SolveArgs& a, const cf_dual_quat* T,

@@ -432,6 +432,7 @@ struct EdgeArgs {
   float4* out;     // [kEdgeTerms4 * n_edges]
   double* energy;  // [n_edges]
   int edge_ctas;   // the launch's first CTAs
+  float2* fr;      // non-null: (weight, residual) per correspondence, for the features
 };
 
 __device__ __forceinline__ int tri6(int p, int q) { return p * 6 - p * (p - 1) / 2 + (q - p); }
@@ -539,6 +540,7 @@ __global__ void __launch_bounds__(kThreads) residual_kernel(Table tb, Work w, Ed
     }
     w.c_srcfw[c] = make_float4(src.x, src.y, src.z, fw);
     w.c_nres[c] = make_float4(n.x, n.y, n.z, res);
+    if (ea.fr) ea.fr[c] = make_float2(fw, res);
   }
   double t = block_sum_d(e, red);
   if (threadIdx.x == 0) w.e_data_part[cta] = t;
@@ -577,11 +579,25 @@ __global__ void __launch_bounds__(kThreads) energy_kernel(Table tb, Work w, Patt
   if (threadIdx.x == 0) w.e_data_part[blockIdx.x] = t;
 }
 
+// Sum of p[0..n) by `stride` threads starting at `t`, in a fixed order per
+// thread, with 8 loads in flight at a time.
+__device__ __forceinline__ double strided_sum(const double* p, int n, int t, int stride) {
+  double v = 0.0;
+  for (int k0 = t; k0 < n; k0 += 8 * stride) {
+    double x[8];
+#pragma unroll
+    for (int b = 0; b < 8; b++) x[b] = k0 + b * stride < n ? __ldcg(p + k0 + b * stride) : 0.0;
+#pragma unroll
+    for (int b = 0; b < 8; b++)
+      if (k0 + b * stride < n) v += x[b];
+  }
+  return v;
+}
+
 // One warp per problem: its energy = the sum of its CTAs' partials.
 __global__ void energy_reduce_kernel(Table tb, Work w, int slot) {
   const ProbDesc d = tb.desc[blockIdx.x];
-  double v = 0.0;
-  for (int k = threadIdx.x; k < d.e_ctas; k += 32) v += w.e_data_part[d.e_cta0 + k];
+  double v = strided_sum(w.e_data_part + d.e_cta0, d.e_ctas, threadIdx.x, 32);
   v = warp_sum_d(v);
   if (threadIdx.x == 0) {
     if (slot >= 0) {
@@ -596,13 +612,18 @@ __global__ void energy_reduce_kernel(Table tb, Work w, int slot) {
 // One warp per problem: the energy at the transforms the residual launch just
 // linearised at, from that launch's own partials (data-term CTA partials and
 // per-edge ARAP energies) -- no second skinning pass.
-__global__ void residual_energy_kernel(Table tb, Work w, Pattern pt, int slot) {
+// One CTA of 1024 threads per problem.
+__global__ void __launch_bounds__(1024) residual_energy_kernel(Table tb, Work w, Pattern pt, int slot) {
+  __shared__ double red[32];
   const ProbDesc d = tb.desc[blockIdx.x];
-  double v = 0.0;
-  for (int k = threadIdx.x; k < d.e_ctas; k += 32) v += w.e_data_part[d.e_cta0 + k];
   const int e0 = pt.prob_edge_off[blockIdx.x], e1 = pt.prob_edge_off[blockIdx.x + 1];
-  for (int e = e0 + threadIdx.x; e < e1; e += 32) v += pt.edge_energy[e];
+  double v = strided_sum(w.e_data_part + d.e_cta0, d.e_ctas, threadIdx.x, 1024) +
+             strided_sum(pt.edge_energy + e0, e1 - e0, threadIdx.x, 1024);
   v = warp_sum_d(v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x >= 32) return;
+  v = warp_sum_d(red[threadIdx.x]);
   if (threadIdx.x == 0) {
     if (slot >= 0) {
       w.stats[blockIdx.x].energy[slot] = v;
@@ -739,7 +760,7 @@ cudaError_t launch_node_plain(const Work& w, const cf_deform_node* nodes, const 
 }
 
 cudaError_t launch_residual(const Work& w, const Table& tb, const Pattern& p, const SolveArgs& a,
-                            const cf_dual_quat* T, bool skin, cudaStream_t s) {
+                            const cf_dual_quat* T, bool skin, cudaStream_t s, bool fr) {
   EdgeArgs ea;
   ea.edge_ijk = p.edge_ijk;
   ea.n_edges = p.n_edges;
@@ -750,6 +771,7 @@ cudaError_t launch_residual(const Work& w, const Table& tb, const Pattern& p, co
   ea.out = p.edge_terms;
   ea.energy = p.edge_energy;
   ea.edge_ctas = cdiv(p.n_edges, kThreads);
+  ea.fr = fr ? w.c_fr : nullptr;
   const int grid = tb.n_e + ea.edge_ctas;
   if (grid <= 0) return cudaSuccess;
   if (skin)
@@ -761,7 +783,7 @@ cudaError_t launch_residual(const Work& w, const Table& tb, const Pattern& p, co
 
 cudaError_t launch_residual_energy(const Work& w, const Pattern& p, const SolveArgs& a, int slot, cudaStream_t s) {
   if (a.tb.P <= 0) return cudaSuccess;
-  residual_energy_kernel<<<a.tb.P, 32, 0, s>>>(a.tb, w, p, slot);
+  residual_energy_kernel<<<a.tb.P, 1024, 0, s>>>(a.tb, w, p, slot);
   return cudaGetLastError();
 }
 

@@ -415,17 +415,14 @@ __global__ void increments_kernel(const cf_dual_quat* __restrict__ to, const cf_
 // residual launch at T must have run; warp per node over its incidences).
 __global__ void features_kernel(const cf_dual_quat* __restrict__ T, const cf_dual_quat* __restrict__ hist, int N,
                                 const int* __restrict__ inc_start, const int* __restrict__ inc,
-                                const float4* __restrict__ c_srcfw, const float4* __restrict__ c_nres,
-                                float* __restrict__ feat) {
+                                const float2* __restrict__ c_fr, float* __restrict__ feat) {
   const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (i >= N) return;
   float s = 0.f, mx = 0.f;
   int cnt = 0;
-  // 4 incidences per lane in flight: their ids, then the weight and the
-  // residual of each (the .w of the two records), summed in incidence order
+  // 4 incidences per lane in flight: their ids, then the (weight, residual)
+  // pair of each (8 B, written by the residual launch), summed in incidence order
   const int q1 = inc_start[i + 1];
-  const float* fw = reinterpret_cast<const float*>(c_srcfw) + 3;
-  const float* rs = reinterpret_cast<const float*>(c_nres) + 3;
   for (int q0 = inc_start[i] + lane; q0 < q1; q0 += 4 * 32) {
     int c[4];
 #pragma unroll
@@ -433,8 +430,9 @@ __global__ void features_kernel(const cf_dual_quat* __restrict__ T, const cf_dua
     float f[4], r[4];
 #pragma unroll
     for (int b = 0; b < 4; b++) {
-      f[b] = c[b] >= 0 ? __ldg(fw + 4 * (size_t)c[b]) : 0.f;
-      r[b] = c[b] >= 0 ? __ldg(rs + 4 * (size_t)c[b]) : 0.f;
+      const float2 fr = c[b] >= 0 ? __ldg(c_fr + c[b]) : make_float2(0.f, 0.f);
+      f[b] = fr.x;
+      r[b] = fr.y;
     }
 #pragma unroll
     for (int b = 0; b < 4; b++)
@@ -634,7 +632,7 @@ cudaError_t launch_increments(const cf_dual_quat* to, const cf_dual_quat* from, 
 cudaError_t launch_features(const Work& w, const cf_dual_quat* T, const cf_dual_quat* hist, int N, float* feat,
                             cudaStream_t s) {
   if (N <= 0) return cudaSuccess;
-  features_kernel<<<cdiv(N * 32, 256), 256, 0, s>>>(T, hist, N, w.inc_start, w.inc, w.c_srcfw, w.c_nres, feat);
+  features_kernel<<<cdiv(N * 32, 256), 256, 0, s>>>(T, hist, N, w.inc_start, w.inc, w.c_fr, feat);
   return cudaGetLastError();
 }
 
