@@ -161,7 +161,7 @@ struct Work {
   long long* timers = nullptr;  // [kTimerSlots] phase cycles of the grid PCG (debug)
 };
 
-constexpr int kEnergyCtas = 592;  // residual/energy CTAs of a single solve
+constexpr int kEnergyCtas = 512;  // residual/energy CTAs of a single solve (with the edge CTAs, one wave at 4 per SM)
 constexpr int kMaxPcgCtas = 1024;
 constexpr int kSortCorrs = 4096;     // correspondences per sort CTA of a batched solve (at least)
 constexpr int kMaxSortCtas = 1 << 16;
