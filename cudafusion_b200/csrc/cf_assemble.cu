@@ -338,11 +338,11 @@ __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern p
   const float3 xr = node_pos(aa.nodes, r);
   int k = 0;
   while (k < nb && s_wpre[k + 1] <= wa) k++;
-  float acc[36], rhs[6];
+  // lane-private sums: an off-diagonal block's 36 values (p * 6 + q); the
+  // diagonal block's upper triangle (tri(p, q)) and its rhs (21 + p)
+  float acc[36];
 #pragma unroll
   for (int q = 0; q < 36; q++) acc[q] = 0.f;
-#pragma unroll
-  for (int q = 0; q < 6; q++) rhs[q] = 0.f;
   float3 xc = node_pos(aa.nodes, k < nb ? s_blk[k].z : r);
   int seg0 = k < nb ? s_blk[k].x : 0, segn = k < nb ? s_blk[k].y : 0;
   for (int win = wa; win < wb; win++) {
@@ -358,35 +358,41 @@ __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern p
         float Ja[6], Jb[6];
         jac_row(src, xr, n, sel4(w4, a), Ja);
         jac_row(src, xc, n, sel4(w4, b), Jb);
+        if (k == 0) {  // (the block index is uniform in the warp)
 #pragma unroll
-        for (int p = 0; p < 6; p++) {
-          const float f = sf.w * Ja[p];
+          for (int p = 0; p < 6; p++) {
+            const float f = sf.w * Ja[p];
 #pragma unroll
-          for (int q = 0; q < 6; q++) acc[p * 6 + q] += f * Jb[q];
-        }
-        if (k == 0 && a == b) {
+            for (int q = p; q < 6; q++) acc[tri(p, q)] += f * Jb[q];
+          }
+          if (a == b) {
 #pragma unroll
-          for (int p = 0; p < 6; p++) rhs[p] += -sf.w * Ja[p] * nr.w;
+            for (int p = 0; p < 6; p++) acc[21 + p] += -sf.w * Ja[p] * nr.w;
+          }
+        } else {
+#pragma unroll
+          for (int p = 0; p < 6; p++) {
+            const float f = sf.w * Ja[p];
+#pragma unroll
+            for (int q = 0; q < 6; q++) acc[p * 6 + q] += f * Jb[q];
+          }
         }
       }
     }
     // leaving block k (next window belongs to another block, or the run ends)
     if (win + 1 == wb || win + 1 == s_wpre[k + 1]) {
       float* dst = s_part + (size_t)(k + wid) * kPartVals;
-      float extra[4] = {acc[32], acc[33], acc[34], acc[35]};
-      reduce_scatter32(acc);
-      dst[lane] = acc[0];
+      if (k == 0) {  // 27 values (acc[27..31] stay zero): one reduce-scatter
+        reduce_scatter32(acc);
+        if (lane < 27) dst[lane] = acc[0];
+      } else {
+        float extra[4] = {acc[32], acc[33], acc[34], acc[35]};
+        reduce_scatter32(acc);
+        dst[lane] = acc[0];
 #pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const float v = warp_sum_f(extra[q]);
-        if (lane == 0) dst[32 + q] = v;
-      }
-      if (k == 0) {
-#pragma unroll
-        for (int q = 0; q < 6; q++) {
-          const float v = warp_sum_f(rhs[q]);
-          if (lane == 0) dst[36 + q] = v;
-          rhs[q] = 0.f;
+        for (int q = 0; q < 4; q++) {
+          const float v = warp_sum_f(extra[q]);
+          if (lane == 0) dst[32 + q] = v;
         }
       }
 #pragma unroll
@@ -417,14 +423,7 @@ __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern p
     const int w0 = s_wpre[kb], w1 = s_wpre[kb + 1];
     float tot = 0.f, comp = 0.f;
     if (w1 > w0) {
-      int idx;
-      if (kb == 0) {
-        int p = 0;
-        while (v >= 21 ? false : (tri(p, 5) < v)) p++;  // row of the upper-triangle index
-        idx = v < 21 ? p * 6 + (v - tri(p, p) + p) : 36 + (v - 21);
-      } else {
-        idx = v;
-      }
+      const int idx = v;  // diagonal block: tri(p, q), then the rhs at 21 + p; off-diagonal: p * 6 + q
       for (int ww = 0; ww < kWarps; ww++) {  // the warps whose window runs met block kb
         const int a_w = (int)((long long)W * ww / kWarps), b_w = (int)((long long)W * (ww + 1) / kWarps);
         if (a_w >= b_w || a_w >= w1 || b_w <= w0) continue;
