@@ -53,6 +53,7 @@ __device__ __forceinline__ double block_sum_d(double v, double* red) {
 __global__ void __launch_bounds__(kThreads) pack_count_kernel(Table tb, Work w) {
   extern __shared__ int hist[];
   __shared__ __align__(16) uint32_t stage2[2][kThreads * kWords];  // double-buffered tiles of records
+  __shared__ __align__(16) float cstage[2][kThreads * 3];           // and of canonical points
   const int tid = threadIdx.x;
   const ProbDesc d = tb.desc[tb.bin_prob[blockIdx.x]];
   const int N = d.N, lc = blockIdx.x - d.bin_cta0;
@@ -60,26 +61,37 @@ __global__ void __launch_bounds__(kThreads) pack_count_kernel(Table tb, Work w) 
   const cf_correspondence* corrs = d.corrs;
   const float* canon = d.canon;
   const bool al16 = ((reinterpret_cast<uintptr_t>(corrs) & 15u) == 0);
+  const bool cal16 = ((reinterpret_cast<uintptr_t>(canon) & 15u) == 0);
   const int cb = lc * d.chunk;
   const int ce = min(d.M, cb + d.chunk);
   // the next tile's records are in flight (cp.async) while this one is packed
-  auto issue = [&](int t0, uint32_t* buf) {
-    const int nw = min(kThreads, ce - t0) * kWords;
+  auto issue = [&](int t0, int b) {
+    const int nt = min(kThreads, ce - t0), nw = nt * kWords;
     const uint32_t* src = reinterpret_cast<const uint32_t*>(corrs) + (size_t)t0 * kWords;
+    uint32_t* buf = stage2[b];
     if (al16 && (nw & 3) == 0) {
       for (int i = tid; i < (nw >> 2); i += kThreads) cp_async16(buf + 4 * i, src + 4 * i);
     } else {
       for (int i = tid; i < nw; i += kThreads) cp_async4(buf + i, src + i);
     }
+    if (canon) {
+      const float* csrc = canon + 3 * (size_t)t0;
+      if (cal16 && ((3 * nt) & 3) == 0) {
+        for (int i = tid; i < (3 * nt) >> 2; i += kThreads) cp_async16(cstage[b] + 4 * i, csrc + 4 * i);
+      } else {
+        for (int i = tid; i < 3 * nt; i += kThreads) cp_async4(cstage[b] + i, csrc + i);
+      }
+    }
     cp_async_commit();
   };
-  if (cb < ce) issue(cb, stage2[0]);
+  if (cb < ce) issue(cb, 0);
   __syncthreads();
   for (int t0 = cb, it = 0; t0 < ce; t0 += kThreads, it++) {
     const int n = min(kThreads, ce - t0);
     const uint32_t* stage = stage2[it & 1];
+    const float* cst = cstage[it & 1];
     if (t0 + kThreads < ce) {
-      issue(t0 + kThreads, stage2[(it & 1) ^ 1]);
+      issue(t0 + kThreads, (it & 1) ^ 1);
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
@@ -91,7 +103,7 @@ __global__ void __launch_bounds__(kThreads) pack_count_kernel(Table tb, Work w) 
       const int c = d.corr_off + cl;     // concatenated index
       float3 p;
       if (canon) {
-        p = f3(__ldg(canon + 3 * (size_t)cl), __ldg(canon + 3 * (size_t)cl + 1), __ldg(canon + 3 * (size_t)cl + 2));
+        p = f3(cst[3 * tid], cst[3 * tid + 1], cst[3 * tid + 2]);
       } else {
         p = f3(__uint_as_float(rec[0]), __uint_as_float(rec[1]), __uint_as_float(rec[2]));
       }
