@@ -130,3 +130,24 @@ def test_autotune_chooses_times_and_remembers(batch):
     s2 = _solver(batch)
     r2 = s2.autotune(dps, [d.init_transforms.clone() for d in dps], *CLAMPS)
     assert r2["from_cache"] == 1 and r2["pcg_mode"] == r["pcg_mode"] and r2["stream_tile"] == r["stream_tile"]
+
+
+def test_batched_large_sort_grid(batch):
+    """A batch past 2 sort CTAs per SM (one per 4096 correspondences: 1.8M
+    correspondences, ~440 sort CTAs), after a small batch on the same handle
+    (the sort table grows): each problem still gets its own solve's result."""
+    big = [synth.sphere_problem(num_nodes=3000, num_corrs=600000, node_radius=np.sqrt(4 * np.pi * 0.09 / 3000),
+                                seed=40 + k) for k in range(3)]
+    s = GaussNewtonSolver(Params(**KW), max_nodes=sum(p.num_nodes for p in big),
+                          max_corrs=sum(p.num_corrs for p in big))
+    _run_batched(s, batch)
+    Tb, st = _run_batched(s, big)
+    for k, p in enumerate(big):
+        s1 = GaussNewtonSolver(Params(**KW), max_nodes=p.num_nodes, max_corrs=p.num_corrs)
+        s1.set_option(_lib.CF_OPT_PCG_MODE, 1)
+        d = DeviceProblem(p)
+        T = d.init_transforms.clone()
+        st1 = s1.gn_solve(d, T, *CLAMPS)
+        assert st[k]["error_flags"] == 0
+        assert np.abs(Tb[k] - dq_as_array(T.cpu().numpy().view(DQ_DTYPE))).max() < 2e-5
+        assert abs(st[k]["energy_final"] - st1["energy_final"]) / abs(st1["energy_final"]) < 1e-5
