@@ -389,11 +389,24 @@ __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern p
         float extra[4] = {acc[32], acc[33], acc[34], acc[35]};
         reduce_scatter32(acc);
         dst[lane] = acc[0];
+        // the last 4 values: halved over lane bits 4 and 3 (3 exchanges),
+        // then summed over bits 2..0; lane 8g holds value 2 (g >> 1) + (g & 1)
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-          const float v = warp_sum_f(extra[q]);
-          if (lane == 0) dst[32 + q] = v;
+        for (int q = 0; q < 2; q++) {
+          const bool up = (lane & 16) != 0;
+          const float send = up ? extra[q] : extra[q + 2];
+          const float keep = up ? extra[q + 2] : extra[q];
+          extra[q] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
         }
+        {
+          const bool up = (lane & 8) != 0;
+          const float send = up ? extra[0] : extra[1];
+          const float keep = up ? extra[1] : extra[0];
+          extra[0] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+        }
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) extra[0] += __shfl_xor_sync(0xffffffffu, extra[0], o);
+        if ((lane & 7) == 0) dst[32 + 2 * ((lane >> 4) & 1) + ((lane >> 3) & 1)] = extra[0];
       }
 #pragma unroll
       for (int q = 0; q < 36; q++) acc[q] = 0.f;
