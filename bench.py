@@ -168,6 +168,21 @@ def algorithmic_bytes(N, M, nnzb, pcg_iters_used):
     return {"assembly": b_asm, "pcg": b_pcg_it * pcg_iters_used, "pcg_per_iteration": b_pcg_it}
 
 
+def pattern_blocks(nodes):
+    """Blocks of a problem's BSR pattern: the diagonal and every graph edge in
+    both directions (the rule of kernels/solver_kernels.cu:498-541)."""
+    import numpy as np
+
+    N = len(nodes)
+    nn = np.minimum(np.maximum(nodes["num_neighbors"], 0), 8)
+    i = np.repeat(np.arange(N, dtype=np.int64), 8)
+    j = nodes["neighbors"].reshape(-1).astype(np.int64)
+    ok = (np.tile(np.arange(8), N) < nn[i]) & (j >= 0) & (j < N)
+    i, j = i[ok], j[ok]
+    d = np.arange(N, dtype=np.int64)
+    return int(np.unique(np.concatenate([i * N + j, j * N + i, d * (N + 1)])).size)
+
+
 def cpu_baseline(problem, nthreads, reps=3):
     """The oracle (FP32, reference operation order) on the host cores."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -500,6 +515,15 @@ def run_batch(args, world, rank, local):
         side.synchronize()
         ms = [ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(args.steps)]
         st = s.gn_solve_batched(dps, Ts, MAX_ROT, MAX_TRANS, stream=side)
+        graphed = bool(s.get_option(_lib.CF_OPT_GRAPH_ACTIVE))
+        # per-phase device times of one direct-launch pass (the profiler turns
+        # the graph off) for the bandwidth figures
+        s.profile_enable(True)
+        reset()
+        s.gn_solve_batched(dps, Ts, MAX_ROT, MAX_TRANS, stats=False, stream=side)
+        side.synchronize()
+        ph = s.profile_read()
+        s.profile_enable(False)
         one = GaussNewtonSolver(prm, max_nodes=max(p.num_nodes for p in probs),
                                 max_corrs=max(p.num_corrs for p in probs))
         seq = []
@@ -515,13 +539,27 @@ def run_batch(args, world, rank, local):
             side.synchronize()
             seq.append(a.elapsed_time(b))
     batch_ms = float(np.median(ms))
+    # algorithmic bytes of the workload model, per problem (its own PCG iterations)
+    b_asm = b_pcg = 0
+    for p, x in zip(probs, st):
+        ab = algorithmic_bytes(p.num_nodes, p.num_corrs, pattern_blocks(p.nodes), 1)
+        b_asm += GN_ITERS * ab["assembly"]
+        b_pcg += sum(x["pcg_iterations"]) * ab["pcg_per_iteration"]
+    hbm, peak_kind = peaks()
+    asm_gbs = b_asm / (ph["assemble"][0] * 1e-3) / 1e9
+    pcg_gbs = b_pcg / (ph["pcg"][0] * 1e-3) / 1e9
     return {"workload": f"batched uneven solves: {len(probs)} sphere problems, N={Nt} nodes, M={Mt} "
                         f"correspondences in total, {GN_ITERS} GN x {PCG_ITERS} PCG, lambda_smooth 10, damping 1.0",
             "batched_ms": batch_ms, "solves_per_s": len(probs) / (batch_ms * 1e-3),
             "per_problem_latency_ms": batch_ms, "sequential_ms": float(sum(seq)),
             "sequential_per_problem_ms": float(np.mean(seq)), "speedup_vs_sequential": float(sum(seq)) / batch_ms,
-            "autotune": tune, "cuda_graph": bool(s.get_option(_lib.CF_OPT_GRAPH_ACTIVE)),
-            "error_flags": int(max(x["error_flags"] for x in st)), "steps": args.steps, "warmup": args.warmup}
+            "autotune": tune, "cuda_graph": graphed,
+            "error_flags": int(max(x["error_flags"] for x in st)), "steps": args.steps, "warmup": args.warmup,
+            "assembly_gbs": asm_gbs, "pcg_gbs": pcg_gbs,
+            "assembly_frac_of_hbm": asm_gbs / hbm, "pcg_frac_of_hbm": pcg_gbs / hbm,
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+            "note": "the batch's system and records exceed the 126 MB L2: the streamed PCG re-reads A from HBM "
+                    "every iteration (algorithmic bytes of the workload model / event-timed device time)"}
 
 
 def run_reference(args, world, rank, local):
