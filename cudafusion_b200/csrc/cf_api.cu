@@ -114,7 +114,7 @@ void free_pattern(Pattern& p) {
   dfree(p.clu_row_begin); dfree(p.ustart); dfree(p.low_ptr); dfree(p.clu_opnd); dfree(p.clu_push);
   dfree(p.clu_halo_ptr); dfree(p.clu_halo); dfree(p.g_vidx); dfree(p.g_halo_ptr); dfree(p.g_halo_col);
   dfree(p.off_upper); dfree(p.pcg_cta_off); dfree(p.pcg_prob); dfree(p.prob_edge_off);
-  dfree(p.st_tile_ptr); dfree(p.st_tile_row); dfree(p.edge_terms); dfree(p.edge_energy);
+  dfree(p.st_tile_ptr); dfree(p.st_tile_row); dfree(p.st_tile_cols); dfree(p.edge_terms); dfree(p.edge_energy);
   p = Pattern();
 }
 
@@ -480,7 +480,7 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
     break;
   }
   // systems too large for shared memory (or mode 3): the streaming PCG
-  std::vector<int> tile_ptr, tile_row;
+  std::vector<int> tile_ptr, tile_row, tile_cols;
   const bool stream = rb2.empty();
   if (stream) {
     const int TB = h->stream_tile == 128 ? 128 : 256;
@@ -498,6 +498,13 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
       if (r1 > r0) tile_row.push_back(r1);  // end of the last tile
       tile_ptr.push_back((int)tile_row.size());
     }
+    // each tile's column indices, padded to TB with -1 (a stage's second copy)
+    tile_cols.assign(tile_row.size() * (size_t)TB, -1);
+    for (size_t c = 0; c + 1 < tile_ptr.size(); c++)
+      for (int t = tile_ptr[c]; t + 1 < tile_ptr[c + 1]; t++) {
+        const int b0 = row_ptr[tile_row[t]], b1 = row_ptr[tile_row[t + 1]];
+        for (int q = b0; q < b1 && q - b0 < TB; q++) tile_cols[(size_t)t * TB + (q - b0)] = col_idx[q];
+      }
     g_halo_ptr.assign(rb2.size(), 0);
     g_halo_col.clear();
     smem = pcg_stream_smem_bytes(TB);
@@ -635,6 +642,7 @@ cf_status build_pattern_host(cf_gn* h, const std::vector<cf_deform_node>& nodes,
   if (stream) {
     CF_TRY(up(&p.st_tile_ptr, tile_ptr));
     CF_TRY(up(&p.st_tile_row, tile_row));
+    CF_TRY(up(&p.st_tile_cols, tile_cols));
     Work& w = h->w;
     if (!w.minv32) {
       CF_TRY(dalloc(&w.r, 6 * (size_t)w.max_nodes));

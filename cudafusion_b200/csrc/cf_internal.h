@@ -116,6 +116,7 @@ struct Pattern {
   int st_tile_blocks = 256;    // blocks per tile (256 or 128)
   int* st_tile_ptr = nullptr;  // [pcg_ctas+1] into st_tile_row
   int* st_tile_row = nullptr;  // per CTA: its tiles' first rows, then its end row
+  int* st_tile_cols = nullptr; // [entries of st_tile_row][tile blocks] each tile's column indices, -1 padded
 };
 
 // Per-handle work buffers sized by (max_nodes, max_corrs).

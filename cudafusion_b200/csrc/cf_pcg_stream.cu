@@ -20,7 +20,10 @@
 //   update thread per row: x += alpha p, r -= alpha Ap, z = M^-1 r, r.r and
 //          r.z accumulated.  -> group reduction (barrier B)
 // The tiles of the next iteration are prefetched while the reductions run;
-// copies still in flight when the loop ends are drained before exit.
+// copies still in flight when the loop ends are drained before exit.  Each
+// stage also brings the tile's column indices (a padded copy made with the
+// pattern), so the SpMV operand of tile t + 1 is gathered while tile t's rows
+// are summed: one exposed gather per iteration instead of one per tile.
 #include "cf_device.cuh"
 #include "cf_internal.h"
 
@@ -133,11 +136,13 @@ struct StreamArgs {
 template <int TB>
 __global__ void __launch_bounds__(kThreads, 2) pcg_stream_kernel(StreamArgs P) {
   static_assert(TB <= kThreads, "one thread per block of a tile");
-  constexpr int kTileBlocks = TB, kTileBytes = TB * 36 * 4;
+  constexpr int kTileBlocks = TB, kTileBytes = TB * 36 * 4, kStageBytes = kTileBytes + TB * 4;
   extern __shared__ __align__(128) unsigned char smem[];
-  float* ring = reinterpret_cast<float*>(smem);                          // [kStages][kTileBlocks*36]
-  float* sPart = reinterpret_cast<float*>(smem + kStages * kTileBytes);  // [kTileBlocks][7]
-  double* sRed = reinterpret_cast<double*>(smem + kStages * kTileBytes + kTileBlocks * kPartStride * 4);  // [64]
+  float* ring = reinterpret_cast<float*>(smem);                           // [kStages] x (A tile, column indices)
+  float* sPart = reinterpret_cast<float*>(smem + kStages * kStageBytes);  // [kTileBlocks][7]
+  double* sRed = reinterpret_cast<double*>(smem + kStages * kStageBytes + kTileBlocks * kPartStride * 4);  // [64]
+  auto stageA = [&](int s) { return reinterpret_cast<const float*>(smem + (size_t)s * kStageBytes); };
+  auto stageC = [&](int s) { return reinterpret_cast<const int*>(smem + (size_t)s * kStageBytes + kTileBytes); };
   __shared__ uint64_t mbar[kStages];
   const Work& w = P.w;
   const Pattern& pt = P.pt;
@@ -169,9 +174,11 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_stream_kernel(StreamArgs P) {
     const int t = (int)(k % n_tiles), s = (int)(k % kStages);
     const int b0 = pt.row_ptr[trow[t]], b1 = pt.row_ptr[trow[t + 1]];
     const unsigned bytes = (unsigned)(b1 - b0) * 144u;
+    unsigned char* dst = smem + (size_t)s * kStageBytes;
     fence_proxy_async();
-    mbar_expect_tx(&mbar[s], bytes);
-    bulk_g2s(ring + (size_t)s * kTileBlocks * 36, pt.values + (size_t)b0 * 36, bytes, &mbar[s]);
+    mbar_expect_tx(&mbar[s], bytes + TB * 4u);
+    bulk_g2s(dst, pt.values + (size_t)b0 * 36, bytes, &mbar[s]);
+    bulk_g2s(dst + kTileBytes, pt.st_tile_cols + (size_t)(t_begin + t) * TB, TB * 4u, &mbar[s]);
   };
   auto top_up = [&]() {  // keep kStages tiles in flight
     while (issued < consumed + kStages) {
@@ -278,23 +285,28 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_stream_kernel(StreamArgs P) {
     float* pnew = (it & 1) ? w.p1 : w.p0;
     // ---- Ap = A (z + beta p_old), p = z + beta p_old, p.Ap ----
     double ppap = 0.0;
+    // the operand of the tile in stage s (its column indices came with A;
+    // -1 pads past the tile's blocks): z_j and p_old_j into registers
+    float gz[6], gp[6];
+    auto gather = [&](int s) {
+      const int j = stageC(s)[tid < TB ? tid : 0];
+      if (tid < TB && j >= 0) {
+        ld6(w.z + (size_t)j * 6, gz);
+        if (it > 0) ld6(pold + (size_t)j * 6, gp);
+      }
+    };
     for (int t = 0; t < n_tiles; t++) {
       const int s = (int)(consumed % kStages);
       if (!mbar_wait(&mbar[s], (phase_bits >> s) & 1u, err, kCopyWaitLimit)) ok = false;
+      if (t == 0) gather(s);  // (later tiles were gathered during the previous one)
       phase_bits ^= 1u << s;
-      const float* A = ring + (size_t)s * kTileBlocks * 36;
+      const float* A = stageA(s);
       const int ra = trow[t], rb_ = trow[t + 1];
       const int b0 = pt.row_ptr[ra], nb = pt.row_ptr[rb_] - b0;
       if (tid < nb) {
-        const int j = pt.col_idx[b0 + tid];
         float v[6];
-        ld6(w.z + (size_t)j * 6, v);
-        if (it > 0) {
-          float po[6];
-          ld6(pold + (size_t)j * 6, po);
 #pragma unroll
-          for (int q = 0; q < 6; q++) v[q] = __fmaf_rn(betaf, po[q], v[q]);
-        }
+        for (int q = 0; q < 6; q++) v[q] = (it > 0) ? __fmaf_rn(betaf, gp[q], gz[q]) : gz[q];
         const float4* A4 = reinterpret_cast<const float4*>(A + tid * 36);
         float Ab[36];
 #pragma unroll
@@ -309,6 +321,11 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_stream_kernel(StreamArgs P) {
           for (int q = 0; q < 6; q++) acc = __fmaf_rn(Ab[c * 6 + q], v[q], acc);
           sPart[tid * kPartStride + c] = acc;
         }
+      }
+      if (t + 1 < n_tiles) {  // the next tile's operand, in flight during this tile's row sums
+        const int s2 = (int)((consumed + 1) % kStages);
+        if (!mbar_wait(&mbar[s2], (phase_bits >> s2) & 1u, err, kCopyWaitLimit)) ok = false;
+        gather(s2);
       }
       __syncthreads();
       consumed++;
@@ -413,7 +430,7 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_stream_kernel(StreamArgs P) {
 
 }  // namespace
 
-int pcg_stream_smem_bytes(int tb) { return kStages * tb * 144 + tb * kPartStride * 4 + 64 * 8; }
+int pcg_stream_smem_bytes(int tb) { return kStages * tb * 148 + tb * kPartStride * 4 + 64 * 8; }
 static_assert(kStages * 128 * 144 >= (kThreads / 8) * 108 * 8, "the ring holds the inversion scratch");
 
 namespace {
