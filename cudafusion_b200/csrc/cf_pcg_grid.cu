@@ -79,7 +79,7 @@ __device__ __forceinline__ double bsum(double v, double* red) {
 // an acquire poll.  (Per-CTA flags polled by every CTA measured 2-3x slower
 // on B200: G*G acquire loads per round.)  Bounded: gives up after spin_limit
 // polls, records kErrTimeout, and every later barrier of the launch returns
-// at once.
+// within 32 polls.
 // The arrive and the bounded wait of the barrier, by one thread.
 __device__ __forceinline__ void arrive_wait(unsigned* ctr, unsigned gen, int G, int* err, unsigned spin_limit,
                                             unsigned extra) {
@@ -87,7 +87,9 @@ __device__ __forceinline__ void arrive_wait(unsigned* ctr, unsigned gen, int G, 
   const unsigned target = (gen + 1u) * (unsigned)G + extra;
   unsigned polls = 0;
   while (ld_acquire_gpu(ctr) < target) {
-    if (*(volatile int*)err != 0) break;
+    // the error word only every 32 polls: a poll is then one round trip
+    // to L2, not two
+    if ((polls & 31) == 31 && *(volatile int*)err != 0) break;
     if (++polls > spin_limit) {
       atomicOr(err, kErrTimeout);
       break;

@@ -103,7 +103,9 @@ __device__ __forceinline__ void gbar_s(unsigned* ctr, unsigned gen, int G, int* 
     const unsigned target = (gen + 1u) * (unsigned)G + extra;
     unsigned polls = 0;
     while (ld_acquire_gpu(ctr) < target) {
-      if (*(volatile int*)err != 0) break;
+      // the error word only every 32 polls: a poll is then one round trip
+      // to L2, not two
+      if ((polls & 31) == 31 && *(volatile int*)err != 0) break;
       if (++polls > spin_limit) {
         atomicOr(err, kErrTimeout);
         break;
