@@ -562,6 +562,255 @@ def run_batch(args, world, rank, local):
                     "every iteration (algorithmic bytes of the workload model / event-timed device time)"}
 
 
+CORR_METRIC = "ms per projective correspondence search, 640x480 frame, stock window (radius 50)"
+
+
+def corr_workload():
+    """The correspondence-search workload: the 640x480 two-cylinder frame
+    (camera moved 0.6 deg / 4 mm, joint estimate 3 deg behind the depth) and
+    the stock search parameters of config/params.yaml:60-63."""
+    from cudafusion_b200 import synth
+    from cudafusion_b200.corr import CorrParams
+
+    return synth.corr_frame(seed=37), CorrParams()
+
+
+def corr_candidates(frame, prm):
+    """Candidates the searched pixels of `frame` evaluate: each pixel's window
+    clipped to the image (projection rounded in FP64: within a few pixels of
+    the kernel's count over the frame)."""
+    W, H = frame.width, frame.height
+    fx, fy, cx, cy = (float(v) for v in frame.cam)
+    v = frame.live_vertices.astype(np.float64)
+    n = frame.live_normals.astype(np.float64)
+    T = frame.T_cam_world.astype(np.float64)
+    vc = v @ T[:3, :3].T + T[:3, 3]
+    nc = n @ T[:3, :3].T
+    ok = (np.linalg.norm(v, axis=-1) >= 1e-6) & (np.linalg.norm(n, axis=-1) >= 1e-6) & (vc[:, 2] > 0)
+    z = np.where(ok, vc[:, 2], 1.0)
+    pu = np.rint(fx * vc[:, 0] / z + cx)
+    pv = np.rint(fy * vc[:, 1] / z + cy)
+    ok &= (pu >= 0) & (pu < W) & (pv >= 0) & (pv < H)
+    vd = -vc / np.maximum(np.linalg.norm(vc, axis=-1, keepdims=True), 1e-300)
+    ok &= np.abs(np.sum(nc * vd, -1)) >= prm.view_threshold
+    r = max(0, prm.search_radius_px)
+    wx = np.minimum(pu + r, W - 1) - np.maximum(pu - r, 0) + 1
+    wy = np.minimum(pv + r, H - 1) - np.maximum(pv - r, 0) + 1
+    return int(np.sum(np.where(ok, wx * wy, 0)))
+
+
+def run_corr(args, world, rank, local):
+    """`--workload corr`: the projective correspondence search (the solve's
+    input, DynamicFusionPipeline::find_correspondences) on the B200."""
+    import torch
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from cudafusion_b200.corr import CORR_BYTES, CorrespondenceSearch, DeviceCorrFrame
+
+    frame, prm = corr_workload()
+    P = frame.num_pixels
+    dev = DeviceCorrFrame(frame)
+    search = CorrespondenceSearch(frame.width, frame.height)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        for _ in range(args.warmup):
+            flush.fill_(1)
+            search.launch(dev, prm, stream=side)
+        search.launch(dev, prm, debug=True, stream=side)
+    side.synchronize()
+    stats = search.stats.cpu().numpy().tolist()
+    num_valid = int(search.num_valid.item())
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    sampler = ClockSampler(local) if rank == 0 else None
+    barrier(world)
+    if sampler:
+        sampler.start()
+    launches0 = search.launch_count()
+    t_wall = time.perf_counter()
+    with torch.cuda.stream(side):
+        for k in range(args.steps):
+            flush.fill_(1)
+            evs[k][0].record(side)
+            search.launch(dev, prm, stream=side)
+            evs[k][1].record(side)
+    side.synchronize()
+    barrier(world)
+    t_wall = time.perf_counter() - t_wall
+    clocks = sampler.stop() if sampler else None
+    launches = search.launch_count() - launches0
+    per_step = [a.elapsed_time(b) for a, b in evs]
+    value = replica_value(sum(per_step), args.steps, world)
+
+    # end to end through the public API: the frame's per-pixel inputs from
+    # pinned host memory, the search, the records and the count back
+    def pin(t):
+        return t.cpu().pin_memory()
+
+    hosts = [(dev.live_vertices, pin(dev.live_vertices)), (dev.live_normals, pin(dev.live_normals)),
+             (dev.depth, pin(dev.depth)), (dev.depth_normals, pin(dev.depth_normals)),
+             (dev.pixel_knn, pin(dev.pixel_knn)), (dev.pixel_knn_w, pin(dev.pixel_knn_w))]
+    h_out = torch.empty(P * CORR_BYTES, dtype=torch.uint8).pin_memory()
+    h_n = torch.empty(1, dtype=torch.int32).pin_memory()
+    e2e_times = []
+    barrier(world)
+    with torch.cuda.stream(side):
+        for _ in range(max(3, min(args.steps, 10))):
+            flush.fill_(1)
+            side.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(side)
+            for d, h in hosts:
+                d.copy_(h, non_blocking=True)
+            search.launch(dev, prm, stream=side)
+            h_out.copy_(search.corrs[: P * CORR_BYTES], non_blocking=True)
+            h_n.copy_(search.num_valid, non_blocking=True)
+            b.record(side)
+            side.synchronize()
+            e2e_times.append(a.elapsed_time(b))
+    e2e_ms = replica_value(sum(e2e_times), len(e2e_times), world)
+    h2d = sum(h.numel() * h.element_size() for _, h in hosts)
+    d2h = P * CORR_BYTES + 4
+    if rank != 0:
+        return None
+
+    hbm, peak_kind = peaks()
+    cands = corr_candidates(frame, prm)
+    # per-pixel bytes the search must move at least once: live vertex and
+    # normal, depth and its normal, the node lists in, the record out
+    alg_bytes = P * (12 + 12 + 4 + 12 + 32 + CORR_BYTES)
+    achieved = alg_bytes / (value * 1e-3) / 1e9
+    smem_peak = 148 * 128 * 1.965e9 / 1e9  # nominal: 148 SMs x 128 B/clock x 1965 MHz
+    smem_achieved = cands * 24 / (value * 1e-3) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline:
+        import oracle as O
+
+        sample = np.sort(np.random.default_rng(0).choice(P, 8192, replace=False)).astype(np.int32)
+        t0 = time.perf_counter()
+        O.find_correspondences(frame, prm.dist_threshold, prm.angle_threshold, prm.view_threshold,
+                               prm.search_radius_px, pixels=sample)
+        dt = time.perf_counter() - t0
+        cpu = {"value": dt * 1e3 * P / sample.size, "unit": "ms", "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": f"{sample.size} random pixels of the frame (FP32 C oracle, OpenMP), scaled to {P} pixels"}
+    return {
+        "metric": CORR_METRIC,
+        "value": value,
+        "unit": "ms",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": value * world,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": f"two-cylinder {frame.width}x{frame.height} frame, projective search radius "
+                        f"{prm.search_radius_px}, dist {prm.dist_threshold}, angle {prm.angle_threshold}, "
+                        f"view {prm.view_threshold} (config/params.yaml:60-63)",
+            "pixels": P, "valid": num_valid, "stats": stats, "candidates": cands,
+            "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
+        },
+        "roofline": {"kernel": "corr_search", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": load_traffic("corr_search"),
+                     "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": value,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "note": "HBM is not what bounds this search: every candidate is read from shared memory; "
+                             "see roofline_smem"},
+        "roofline_smem": {"bound": "shared memory", "achieved": smem_achieved, "peak": smem_peak, "unit": "GB/s",
+                          "frac": smem_achieved / smem_peak, "bytes_per_candidate": 24, "candidates": cands,
+                          "peak_source": "nominal (148 SMs x 128 B/clock x 1965 MHz)"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "gpu_launches_per_step": launches / args.steps,
+        "clocks": clocks,
+        "wall_s_timed_region": t_wall,
+    }
+
+
+def run_reference_corr(args, world, rank, local):
+    """`--impl reference --workload corr`: the reference's own
+    compute_pixel_knn_kernel + find_correspondences_kernel (with the
+    pipeline's memsets, include/fusion_app.h:1791-1845) on the same frame."""
+    import torch
+
+    if rank != 0:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_corr
+
+    if not ref_corr.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libcfref_corr.so was not built "
+                "(needs the reference sources: make -C oracle ref)"}
+    from cudafusion_b200.types import CORR_DTYPE
+
+    frame, prm = corr_workload()
+    ref = ref_corr.RefCorrSearch(frame)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    def one():
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        _, ms = ref.run(prm.dist_threshold, prm.angle_threshold, prm.view_threshold, prm.search_radius_px,
+                        debug=False)
+        return ms
+
+    for _ in range(args.warmup):
+        one()
+    sampler = ClockSampler(local)
+    sampler.start()
+    times = [one() for _ in range(args.steps)]
+    clocks = sampler.stop()
+    value = sum(times) / len(times)
+    out = np.zeros(frame.num_pixels, CORR_DTYPE)
+    e2e = []
+    for _ in range(max(3, min(args.steps, 5))):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ref.upload()
+        ref.run(prm.dist_threshold, prm.angle_threshold, prm.view_threshold, prm.search_radius_px, debug=False)
+        ref.download_records(out)
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    ref.close()
+    P = frame.num_pixels
+    return {
+        "impl": "reference",
+        "metric": CORR_METRIC,
+        "value": value,
+        "unit": "ms",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": value,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": f"two-cylinder {frame.width}x{frame.height} frame, projective search radius "
+                        f"{prm.search_radius_px}, dist {prm.dist_threshold}, angle {prm.angle_threshold}, "
+                        f"view {prm.view_threshold} (config/params.yaml:60-63)",
+            "implementation": "CUDAFusion compute_pixel_knn_kernel + find_correspondences_kernel with the "
+                              "pipeline's memsets, rebuilt for sm_100a with --use_fast_math "
+                              "(oracle/_ref/libcfref_corr.so)",
+            "l2": "flushed between steps (256 MiB write)",
+            "parallelism": "single GPU (rank 0 of the launch)",
+        },
+        "cpu_baseline": {"value": value, "unit": "ms", "cores": 1, "kind": "reference",
+                         "sample": "the reference path is CUDA: the search timed on the GPU, one host thread"},
+        "e2e": {"value": statistics.median(e2e), "unit": "ms",
+                "h2d_bytes_per_step": int(P * (12 + 12 + 4 + 12 + 4)),
+                "d2h_bytes_per_step": int(P * CORR_DTYPE.itemsize)},
+        "clocks": clocks,
+    }
+
+
 def run_reference(args, world, rank, local):
     import torch
 
@@ -657,17 +906,21 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-start comparison")
     ap.add_argument("--no-precision", action="store_true", help="skip the 8192-node precision study")
     ap.add_argument("--pcg-mode", type=int, default=0, help="0 auto, 1 grid-wide, 2 single cluster, 3 streaming")
-    ap.add_argument("--workload", default="frame", choices=["frame", "batch", "learned"],
+    ap.add_argument("--workload", default="frame", choices=["frame", "batch", "learned", "corr"],
                     help="frame: the headline line; batch / learned: the batched-solve and learned-start "
-                         "measurements alone")
+                         "measurements alone; corr: the projective correspondence search")
     ap.add_argument("--problems", type=int, default=64, help="problems of --workload batch")
     ap.add_argument("--frames", type=int, default=300, help="frames of --workload learned")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
     try:
-        if args.impl == "reference":
+        if args.impl == "reference" and args.workload == "corr":
+            line = run_reference_corr(args, world, rank, local)
+        elif args.impl == "reference":
             line = run_reference(args, world, rank, local)
+        elif args.workload == "corr":
+            line = run_corr(args, world, rank, local)
         elif args.workload == "batch":
             line = run_batch(args, world, rank, local) if rank == 0 else None
         elif args.workload == "learned":

@@ -76,6 +76,12 @@ EXPORTS = [
     "cf_gn_profile_read",
     "cf_gn_profile_name",
     "cf_gn_launch_count",
+    "cf_corr_search_create",
+    "cf_corr_search_destroy",
+    "cf_find_correspondences",
+    "cf_compute_pixel_knn",
+    "cf_corr_search_launch_count",
+    "cf_corr_search_set_chunks",
     "cf_get_version",
     "cf_last_cuda_error",
 ]
@@ -105,6 +111,43 @@ class Problem(ctypes.Structure):
         ("max_rot", ctypes.c_float),
         ("max_trans", ctypes.c_float),
         ("update_scale", ctypes.c_float),
+    ]
+
+
+class Camera(ctypes.Structure):
+    """cf_camera = CameraIntrinsics (include/types.h:148-162)."""
+
+    _fields_ = [("fx", ctypes.c_float), ("fy", ctypes.c_float), ("cx", ctypes.c_float), ("cy", ctypes.c_float),
+                ("width", ctypes.c_int), ("height", ctypes.c_int)]
+
+
+class Mat4(ctypes.Structure):
+    """cf_mat4 = Mat4 (include/types.h:26-27), row-major."""
+
+    _fields_ = [("m", ctypes.c_float * 16)]
+
+
+class CorrParams(ctypes.Structure):
+    _fields_ = [("dist_threshold", ctypes.c_float), ("angle_threshold", ctypes.c_float),
+                ("view_threshold", ctypes.c_float), ("search_radius_px", ctypes.c_int)]
+
+
+class CorrFrameArgs(ctypes.Structure):
+    """cf_corr_frame: device pointers of one frame's inputs."""
+
+    _fields_ = [
+        ("live_vertices", ctypes.c_void_p),
+        ("live_normals", ctypes.c_void_p),
+        ("depth", ctypes.c_void_p),
+        ("depth_normals", ctypes.c_void_p),
+        ("pixel_knn", ctypes.c_void_p),
+        ("pixel_knn_w", ctypes.c_void_p),
+        ("hit_voxel_idx", ctypes.c_void_p),
+        ("voxel_knn", ctypes.c_void_p),
+        ("voxel_knn_w", ctypes.c_void_p),
+        ("num_voxels", ctypes.c_longlong),
+        ("pixel_knn_out", ctypes.c_void_p),
+        ("pixel_knn_w_out", ctypes.c_void_p),
     ]
 
 
@@ -198,6 +241,14 @@ def lib():
         L.cf_gn_profile_read.argtypes = [vp, vp, vp, i]
         L.cf_gn_profile_name.argtypes = [i]
         L.cf_gn_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+        L.cf_corr_search_create.argtypes = [i, i, ctypes.POINTER(vp)]
+        L.cf_corr_search_destroy.argtypes = [vp]
+        L.cf_find_correspondences.argtypes = [vp, ctypes.POINTER(CorrFrameArgs), ctypes.POINTER(Camera),
+                                              ctypes.POINTER(Mat4), ctypes.POINTER(Mat4), ctypes.POINTER(CorrParams),
+                                              vp, vp, vp, vp]
+        L.cf_compute_pixel_knn.argtypes = [vp, i, i, vp, vp, ctypes.c_longlong, vp, vp, vp]
+        L.cf_corr_search_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+        L.cf_corr_search_set_chunks.argtypes = [vp, i]
         L.cf_get_version.argtypes = [ctypes.POINTER(i)] * 3
         L.cf_last_cuda_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
         for name in EXPORTS:

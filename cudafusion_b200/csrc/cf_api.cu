@@ -1660,6 +1660,105 @@ cf_status cf_warp_skin_points(const float* d_points, const int* d_node_ids, cons
   return CF_OK;
 }
 
+struct cf_corr_search {
+  int max_w = 0, max_h = 0;
+  cf::CorrScratch sc = {};
+  int chunks = 0;  // row chunks per tile; 0 = chosen per frame
+  long long launches = 0;
+};
+
+namespace {
+void corr_free(cf_corr_search* h) {
+  cudaFree(h->sc.A);
+  cudaFree(h->sc.B);
+  cudaFree(h->sc.part_pd);
+  cudaFree(h->sc.part_idx);
+  cudaFree(h->sc.flag);
+}
+}  // namespace
+
+cf_status cf_corr_search_create(int max_width, int max_height, cf_corr_search** out) {
+  if (!out) return CF_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (max_width <= 0 || max_height <= 0) return CF_ERR_INVALID_ARG;
+  // per-pixel node lists are indexed with 32-bit pixel offsets times 4
+  if ((long long)max_width * max_height > (1LL << 29)) return CF_ERR_CAPACITY;
+  cf_corr_search* h = new cf_corr_search();
+  h->max_w = max_width;
+  h->max_h = max_height;
+  const size_t P = (size_t)max_width * max_height;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->sc.sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = dalloc(&h->sc.A, P);
+  if (e == cudaSuccess) e = dalloc(&h->sc.B, P);
+  if (e == cudaSuccess) e = dalloc(&h->sc.part_pd, P * kCorrMaxChunks);
+  if (e == cudaSuccess) e = dalloc(&h->sc.part_idx, P * kCorrMaxChunks);
+  if (e == cudaSuccess) e = dalloc(&h->sc.flag, 1);
+  if (e != cudaSuccess) {
+    corr_free(h);
+    delete h;
+    return from_cuda(e);
+  }
+  *out = h;
+  return CF_OK;
+}
+
+cf_status cf_corr_search_destroy(cf_corr_search* h) {
+  if (!h) return CF_OK;
+  corr_free(h);
+  delete h;
+  return CF_OK;
+}
+
+cf_status cf_corr_search_set_chunks(cf_corr_search* h, int chunks) {
+  if (!h || chunks < 0 || chunks > kCorrMaxChunks) return CF_ERR_INVALID_ARG;
+  h->chunks = chunks;
+  return CF_OK;
+}
+
+cf_status cf_find_correspondences(cf_corr_search* h, const cf_corr_frame* frame, const cf_camera* cam,
+                                  const cf_mat4* T_cam_world, const cf_mat4* T_world_cam, const cf_corr_params* params,
+                                  cf_correspondence* d_corrs, int* d_num_valid, int* d_stats, void* stream) {
+  if (!h || !frame || !cam || !T_cam_world || !T_world_cam || !params || !d_num_valid) return CF_ERR_INVALID_ARG;
+  if (cam->width < 0 || cam->height < 0) return CF_ERR_INVALID_ARG;
+  if (cam->width > h->max_w || cam->height > h->max_h) return CF_ERR_CAPACITY;
+  if ((long long)cam->width * cam->height > 0) {
+    if (!frame->d_live_vertices || !frame->d_live_normals || !frame->d_depth || !frame->d_depth_normals || !d_corrs)
+      return CF_ERR_INVALID_ARG;
+    if (frame->d_pixel_knn) {
+      if (!frame->d_pixel_knn_w) return CF_ERR_INVALID_ARG;
+    } else {
+      if (!frame->d_hit_voxel_idx || frame->num_voxels < 0) return CF_ERR_INVALID_ARG;
+      if (frame->num_voxels > 0 && (!frame->d_voxel_knn || !frame->d_voxel_knn_w)) return CF_ERR_INVALID_ARG;
+      if ((frame->d_pixel_knn_out == nullptr) != (frame->d_pixel_knn_w_out == nullptr)) return CF_ERR_INVALID_ARG;
+    }
+  }
+  CF_TRY(launch_corr_search(frame, cam, T_cam_world, T_world_cam, params, h->sc, h->chunks, d_corrs, d_num_valid,
+                            d_stats, (cudaStream_t)stream, &h->launches));
+  return CF_OK;
+}
+
+cf_status cf_compute_pixel_knn(const int* d_hit_voxel_idx, int width, int height, const int* d_voxel_knn,
+                               const float* d_voxel_knn_w, long long num_voxels, int* d_pixel_knn,
+                               float* d_pixel_knn_w, void* stream) {
+  if (width < 0 || height < 0 || num_voxels < 0) return CF_ERR_INVALID_ARG;
+  if ((long long)width * height > (1LL << 29)) return CF_ERR_CAPACITY;
+  const int P = width * height;
+  if (P == 0) return CF_OK;
+  if (!d_hit_voxel_idx || !d_pixel_knn || !d_pixel_knn_w) return CF_ERR_INVALID_ARG;
+  if (num_voxels > 0 && (!d_voxel_knn || !d_voxel_knn_w)) return CF_ERR_INVALID_ARG;
+  CF_TRY(launch_pixel_knn(d_hit_voxel_idx, P, d_voxel_knn, d_voxel_knn_w, num_voxels, d_pixel_knn, d_pixel_knn_w,
+                          (cudaStream_t)stream));
+  return CF_OK;
+}
+
+cf_status cf_corr_search_launch_count(const cf_corr_search* h, long long* launches) {
+  if (!h || !launches) return CF_ERR_INVALID_ARG;
+  *launches = h->launches;
+  return CF_OK;
+}
+
 cf_status cf_get_version(int* major, int* minor, int* patch) {
   if (major) *major = 0;
   if (minor) *minor = 1;

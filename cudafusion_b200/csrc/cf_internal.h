@@ -238,6 +238,22 @@ cudaError_t launch_residual_energy(const Work& w, const Pattern& p, const SolveA
 cudaError_t launch_final_energy(const Work& w, const Pattern& p, const SolveArgs& a, int slot, cudaStream_t s);
 cudaError_t launch_apply_twist(cf_dual_quat* T, const float* dx, int N, float max_rot, float max_trans,
                                float scale, cudaStream_t s);
+// cf_corr.cu: projective correspondence search
+constexpr int kCorrMaxChunks = 8;
+struct CorrScratch {
+  float4* A;       // per pixel: unprojected point (x, y, z) and normal x
+  float2* B;       // per pixel: normal y, z
+  float* part_pd;  // [kCorrMaxChunks][pixels]: each row chunk's best distance ...
+  int* part_idx;   // ... and candidate
+  int* flag;       // set when a value could make a distance NaN
+  int sms;
+};
+int corr_pick_chunks(int tiles, int sms, int radius, int W, int H);
+cudaError_t launch_corr_search(const cf_corr_frame* f, const cf_camera* cam, const cf_mat4* Tcw, const cf_mat4* Twc,
+                               const cf_corr_params* p, const CorrScratch& sc, int chunks, cf_correspondence* out,
+                               int* num_valid, int* stats, cudaStream_t s, long long* launches);
+cudaError_t launch_pixel_knn(const int* hit, int P, const int* vk, const float* vw, long long num_voxels, int* pk,
+                             float* pw, cudaStream_t s);
 cudaError_t launch_skin_points(const float* pts, const int* ids, const float* ws, int M,
                                const cf_deform_node* nodes, const cf_dual_quat* T, int N, float* out,
                                cudaStream_t s);

@@ -611,3 +611,187 @@ def cylinder_sequence(seed=5, num_nodes=2048, randomize=False, **kw):
         seed=seed,
         **params,
     )
+
+
+# --------------------------------------------------------------------------
+# projective correspondence search frames
+# --------------------------------------------------------------------------
+
+
+@dataclass
+class CorrFrame:
+    """The inputs of one projective correspondence search
+    (DynamicFusionPipeline::find_correspondences, include/fusion_app.h:1791-1845):
+    the raycast live surface, the observed depth with its normals, the camera
+    motion and the canonical voxel hit per pixel with the voxels' node lists.
+    Per-pixel arrays are row-major over height x width."""
+
+    width: int
+    height: int
+    cam: np.ndarray  # float32[4]: fx, fy, cx, cy
+    live_vertices: np.ndarray  # float32[H*W, 3], (0,0,0) where the ray missed
+    live_normals: np.ndarray  # float32[H*W, 3]
+    depth: np.ndarray  # float32[H*W], 0 = no depth
+    depth_normals: np.ndarray  # float32[H*W, 3], (0,0,0) = none
+    T_cam_world: np.ndarray  # float32[4, 4]
+    T_world_cam: np.ndarray  # float32[4, 4]
+    hit_voxel_idx: np.ndarray  # int32[H*W], -1 = none
+    voxel_knn: np.ndarray  # int32[V, 4]
+    voxel_knn_w: np.ndarray  # float32[V, 4]
+    pixel_knn: np.ndarray  # int32[H*W, 4]: the voxel lists gathered per pixel
+    pixel_knn_w: np.ndarray  # float32[H*W, 4]
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def num_pixels(self):
+        return self.width * self.height
+
+
+def _rotmat(q):
+    x, y, z, w = q
+    return np.array(
+        [
+            [1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+            [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+            [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)],
+        ]
+    )
+
+
+def _tube_normals(P, axis_pt, axis_dir):
+    q = P - axis_pt
+    radial = q - (q @ axis_dir)[:, None] * axis_dir
+    n = radial / np.maximum(np.linalg.norm(radial, axis=-1, keepdims=True), 1e-300)
+    # face the camera at the origin
+    return np.where((np.sum(n * P, -1) > 0)[:, None], -n, n)
+
+
+def corr_frame(
+    width=640,
+    height=480,
+    bend_deg=30.0,
+    est_bend_deg=27.0,
+    cam_rot_deg=0.6,
+    cam_trans=(0.003, -0.002, 0.002),
+    noise=0.001,
+    hole_frac=0.01,
+    voxel_size=0.004,
+    num_nodes=None,
+    seed=11,
+):
+    """Two-cylinder frame (radii 6 and 5 cm, the full-frame workload's
+    surface) for the correspondence search.  The live maps are the model
+    warped by the current estimate (joint bent by `est_bend_deg`) raycast from
+    the previous camera, which is the world frame; the depth is the surface at
+    `bend_deg` seen from the camera moved by `cam_rot_deg` about a random axis
+    and `cam_trans` metres (T_cam_world), with sigma=`noise` depth noise and a
+    `hole_frac` share of pixels without depth.  Depth normals are the
+    reference's forward differences flipped toward the camera
+    (kernels/tsdf_kernels.cu:180-230).  Each live pixel's canonical point (the
+    estimate's articulation undone) falls in a voxel of a `voxel_size` grid;
+    the voxels hit carry their 4 nearest nodes with weights
+    exp(-d^2 / (2 r^2)) normalised (src/warp_field.cu:379-404).  Intrinsics
+    scale with width from fx = fy = 570.342 at 640 x 480."""
+    rng = np.random.default_rng(seed)
+    s = width / 640.0
+    fx = fy = 570.342 * s
+    cx, cy = width / 2.0, height / 2.0
+    radii, lengths = (0.06, 0.05), (0.08, 0.09)
+    joint = np.array([0.0, 0.0, 0.14])
+    ex = np.array([1.0, 0.0, 0.0])
+    q_est = _rot_y(np.deg2rad(est_bend_deg))
+    q_true = _rot_y(np.deg2rad(bend_deg))
+
+    u, v = np.meshgrid(np.arange(width, dtype=np.float64), np.arange(height, dtype=np.float64))
+    dirs = np.stack([(u - cx) / fx, (v - cy) / fy, np.ones_like(u)], -1).reshape(-1, 3)
+
+    # live maps: the estimate raycast from the previous camera (= world)
+    w2 = _qrotate(q_est, ex)
+    t1, _ = _ray_tube(dirs, joint, ex, radii[0], -lengths[0], 0.0)
+    t2, _ = _ray_tube(dirs, joint, w2, radii[1], 0.0, lengths[1])
+    seg2 = t2 < t1
+    t = np.minimum(t1, t2)
+    hit = np.isfinite(t)
+    P = dirs * np.where(hit, t, 0.0)[:, None]
+    n1 = _tube_normals(P, joint, ex)
+    n2 = _tube_normals(P, joint, w2)
+    live_n = np.where(seg2[:, None], n2, n1) * hit[:, None]
+
+    # the observed frame: the true surface from the moved camera
+    axis = rng.normal(size=3)
+    axis /= np.linalg.norm(axis)
+    R = _rotmat(quat_from_rotvec(axis * np.deg2rad(cam_rot_deg)))
+    tc = np.asarray(cam_trans, np.float64)
+    T_cw = np.eye(4)
+    T_cw[:3, :3] = R
+    T_cw[:3, 3] = tc
+    T_wc = np.eye(4)
+    T_wc[:3, :3] = R.T
+    T_wc[:3, 3] = -R.T @ tc
+    jc = R @ joint + tc
+    t1c, _ = _ray_tube(dirs, jc, R @ ex, radii[0], -lengths[0], 0.0)
+    t2c, _ = _ray_tube(dirs, jc, R @ _qrotate(q_true, ex), radii[1], 0.0, lengths[1])
+    tcam = np.minimum(t1c, t2c)
+    dhit = np.isfinite(tcam)
+    depth = np.where(dhit, tcam + rng.normal(scale=noise, size=tcam.shape), 0.0)
+    depth[rng.random(depth.shape) < hole_frac] = 0.0
+    depth = depth.astype(np.float32)
+
+    # forward-difference depth normals (kernels/tsdf_kernels.cu:180-230)
+    D = depth.reshape(height, width).astype(np.float64)
+    Pc = dirs.reshape(height, width, 3) * D[..., None]
+    dn = np.zeros((height, width, 3))
+    dxv = Pc[:-1, 1:] - Pc[:-1, :-1]
+    dyv = Pc[1:, :-1] - Pc[:-1, :-1]
+    nn = np.cross(dxv, dyv)
+    nrm = np.linalg.norm(nn, axis=-1, keepdims=True)
+    nn = -np.where(nrm > 1e-9, nn / np.maximum(nrm, 1e-300), nn)
+    ok = (D[:-1, :-1] > 0) & (D[:-1, 1:] > 0) & (D[1:, :-1] > 0)
+    dn[:-1, :-1] = np.where(ok[..., None], nn, 0.0)
+
+    # canonical voxel per live pixel and the voxels' node lists
+    canon = P.copy()
+    if np.any(seg2 & hit):
+        m = seg2 & hit
+        canon[m] = joint + _qrotate(np.broadcast_to(_qconj(q_est), (int(m.sum()), 4)), P[m] - joint)
+    ch = canon[hit]
+    lo = ch.min(0) - 2 * voxel_size
+    dims = np.ceil((ch.max(0) - lo) / voxel_size).astype(np.int64) + 3
+    ijk = np.floor((canon - lo) / voxel_size).astype(np.int64)
+    vidx = (ijk[:, 2] * dims[1] + ijk[:, 1]) * dims[0] + ijk[:, 0]
+    hit_voxel = np.where(hit, vidx, -1).astype(np.int32)
+    V = int(np.prod(dims))
+    if num_nodes is None:
+        num_nodes = max(16, int(round(2048 * s * s)))
+    num_nodes = min(num_nodes, max(4, ch.shape[0] // 4))
+    sel, h = _blue_noise_subsample(ch, num_nodes, rng)
+    node_pos = ch[sel]
+    used = np.unique(hit_voxel[hit])
+    centers = lo + (np.stack([used % dims[0], (used // dims[0]) % dims[1], used // (dims[0] * dims[1])], -1) + 0.5) * voxel_size
+    ids, ws = _skin_weights(centers, node_pos, h)
+    voxel_knn = np.full((V, K_NEIGHBORS), -1, np.int32)
+    voxel_knn_w = np.zeros((V, K_NEIGHBORS), np.float32)
+    voxel_knn[used] = ids
+    voxel_knn_w[used] = ws
+    pk = np.where(hit[:, None], voxel_knn[np.maximum(hit_voxel, 0)], -1).astype(np.int32)
+    pw = np.where(hit[:, None], voxel_knn_w[np.maximum(hit_voxel, 0)], 0.0).astype(np.float32)
+
+    return CorrFrame(
+        width=width,
+        height=height,
+        cam=np.array([fx, fy, cx, cy], np.float32),
+        live_vertices=P.astype(np.float32),
+        live_normals=live_n.astype(np.float32),
+        depth=depth.reshape(-1),
+        depth_normals=dn.reshape(-1, 3).astype(np.float32),
+        T_cam_world=T_cw.astype(np.float32),
+        T_world_cam=T_wc.astype(np.float32),
+        hit_voxel_idx=hit_voxel,
+        voxel_knn=voxel_knn,
+        voxel_knn_w=voxel_knn_w,
+        pixel_knn=pk,
+        pixel_knn_w=pw,
+        meta=dict(kind="cylinders-corr", seed=seed, width=width, height=height, live_coverage=float(hit.mean()),
+                  depth_coverage=float((depth > 0).mean()), num_voxels=V, num_nodes=int(node_pos.shape[0]),
+                  bend_deg=bend_deg, est_bend_deg=est_bend_deg),
+    )

@@ -408,6 +408,97 @@ CF_API cf_status cf_warp_skin_points(const float* d_points, const int* d_node_id
                               const cf_dual_quat* d_transforms, int num_nodes,
                               float* d_out, void* stream);
 
+/* ------------------------------------------------------------------------ */
+/* Projective correspondence search: the producer of the solve's input.     */
+/* DynamicFusionPipeline::find_correspondences, include/fusion_app.h:1791-1845:*/
+/* compute_pixel_knn_kernel (kernels/tsdf_kernels.cu:573-604) followed by    */
+/* find_correspondences_kernel (kernels/tsdf_kernels.cu:386-563).           */
+/* ------------------------------------------------------------------------ */
+
+/* CameraIntrinsics, include/types.h:148-162: project(p) = (fx x/z + cx,
+ * fy y/z + cy), unproject(u, v, z) = (z (u-cx)/fx, z (v-cy)/fy, z). */
+typedef struct cf_camera {
+  float fx, fy, cx, cy;
+  int width, height;
+} cf_camera;
+
+/* Mat4, include/types.h:26-60: row-major rigid transform, p' = M[0:3,0:3] p
+ * + M[0:3,3]. */
+typedef struct cf_mat4 {
+  float m[4][4];
+} cf_mat4;
+
+/* The search thresholds of the reference's pipeline parameters
+ * (config/params.yaml:60-63; the stock values are 0.2, 0.0, 0.0, 50). */
+typedef struct cf_corr_params {
+  float dist_threshold;  /* a pair needs |n_dst . (v_live - v_dst)| < this (m) */
+  float angle_threshold; /* and |n_live . n_dst| >= this */
+  float view_threshold;  /* a live pixel needs |n_live . view ray| >= this */
+  int search_radius_px;  /* (2r+1)^2 window around the projection; < 0 acts as 0 */
+} cf_corr_params;
+
+/* One frame's inputs, all device arrays of width*height pixels in row-major
+ * order, owned by the caller.  The node ids/weights of a pixel come either
+ * from d_pixel_knn/d_pixel_knn_w (what find_correspondences_kernel reads) or,
+ * when d_pixel_knn is NULL, from the canonical voxel the pixel's ray hit
+ * (compute_pixel_knn_kernel fused into the search). */
+typedef struct cf_corr_frame {
+  const float* d_live_vertices; /* float3 [H*W]: raycast live surface (world); |v| < 1e-6 = none */
+  const float* d_live_normals;  /* float3 [H*W]; |n| < 1e-6 = none */
+  const float* d_depth;         /* float [H*W]: observed depth (m); <= 0 = none */
+  const float* d_depth_normals; /* float3 [H*W] (camera frame); |n| < 1e-6 = none */
+  const int* d_pixel_knn;       /* int [H*W][CF_K_NEIGHBORS] or NULL */
+  const float* d_pixel_knn_w;   /* float [H*W][CF_K_NEIGHBORS] */
+  const int* d_hit_voxel_idx;   /* int [H*W]: canonical voxel hit per pixel, < 0 = none */
+  const int* d_voxel_knn;       /* int [num_voxels][CF_K_NEIGHBORS] */
+  const float* d_voxel_knn_w;   /* float [num_voxels][CF_K_NEIGHBORS] */
+  long long num_voxels;         /* voxel indices >= this count as none */
+  int* d_pixel_knn_out;         /* optional (voxel path): the gathered per-pixel ids ... */
+  float* d_pixel_knn_w_out;     /* ... and weights, as compute_pixel_knn_kernel writes them */
+} cf_corr_frame;
+
+/* Opaque search handle: owns the per-pixel candidate records and the row
+ * chunks' partial results (88 B per pixel of the largest frame). */
+typedef struct cf_corr_search cf_corr_search;
+CF_API cf_status cf_corr_search_create(int max_width, int max_height, cf_corr_search** out);
+CF_API cf_status cf_corr_search_destroy(cf_corr_search* h);
+
+/* find_correspondences_kernel over every pixel of a cam->width x
+ * cam->height frame: project the live vertex with T_cam_world, search the
+ * (2r+1)^2 depth pixels around the projection in row-major order and keep
+ * the first candidate of least point-to-plane distance among those within
+ * max(3 d, d + 0.03) m (d = dist_threshold) whose normal agrees; the pair is
+ * (src = live vertex, dst / normal = the candidate mapped by T_world_cam,
+ * weight = the reference's squared mean of distance, normal and view
+ * confidences, node ids/weights of the pixel).  Writes all H*W records
+ * (invalid ones: valid = 0, weight = 0, ids = -1, other fields 0), the valid
+ * count to *d_num_valid and, when d_stats is not NULL, the reference's six
+ * debug counters (invalid_live, out_proj, no_depth, far, angle, valid) to
+ * d_stats[0..5]; both are overwritten, not accumulated.  FP32 with fused
+ * multiply-add accumulation and IEEE division and square roots (the
+ * reference's build uses approximate ones: results agree to rounding, and a
+ * candidate choice can differ where two candidates tie to a few ulps).
+ * Asynchronous on `stream`. */
+CF_API cf_status cf_find_correspondences(cf_corr_search* h, const cf_corr_frame* frame, const cf_camera* cam,
+                                         const cf_mat4* T_cam_world, const cf_mat4* T_world_cam,
+                                         const cf_corr_params* params, cf_correspondence* d_corrs,
+                                         int* d_num_valid, int* d_stats, void* stream);
+
+/* compute_pixel_knn_kernel, kernels/tsdf_kernels.cu:573-604: per pixel the
+ * CF_K_NEIGHBORS node ids/weights of its hit voxel, (-1, 0) where none. */
+CF_API cf_status cf_compute_pixel_knn(const int* d_hit_voxel_idx, int width, int height, const int* d_voxel_knn,
+                                      const float* d_voxel_knn_w, long long num_voxels, int* d_pixel_knn,
+                                      float* d_pixel_knn_w, void* stream);
+
+/* Kernel launches made through the handle since its creation. */
+CF_API cf_status cf_corr_search_launch_count(const cf_corr_search* h, long long* launches);
+
+/* Tuning knob (no reference counterpart): the search splits the rows each
+ * 32 x 8 tile of pixels scans into `chunks` parts run by separate CTAs
+ * (1..8; 0, the default, picks the count per frame from the tile count and
+ * the SM count).  Results do not depend on it. */
+CF_API cf_status cf_corr_search_set_chunks(cf_corr_search* h, int chunks);
+
 /* Library / device information. */
 CF_API cf_status cf_get_version(int* major, int* minor, int* patch);
 CF_API cf_status cf_last_cuda_error(char* buf, size_t len);

@@ -200,3 +200,52 @@ def energy(problem, transforms, lambda_smooth, precision="f64", nthreads=1):
     f.restype = ctypes.c_double
     return f(_p(canon), _p(corrs), corrs.shape[0], _p(nodes), _p(T), nodes.shape[0], ctypes.c_float(lambda_smooth),
              nthreads)
+
+
+# ---- projective correspondence search (oracle/cf_oracle_corr.c) ----
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+def find_correspondences(frame, dist_threshold, angle_threshold, view_threshold, search_radius_px, pixels=None,
+                         pixel_knn=None, pixel_knn_w=None):
+    """find_correspondences_kernel (kernels/tsdf_kernels.cu:386-563) over all
+    pixels of `frame` (a synth.CorrFrame) or over `pixels` (int array).
+    Returns (records CORR_DTYPE[n], valid count, debug counters int[6])."""
+    L = lib()
+    f = L.cfo_find_correspondences
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 5 + \
+        [ctypes.c_float] * 3 + [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    lv, ln = _f32(frame.live_vertices), _f32(frame.live_normals)
+    d, dn = _f32(frame.depth), _f32(frame.depth_normals)
+    cam, cw, wc = _f32(frame.cam), _f32(frame.T_cam_world), _f32(frame.T_world_cam)
+    pk = np.ascontiguousarray(frame.pixel_knn if pixel_knn is None else pixel_knn, np.int32)
+    pw = _f32(frame.pixel_knn_w if pixel_knn_w is None else pixel_knn_w)
+    pix = None if pixels is None else np.ascontiguousarray(pixels, np.int32)
+    n = frame.width * frame.height if pix is None else pix.shape[0]
+    out = np.zeros(n, CORR_DTYPE)
+    stats = np.zeros(6, np.int32)
+    nv = f(_p(lv), _p(ln), _p(d), _p(dn), frame.width, frame.height, _p(cam), _p(cw), _p(wc), _p(pk), _p(pw),
+           dist_threshold, angle_threshold, view_threshold, int(search_radius_px), _p(pix), int(n), _p(out),
+           _p(stats))
+    return out, int(nv), stats
+
+
+def compute_pixel_knn(hit_voxel_idx, voxel_knn, voxel_knn_w):
+    """compute_pixel_knn_kernel (kernels/tsdf_kernels.cu:573-604)."""
+    L = lib()
+    f = L.cfo_compute_pixel_knn
+    f.restype = None
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong,
+                  ctypes.c_void_p, ctypes.c_void_p]
+    hit = np.ascontiguousarray(hit_voxel_idx, np.int32)
+    vk = np.ascontiguousarray(voxel_knn, np.int32)
+    vw = _f32(voxel_knn_w)
+    P = hit.shape[0]
+    pk = np.zeros((P, 4), np.int32)
+    pw = np.zeros((P, 4), np.float32)
+    f(_p(hit), P, _p(vk), _p(vw), vk.shape[0], _p(pk), _p(pw))
+    return pk, pw
