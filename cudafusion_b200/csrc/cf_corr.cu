@@ -23,21 +23,27 @@
 //
 // Launches per frame:
 //  corr_prep_kernel    per depth pixel one 24-byte candidate record: the
-//                      unprojected point and the normal, with the two skip
-//                      cases folded into z (0: no depth; -1: no normal).  The
-//                      reference recomputes the unprojection, two divisions,
-//                      for every (pixel, candidate) pair.
-//  corr_search_kernel  one thread per live pixel, 32 x 8 pixels per CTA, and
+//                      unprojected point and the normal.  The two skip cases
+//                      are folded into z (0: no depth; -1: no normal) with x, y
+//                      and the normal's x so large that the record's
+//                      point-to-plane distance is +inf.
+//                      The reference recomputes the unprojection, two
+//                      divisions, for every (pixel, candidate) pair.
+//  corr_search_kernel  one thread per two vertically adjacent live pixels (one
+//                      shared-memory load serves both windows; each pixel still
+//                      meets its candidates in row-major order), 32 x 16 pixels
+//                      per CTA, and
 //                      blockIdx.z = one of C chunks of the rows that the CTA's
 //                      windows cover (C from a cost model of the waves of
 //                      tiles x C CTAs over the resident slots).  The CTA stages
 //                      its chunk in shared memory one band of rows at a time;
 //                      each thread scans its window's rows in the chunk in
 //                      row-major order with the reference's acceptance rule,
-//                      branch-free.  The Euclidean test compares the squared
-//                      distance with the largest float whose IEEE square root
-//                      is within the cap (exact: the rounded square root is
-//                      monotonic).  With one chunk the kernel writes the
+//                      branch-free.  The Euclidean test compares the
+//                      squared distance with the largest float whose IEEE
+//                      square root is within the cap (exact: the rounded
+//                      square root is monotonic), and is left out for a band
+//                      whose bounding box of real points lies within the cap.  With one chunk the kernel writes the
 //                      records itself; otherwise each (chunk, pixel) leaves its
 //                      best distance and candidate for
 //  corr_merge_kernel   which takes the chunks in row order with the same
@@ -61,11 +67,13 @@ namespace {
 
 constexpr int kCsTx = 32;
 constexpr int kCsTy = 8;
+constexpr int kCsPy = 2 * kCsTy;  // pixel rows per tile: each thread scans two
 constexpr int kCsThreads = kCsTx * kCsTy;
 constexpr int kCsSmem = 55 * 1024;  // one band of records; 4 CTAs per SM with the 1 KB reserve each
 constexpr int kCsCtasPerSm = 4;
 constexpr int kCsRecBytes = (int)(sizeof(float4) + sizeof(float2));
 constexpr float kCsBig = 1e18f;  // squares and three-term sums of such values stay finite in FP32
+constexpr float kCsFar = 1e30f;  // x, y and normal x of a skip record: its distance overflows to +inf
 
 struct CorrConsts {
   float fx, fy, cx, cy;
@@ -117,7 +125,7 @@ __global__ void corr_prep_kernel(const float* __restrict__ depth, const float* _
   if (i >= W * H) return;
   const int y = i / W, x = i - y * W;
   const float d = depth[i];
-  float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 a = make_float4(kCsFar, kCsFar, 0.f, kCsFar);
   float2 b = make_float2(0.f, 0.f);
   if (!(d <= 0.f)) {
     const float nx = dn[3 * i], ny = dn[3 * i + 1], nz = dn[3 * i + 2];
@@ -188,25 +196,116 @@ __device__ __forceinline__ CsPixel cs_pixel(const CorrConsts& k, const float* __
   return p;
 }
 
-// One row segment of a window: ra/rb point at the row's records indexed by
-// image column.  Branch-free form of the acceptance rule for finite values.
-template <bool kAngle>
-__device__ __forceinline__ void cs_row(const float4* ra, const float2* rb, int x0, int x1, int row_base,
-                                       const CsPixel& p, const CorrConsts& k, float& best, int& best_i) {
+// The scan state of one pixel: its projection, camera-frame point and normal,
+// and the best candidate so far.
+struct CsScan {
+  int pu, pv;
+  float vx, vy, vz, nx, ny, nz;
+  float best;
+  int bi;
+  bool on;  // the pixel is scanned here
+};
+
+__device__ __forceinline__ CsScan cs_scan_state(const CsPixel& p, bool on, float dist_thr) {
+  CsScan q;
+  q.pu = p.pu;
+  q.pv = p.pv;
+  q.vx = p.vc.x;
+  q.vy = p.vc.y;
+  q.vz = p.vc.z;
+  q.nx = p.nc.x;
+  q.ny = p.nc.y;
+  q.nz = p.nc.z;
+  q.best = dist_thr;
+  q.bi = -1;
+  q.on = on;
+  return q;
+}
+
+// A candidate's point-to-plane distance, +inf where the reference would skip
+// it (finite values only).  A skip record's far-away point and huge normal
+// make its distance +inf by themselves.  kCheckS: apply the Euclidean cap
+// (left out where the band's bounding box proves every record within it);
+// kAngle: apply the angle threshold.
+template <bool kAngle, bool kCheckS>
+__device__ __forceinline__ float cs_pd(const CsScan& q, const float4& a, const float2& b, const CorrConsts& k) {
+  const float ex = __fsub_rn(q.vx, a.x), ey = __fsub_rn(q.vy, a.y), ez = __fsub_rn(q.vz, a.z);
+  float pd = fabsf(cs_dot(a.w, b.x, b.y, ex, ey, ez));
+  if (kCheckS) pd = cs_dot(ex, ey, ez, ex, ey, ez) <= k.s_max ? pd : INFINITY;
+  if (kAngle) pd = fabsf(cs_dot(q.nx, q.ny, q.nz, a.w, b.x, b.y)) < k.angle_thr ? INFINITY : pd;
+  return pd;
+}
+
+// The acceptance rule over columns lo..hi of one row, for one pixel or for
+// two at one load each.  best starts at the distance bound and only falls,
+// so pd < best also keeps pd below the bound.
+template <bool kAngle, bool kCheckS>
+__device__ __forceinline__ void cs_eval(CsScan& q, const float4& a, const float2& b, int idx, const CorrConsts& k) {
+  const float pd = cs_pd<kAngle, kCheckS>(q, a, b, k);
+  const bool acc = pd < q.best;
+  q.best = acc ? pd : q.best;
+  q.bi = acc ? idx : q.bi;
+}
+template <bool kAngle, bool kCheckS>
+__device__ __forceinline__ void cs_seg1(const float4* ra, const float2* rb, int lo, int hi, int row_base, CsScan& q,
+                                        const CorrConsts& k) {
 #pragma unroll 4
-  for (int xx = x0; xx <= x1; ++xx) {
+  for (int xx = lo; xx <= hi; ++xx) cs_eval<kAngle, kCheckS>(q, ra[xx], rb[xx], row_base + xx, k);
+}
+template <bool kAngle, bool kCheckS>
+__device__ __forceinline__ void cs_seg2(const float4* ra, const float2* rb, int lo, int hi, int row_base, CsScan& q0,
+                                        CsScan& q1, const CorrConsts& k) {
+#pragma unroll 2
+  for (int xx = lo; xx <= hi; ++xx) {
     const float4 a = ra[xx];
     const float2 b = rb[xx];
-    const float ex = __fsub_rn(p.vc.x, a.x), ey = __fsub_rn(p.vc.y, a.y), ez = __fsub_rn(p.vc.z, a.z);
-    const float s = cs_dot(ex, ey, ez, ex, ey, ez);
-    const float pd = fabsf(cs_dot(a.w, b.x, b.y, ex, ey, ez));
-    // best starts at the distance bound and only falls, so pd < best also
-    // keeps pd below the bound
-    bool acc = (a.z > 0.f) & (s <= k.s_max) & (pd < best);
-    if (kAngle) acc = acc & !(fabsf(cs_dot(p.nc.x, p.nc.y, p.nc.z, a.w, b.x, b.y)) < k.angle_thr);
-    best = acc ? pd : best;
-    best_i = acc ? row_base + xx : best_i;
+    cs_eval<kAngle, kCheckS>(q0, a, b, row_base + xx, k);
+    cs_eval<kAngle, kCheckS>(q1, a, b, row_base + xx, k);
   }
+}
+
+// Row yy of the two pixels' windows (ra/rb: the row's records indexed by
+// image column).  Each pixel still meets its candidates in increasing column
+// order: the row splits into the part only one window covers on the left,
+// the shared part, and the part only one covers on the right.
+template <bool kAngle, bool kCheckS>
+__device__ __forceinline__ void cs_pair_row(const float4* ra, const float2* rb, int yy, CsScan& q0, CsScan& q1,
+                                            const CorrConsts& k) {
+  const int r = k.radius, row_base = yy * k.W;
+  const bool in0 = q0.on && yy >= q0.pv - r && yy <= q0.pv + r;
+  const bool in1 = q1.on && yy >= q1.pv - r && yy <= q1.pv + r;
+  const int l0 = max(0, q0.pu - r), h0 = min(k.W - 1, q0.pu + r);
+  const int l1 = max(0, q1.pu - r), h1 = min(k.W - 1, q1.pu + r);
+  if (in0 && in1) {
+    const int slo = max(l0, l1), shi = min(h0, h1);
+    if (slo <= shi) {
+      if (l0 < slo) cs_seg1<kAngle, kCheckS>(ra, rb, l0, slo - 1, row_base, q0, k);
+      else if (l1 < slo) cs_seg1<kAngle, kCheckS>(ra, rb, l1, slo - 1, row_base, q1, k);
+      cs_seg2<kAngle, kCheckS>(ra, rb, slo, shi, row_base, q0, q1, k);
+      if (h0 > shi) cs_seg1<kAngle, kCheckS>(ra, rb, shi + 1, h0, row_base, q0, k);
+      else if (h1 > shi) cs_seg1<kAngle, kCheckS>(ra, rb, shi + 1, h1, row_base, q1, k);
+    } else {
+      cs_seg1<kAngle, kCheckS>(ra, rb, l0, h0, row_base, q0, k);
+      cs_seg1<kAngle, kCheckS>(ra, rb, l1, h1, row_base, q1, k);
+    }
+  } else if (in0) {
+    cs_seg1<kAngle, kCheckS>(ra, rb, l0, h0, row_base, q0, k);
+  } else if (in1) {
+    cs_seg1<kAngle, kCheckS>(ra, rb, l1, h1, row_base, q1, k);
+  }
+}
+
+// Whether every record of a band whose real points lie in the box lo..hi is
+// within the Euclidean cap of the pixel's point: the box's farthest corner,
+// with a relative margin of 1e-4 over the few-ulp rounding of the squared
+// distances, is below the bound.
+__device__ __forceinline__ bool cs_within_cap(const CsScan& q, const float* lo, const float* hi, float s_max) {
+  if (!q.on) return true;
+  if (lo[0] > hi[0]) return true;  // no real record in the band
+  const float dx = fmaxf(fabsf(q.vx - lo[0]), fabsf(q.vx - hi[0]));
+  const float dy = fmaxf(fabsf(q.vy - lo[1]), fabsf(q.vy - hi[1]));
+  const float dz = fmaxf(fabsf(q.vz - lo[2]), fabsf(q.vz - hi[2]));
+  return (dx * dx + dy * dy + dz * dz) * 1.0001f <= s_max;
 }
 
 // find_correspondences_kernel's loop as it stands (kernels/tsdf_kernels.cu:470-524),
@@ -337,6 +436,7 @@ __device__ __forceinline__ void cs_emit(const CorrConsts& k, const CsPixel& p, b
   }
 }
 
+// One thread per vertically adjacent pixel pair, 32 x 16 pixels per CTA.
 // kDirect: one chunk covers every row, and the kernel resolves each pixel and
 // writes its record itself (no partials, no merge launch).
 template <bool kAngle, bool kDirect>
@@ -347,11 +447,13 @@ __global__ void __launch_bounds__(kCsThreads, kCsCtasPerSm)
                        cf_correspondence* __restrict__ out, int* __restrict__ num_valid, int* __restrict__ stats) {
   extern __shared__ float4 cs_smem[];
   __shared__ int s_box[4];  // min pu, max pu, min pv, max pv of the pixels scanned here
+  __shared__ float s_bb[kCsThreads / 32][6];  // per warp: the band's real-point box (min xyz, max xyz)
   const int tid = threadIdx.y * kCsTx + threadIdx.x;
-  const int x = blockIdx.x * kCsTx + threadIdx.x, y = blockIdx.y * kCsTy + threadIdx.y;
+  const int x = blockIdx.x * kCsTx + threadIdx.x;
+  const int y0 = blockIdx.y * kCsPy + 2 * threadIdx.y, y1 = y0 + 1;
   const int chunk = blockIdx.z;
-  const bool inimg = x < k.W && y < k.H;
-  const int px = inimg ? y * k.W + x : 0;
+  const bool img0 = x < k.W && y0 < k.H, img1 = x < k.W && y1 < k.H;
+  const int px0 = img0 ? y0 * k.W + x : 0, px1 = img1 ? y1 * k.W + x : 0;
   if (tid == 0) {
     s_box[0] = INT_MAX;
     s_box[1] = INT_MIN;
@@ -359,23 +461,36 @@ __global__ void __launch_bounds__(kCsThreads, kCsCtasPerSm)
     s_box[3] = INT_MIN;
   }
   const int frame_flag = *flag;
-  CsPixel p;
-  p.search = false;
-  p.code = -1;
-  p.pu = p.pv = 0;
-  if (inimg) p = cs_pixel(k, lv, ln, px, frame_flag);
-  const bool fast = inimg && p.search && !p.special;
+  CsScan q0, q1;
+  {
+    CsPixel p;
+    p.search = false;
+    p.special = false;
+    p.pu = p.pv = 0;
+    p.vc = p.nc = make_float3(0.f, 0.f, 0.f);
+    if (img0) p = cs_pixel(k, lv, ln, px0, frame_flag);
+    q0 = cs_scan_state(p, img0 && p.search && !p.special, k.dist_thr);
+    p.search = false;
+    p.special = false;
+    p.pu = p.pv = 0;
+    if (img1) p = cs_pixel(k, lv, ln, px1, frame_flag);
+    q1 = cs_scan_state(p, img1 && p.search && !p.special, k.dist_thr);
+  }
   __syncthreads();
-  if (fast) {
-    atomicMin(&s_box[0], p.pu);
-    atomicMax(&s_box[1], p.pu);
-    atomicMin(&s_box[2], p.pv);
-    atomicMax(&s_box[3], p.pv);
+  if (q0.on) {
+    atomicMin(&s_box[0], q0.pu);
+    atomicMax(&s_box[1], q0.pu);
+    atomicMin(&s_box[2], q0.pv);
+    atomicMax(&s_box[3], q0.pv);
+  }
+  if (q1.on) {
+    atomicMin(&s_box[0], q1.pu);
+    atomicMax(&s_box[1], q1.pu);
+    atomicMin(&s_box[2], q1.pv);
+    atomicMax(&s_box[3], q1.pv);
   }
   __syncthreads();
 
-  float best = k.dist_thr;
-  int best_i = -1;
   if (s_box[0] <= s_box[1]) {  // uniform over the CTA
     const int r = k.radius;
     const int xlo = max(0, s_box[0] - r), xhi = min(k.W - 1, s_box[1] + r);
@@ -384,51 +499,107 @@ __global__ void __launch_bounds__(kCsThreads, kCsCtasPerSm)
     const int c0 = ylo + chunk * per, c1 = min(yhi, c0 + per - 1);
     const int wu = xhi - xlo + 1;
     const int band = kCsSmem / (kCsRecBytes * wu);
-    const int x0 = max(0, p.pu - r), x1 = min(k.W - 1, p.pu + r);
+    // rows either pixel's window covers
+    const int plo = min(q0.on ? q0.pv : INT_MAX, q1.on ? q1.pv : INT_MAX) - r;
+    const int phi = max(q0.on ? q0.pv : INT_MIN, q1.on ? q1.pv : INT_MIN) + r;
+    const bool any = q0.on || q1.on;
     if (c0 <= c1 && band >= 1) {
       float4* sA = cs_smem;
       float2* sB = reinterpret_cast<float2*>(cs_smem + (size_t)band * wu);
       for (int yb = c0; yb <= c1; yb += band) {
         const int rows = min(band, c1 - yb + 1);
+        // the band's records, and the bounding box of their real points
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
         for (int j = tid; j < rows * wu; j += kCsThreads) {
           const int rr = j / wu;
           const int g = (yb + rr) * k.W + xlo + (j - rr * wu);
-          sA[j] = A[g];
+          const float4 a = A[g];
+          sA[j] = a;
           sB[j] = B[g];
+          if (a.z > 0.f) {
+            lo[0] = fminf(lo[0], a.x);
+            lo[1] = fminf(lo[1], a.y);
+            lo[2] = fminf(lo[2], a.z);
+            hi[0] = fmaxf(hi[0], a.x);
+            hi[1] = fmaxf(hi[1], a.y);
+            hi[2] = fmaxf(hi[2], a.z);
+          }
         }
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          for (int o = 16; o; o >>= 1) {
+            lo[c] = fminf(lo[c], __shfl_xor_sync(0xffffffffu, lo[c], o));
+            hi[c] = fmaxf(hi[c], __shfl_xor_sync(0xffffffffu, hi[c], o));
+          }
+        if ((tid & 31) == 0)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            s_bb[tid >> 5][c] = lo[c];
+            s_bb[tid >> 5][3 + c] = hi[c];
+          }
         __syncthreads();
-        if (fast) {
-          const int y0 = max(yb, p.pv - r), y1 = min(yb + rows - 1, p.pv + r);
-          for (int yy = y0; yy <= y1; ++yy) {
-            const int o = (yy - yb) * wu - xlo;
-            cs_row<kAngle>(sA + o, sB + o, x0, x1, yy * k.W, p, k, best, best_i);
+        if (any) {
+#pragma unroll
+          for (int w = 0; w < kCsThreads / 32; ++w)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              lo[c] = fminf(lo[c], s_bb[w][c]);
+              hi[c] = fmaxf(hi[c], s_bb[w][3 + c]);
+            }
+          const int ya = max(yb, plo), yz = min(yb + rows - 1, phi);
+          if (cs_within_cap(q0, lo, hi, k.s_max) && cs_within_cap(q1, lo, hi, k.s_max)) {
+            for (int yy = ya; yy <= yz; ++yy) {
+              const int o = (yy - yb) * wu - xlo;
+              cs_pair_row<kAngle, false>(sA + o, sB + o, yy, q0, q1, k);
+            }
+          } else {
+            for (int yy = ya; yy <= yz; ++yy) {
+              const int o = (yy - yb) * wu - xlo;
+              cs_pair_row<kAngle, true>(sA + o, sB + o, yy, q0, q1, k);
+            }
           }
         }
         __syncthreads();
       }
-    } else if (c0 <= c1 && fast) {  // the union is wider than a band buffer row: read through L1
-      const int y0 = max(c0, p.pv - r), y1 = min(c1, p.pv + r);
-      for (int yy = y0; yy <= y1; ++yy)
-        cs_row<kAngle>(A + (size_t)yy * k.W, B + (size_t)yy * k.W, x0, x1, yy * k.W, p, k, best, best_i);
+    } else if (c0 <= c1 && any) {  // the union is wider than a band buffer row: read through L1
+      const int ya = max(c0, plo), yz = min(c1, phi);
+      for (int yy = ya; yy <= yz; ++yy)
+        cs_pair_row<kAngle, true>(A + (size_t)yy * k.W, B + (size_t)yy * k.W, yy, q0, q1, k);
     }
   }
   if (kDirect) {
-    int code = p.code;
-    int bi = -1;
-    if (p.search) {
-      bool saw_depth = false;
-      if (p.special) {
-        bi = cs_rescan(k, p, A, B, saw_depth);
-      } else {
-        bi = best_i;
-        if (bi < 0 && stats) saw_depth = cs_any_depth(k, p, A);
+#pragma unroll 1
+    for (int h = 0; h < 2; ++h) {
+      const bool img = h == 0 ? img0 : img1;
+      const int px = h == 0 ? px0 : px1;
+      const int best_i = h == 0 ? q0.bi : q1.bi;
+      CsPixel p;
+      p.search = false;
+      p.code = -1;
+      if (img) p = cs_pixel(k, lv, ln, px, frame_flag);
+      int code = p.code;
+      int bi = -1;
+      if (p.search) {
+        bool saw_depth = false;
+        if (p.special) {
+          bi = cs_rescan(k, p, A, B, saw_depth);
+        } else {
+          bi = best_i;
+          if (bi < 0 && stats) saw_depth = cs_any_depth(k, p, A);
+        }
+        code = bi >= 0 ? 5 : (saw_depth ? 3 : 2);
       }
-      code = bi >= 0 ? 5 : (saw_depth ? 3 : 2);
+      cs_emit(k, p, img, px, bi, code, A, B, knn, out, num_valid, stats, threadIdx.x);
     }
-    cs_emit(k, p, inimg, px, bi, code, A, B, knn, out, num_valid, stats, threadIdx.x);
-  } else if (inimg) {
-    part_pd[(size_t)chunk * k.P + px] = best;
-    part_idx[(size_t)chunk * k.P + px] = best_i;
+  } else {
+    if (img0) {
+      part_pd[(size_t)chunk * k.P + px0] = q0.best;
+      part_idx[(size_t)chunk * k.P + px0] = q0.bi;
+    }
+    if (img1) {
+      part_pd[(size_t)chunk * k.P + px1] = q1.best;
+      part_idx[(size_t)chunk * k.P + px1] = q1.bi;
+    }
   }
 }
 
@@ -499,15 +670,15 @@ float sqrt_bound(float cap) {
 
 }  // namespace
 
-// Row chunks per tile.  Rough model in SM clocks: a CTA scans 256 pixels x
-// S/C candidates at about 1.25 candidates per clock (5 per SM, 4 CTAs) after
+// Row chunks per tile.  Rough model in SM clocks: a CTA scans 512 pixels x
+// S/C candidates at about 1.9 candidates per clock (7.5 per SM, 4 CTAs) after
 // a fixed ~3000-clock set-up, the CTAs run in ceil(tiles x C / slots) waves,
 // and more than one chunk adds the merge launch (~20000 clocks).  One chunk
 // writes the records from the search kernel itself.
 int corr_pick_chunks(int tiles, int sms, int radius, int W, int H) {
   const double slots = (double)(sms > 0 ? sms : 1) * kCsCtasPerSm;
   const double side_x = std::fmin(2.0 * radius + 1.0, (double)W), side_y = std::fmin(2.0 * radius + 1.0, (double)H);
-  const double scan = 256.0 * side_x * side_y / 1.25;
+  const double scan = 512.0 * side_x * side_y / 1.9;
   int best_c = 1;
   double best = 1e300;
   for (int c = 1; c <= kCorrMaxChunks; ++c) {
@@ -569,12 +740,13 @@ cudaError_t launch_corr_search(const cf_corr_frame* f, const cf_camera* cam, con
     if (e != cudaSuccess) return e;
   }
   if (W == 0 || H == 0) return cudaSuccess;
-  // a NaN bound defeats the strict-less merge (the reference then accepts every
-  // candidate it reaches): such a call takes the sequential scan throughout
-  e = cudaMemsetAsync(sc.flag, std::isnan(p->dist_threshold) ? 1 : 0, sizeof(int), s);
+  // a NaN bound defeats the strict-less rule (the reference then accepts every
+  // candidate it reaches) and an infinite one lets a skip record pass the
+  // Euclidean test: such calls take the sequential scan throughout
+  e = cudaMemsetAsync(sc.flag, std::isfinite(p->dist_threshold) ? 0 : 1, sizeof(int), s);
   if (e != cudaSuccess) return e;
 
-  const dim3 tiles((W + kCsTx - 1) / kCsTx, (H + kCsTy - 1) / kCsTy);
+  const dim3 tiles((W + kCsTx - 1) / kCsTx, (H + kCsPy - 1) / kCsPy);
   // the partials hold kCorrMaxChunks entries per pixel of the largest frame
   k.chunks = chunks > 0 ? (chunks > kCorrMaxChunks ? kCorrMaxChunks : chunks)
                         : corr_pick_chunks((int)(tiles.x * tiles.y), sc.sms, k.radius, W, H);
