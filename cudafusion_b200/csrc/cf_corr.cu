@@ -39,7 +39,10 @@
 //                      its chunk in shared memory one band of rows at a time;
 //                      each thread scans its window's rows in the chunk in
 //                      row-major order with the reference's acceptance rule,
-//                      branch-free.  The Euclidean test compares the
+//                      applied to groups of 4 consecutive candidates (one min
+//                      per candidate, one compare per group, the group's first
+//                      column found again at the end).  The Euclidean test
+//                      compares the
 //                      squared distance with the largest float whose IEEE
 //                      square root is within the cap (exact: the rounded
 //                      square root is monotonic), and is left out for a band
@@ -237,31 +240,70 @@ __device__ __forceinline__ float cs_pd(const CsScan& q, const float4& a, const f
 }
 
 // The acceptance rule over columns lo..hi of one row, for one pixel or for
-// two at one load each.  best starts at the distance bound and only falls,
-// so pd < best also keeps pd below the bound.
-template <bool kAngle, bool kCheckS>
-__device__ __forceinline__ void cs_eval(CsScan& q, const float4& a, const float2& b, int idx, const CorrConsts& k) {
-  const float pd = cs_pd<kAngle, kCheckS>(q, a, b, k);
-  const bool acc = pd < q.best;
-  q.best = acc ? pd : q.best;
+// two at one load each, by groups of kCsGroup consecutive candidates: the
+// group's minimum distance (one min per candidate) replaces the best when
+// strictly below it, and q.bi keeps the first candidate of that group.  The
+// winning group is the first one holding the least distance, as in the
+// reference's scan; cs_resolve finds the first candidate in it reaching that
+// distance.  best starts at the distance bound and only falls, so a kept
+// distance is below the bound.
+constexpr int kCsGroup = 4;
+
+__device__ __forceinline__ void cs_keep(CsScan& q, float m, int idx) {
+  const bool acc = m < q.best;
+  q.best = acc ? m : q.best;
   q.bi = acc ? idx : q.bi;
 }
+
 template <bool kAngle, bool kCheckS>
 __device__ __forceinline__ void cs_seg1(const float4* ra, const float2* rb, int lo, int hi, int row_base, CsScan& q,
                                         const CorrConsts& k) {
-#pragma unroll 4
-  for (int xx = lo; xx <= hi; ++xx) cs_eval<kAngle, kCheckS>(q, ra[xx], rb[xx], row_base + xx, k);
+  int xx = lo;
+  for (; xx + kCsGroup - 1 <= hi; xx += kCsGroup) {
+    float m = INFINITY;
+#pragma unroll
+    for (int j = 0; j < kCsGroup; ++j) m = fminf(m, cs_pd<kAngle, kCheckS>(q, ra[xx + j], rb[xx + j], k));
+    cs_keep(q, m, row_base + xx);
+  }
+  for (; xx <= hi; ++xx) cs_keep(q, cs_pd<kAngle, kCheckS>(q, ra[xx], rb[xx], k), row_base + xx);
 }
+
 template <bool kAngle, bool kCheckS>
 __device__ __forceinline__ void cs_seg2(const float4* ra, const float2* rb, int lo, int hi, int row_base, CsScan& q0,
                                         CsScan& q1, const CorrConsts& k) {
-#pragma unroll 2
-  for (int xx = lo; xx <= hi; ++xx) {
+  int xx = lo;
+  for (; xx + kCsGroup - 1 <= hi; xx += kCsGroup) {
+    float m0 = INFINITY, m1 = INFINITY;
+#pragma unroll
+    for (int j = 0; j < kCsGroup; ++j) {
+      const float4 a = ra[xx + j];
+      const float2 b = rb[xx + j];
+      m0 = fminf(m0, cs_pd<kAngle, kCheckS>(q0, a, b, k));
+      m1 = fminf(m1, cs_pd<kAngle, kCheckS>(q1, a, b, k));
+    }
+    cs_keep(q0, m0, row_base + xx);
+    cs_keep(q1, m1, row_base + xx);
+  }
+  for (; xx <= hi; ++xx) {
     const float4 a = ra[xx];
     const float2 b = rb[xx];
-    cs_eval<kAngle, kCheckS>(q0, a, b, row_base + xx, k);
-    cs_eval<kAngle, kCheckS>(q1, a, b, row_base + xx, k);
+    cs_keep(q0, cs_pd<kAngle, kCheckS>(q0, a, b, k), row_base + xx);
+    cs_keep(q1, cs_pd<kAngle, kCheckS>(q1, a, b, k), row_base + xx);
   }
+}
+
+// The first candidate of the kept group whose distance equals the best
+// (recomputed with the cap test: where it was left out it holds anyway).
+template <bool kAngle>
+__device__ __forceinline__ void cs_resolve(CsScan& q, const float4* __restrict__ A, const float2* __restrict__ B,
+                                           const CorrConsts& k) {
+  if (!q.on || q.bi < 0) return;
+  const int last = min(q.bi + kCsGroup - 1, (q.bi / k.W) * k.W + k.W - 1);
+  for (int i = q.bi; i <= last; ++i)
+    if (cs_pd<kAngle, true>(q, A[i], B[i], k) == q.best) {
+      q.bi = i;
+      return;
+    }
 }
 
 // Row yy of the two pixels' windows (ra/rb: the row's records indexed by
@@ -567,6 +609,8 @@ __global__ void __launch_bounds__(kCsThreads, kCsCtasPerSm)
         cs_pair_row<kAngle, true>(A + (size_t)yy * k.W, B + (size_t)yy * k.W, yy, q0, q1, k);
     }
   }
+  cs_resolve<kAngle>(q0, A, B, k);
+  cs_resolve<kAngle>(q1, A, B, k);
   if (kDirect) {
 #pragma unroll 1
     for (int h = 0; h < 2; ++h) {
