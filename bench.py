@@ -682,7 +682,8 @@ def run_corr(args, world, rank, local):
     alg_bytes = P * (12 + 12 + 4 + 12 + 32 + CORR_BYTES)
     achieved = alg_bytes / (value * 1e-3) / 1e9
     smem_peak = 148 * 128 * 1.965e9 / 1e9  # nominal: 148 SMs x 128 B/clock x 1965 MHz
-    smem_achieved = cands * 24 / (value * 1e-3) / 1e9
+    # one 24-byte candidate record is read per pair of pixels: 12 B per evaluation
+    smem_achieved = cands * 12 / (value * 1e-3) / 1e9
     cpu = None
     if not args.no_cpu_baseline:
         import oracle as O
@@ -721,7 +722,7 @@ def run_corr(args, world, rank, local):
                      "note": "HBM is not what bounds this search: every candidate is read from shared memory; "
                              "see roofline_smem"},
         "roofline_smem": {"bound": "shared memory", "achieved": smem_achieved, "peak": smem_peak, "unit": "GB/s",
-                          "frac": smem_achieved / smem_peak, "bytes_per_candidate": 24, "candidates": cands,
+                          "frac": smem_achieved / smem_peak, "bytes_per_evaluation": 12, "candidates": cands,
                           "peak_source": "nominal (148 SMs x 128 B/clock x 1965 MHz)"},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
