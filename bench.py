@@ -812,6 +812,216 @@ def run_reference_corr(args, world, rank, local):
     }
 
 
+RASTER_METRIC = "ms per live-surface prediction (skin + rasterise), 640x480, two-cylinder mesh of 164k triangles"
+
+
+def raster_workload():
+    """The live-surface prediction workload: the two-cylinder surface as a
+    mesh of 2 x 256 x 160 quads (163,840 triangles, 82,432 vertices) bent by
+    30 deg through a 2048-node graph, seen by the 640x480 camera moved
+    0.6 deg / 4 mm."""
+    from cudafusion_b200 import synth
+
+    return synth.mesh_frame(seed=13)
+
+
+def run_raster(args, world, rank, local):
+    """`--workload raster`: DynamicFusionPipeline::rasterize_deformed_mesh_live_surface
+    (mesh skinning through the canonical voxels' node lists, rasterisation,
+    resolve) on the B200."""
+    import torch
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from cudafusion_b200.raster import DeviceMesh, LiveSurfaceRaster
+
+    frame = raster_workload()
+    P = frame.width * frame.height
+    mesh = DeviceMesh(frame)
+    raster = LiveSurfaceRaster(frame.width, frame.height)
+    warped = torch.empty_like(mesh.canonical)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        for _ in range(args.warmup):
+            flush.fill_(1)
+            raster.predict(mesh, warped, stream=side)
+    side.synchronize()
+    hits = int((raster.hit_voxel_idx[:P] >= 0).sum().item())
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    sampler = ClockSampler(local) if rank == 0 else None
+    barrier(world)
+    if sampler:
+        sampler.start()
+    launches0 = raster.launch_count()
+    t_wall = time.perf_counter()
+    with torch.cuda.stream(side):
+        for k in range(args.steps):
+            flush.fill_(1)
+            evs[k][0].record(side)
+            raster.predict(mesh, warped, stream=side)
+            evs[k][1].record(side)
+    side.synchronize()
+    barrier(world)
+    t_wall = time.perf_counter() - t_wall
+    clocks = sampler.stop() if sampler else None
+    launches = raster.launch_count() - launches0
+    value = replica_value(sum(a.elapsed_time(b) for a, b in evs), args.steps, world)
+
+    # end to end through the public API: the frame's node transforms from
+    # pinned host memory (the mesh stays on the device, as the pipeline
+    # caches it), the prediction, the three live maps back
+    h_T = mesh.transforms.cpu().pin_memory()
+    h_lv = torch.empty(P * 3, dtype=torch.float32).pin_memory()
+    h_ln = torch.empty(P * 3, dtype=torch.float32).pin_memory()
+    h_hit = torch.empty(P, dtype=torch.int32).pin_memory()
+    e2e_times = []
+    barrier(world)
+    with torch.cuda.stream(side):
+        for _ in range(max(3, min(args.steps, 10))):
+            flush.fill_(1)
+            side.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(side)
+            mesh.transforms.copy_(h_T, non_blocking=True)
+            raster.predict(mesh, warped, stream=side)
+            h_lv.copy_(raster.live_vertices[: 3 * P], non_blocking=True)
+            h_ln.copy_(raster.live_normals[: 3 * P], non_blocking=True)
+            h_hit.copy_(raster.hit_voxel_idx[:P], non_blocking=True)
+            b.record(side)
+            side.synchronize()
+            e2e_times.append(a.elapsed_time(b))
+    e2e_ms = replica_value(sum(e2e_times), len(e2e_times), world)
+    if rank != 0:
+        return None
+    hbm, peak_kind = peaks()
+    V, NT = frame.meta["vertices"], frame.meta["triangles"]
+    # bytes moved at least once: canonical vertices and their node lists /
+    # weights in, warped vertices out; triangles in; per pixel the depth key
+    # written and read and the three maps out
+    alg_bytes = V * (12 + 32 + 12) + NT * 12 + P * (8 + 8 + 12 + 12 + 4)
+    achieved = alg_bytes / (value * 1e-3) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline:
+        import oracle as O
+
+        vox = O.voxel_of_points(frame.canonical, frame.grid_origin, frame.voxel_size, frame.dims)
+        t0 = time.perf_counter()
+        wv = O.skin(frame.canonical, frame.voxel_knn[vox], frame.voxel_knn_w[vox], frame.nodes, frame.transforms,
+                    precision="f32")
+        O.rasterize(frame, wv)
+        dt = time.perf_counter() - t0
+        cpu = {"value": dt * 1e3, "unit": "ms", "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": "one full prediction of the frame: FP32 C oracle skinning (OpenMP) + rasterisation "
+                         "(one thread)"}
+    return {
+        "metric": RASTER_METRIC,
+        "value": value,
+        "unit": "ms",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": value * world,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": f"two-cylinder mesh ({V} vertices, {NT} triangles) skinned by a "
+                        f"{frame.meta['num_nodes']}-node graph, rasterised at {frame.width}x{frame.height}",
+            "pixels": P, "pixels_hit": hits, "l2": "flushed between steps (256 MiB write)",
+            "parallelism": f"replicas x{world}",
+        },
+        "roofline": {"kernel": "skin + raster + resolve", "bound": "hbm", "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                     "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": value,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "note": "three dependent launches of a few microseconds each: bound by launch and "
+                             "atomic latency, not by bytes"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(h_T.numel()),
+                "d2h_bytes_per_step": int(P * 28)},
+        "gpu_launches": int(launches),
+        "gpu_launches_per_step": launches / args.steps,
+        "clocks": clocks,
+        "wall_s_timed_region": t_wall,
+    }
+
+
+def run_reference_raster(args, world, rank, local):
+    """`--impl reference --workload raster`: the reference's own
+    skin_vertices_from_voxel_knn_kernel + rasterize_triangles_z_kernel +
+    resolve_rasterized_triangles_kernel with the pipeline's memsets
+    (include/fusion_app.h:1216-1318) on the same frame."""
+    import torch
+
+    if rank != 0:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_raster
+
+    if not ref_raster.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libcfref_raster.so was not built "
+                "(needs the reference sources: make -C oracle ref)"}
+    frame = raster_workload()
+    P = frame.width * frame.height
+    ref = ref_raster.RefRaster(frame, with_graph=True)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    def one():
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        return ref.run(skin=True)
+
+    for _ in range(args.warmup):
+        one()
+    sampler = ClockSampler(local)
+    sampler.start()
+    times = [one() for _ in range(args.steps)]
+    clocks = sampler.stop()
+    value = sum(times) / len(times)
+    e2e = []
+    for _ in range(max(3, min(args.steps, 5))):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        one()
+        ref.download()
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    ref.close()
+    return {
+        "impl": "reference",
+        "metric": RASTER_METRIC,
+        "value": value,
+        "unit": "ms",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": value,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": f"two-cylinder mesh ({frame.meta['vertices']} vertices, {frame.meta['triangles']} "
+                        f"triangles) skinned by a {frame.meta['num_nodes']}-node graph, rasterised at "
+                        f"{frame.width}x{frame.height}",
+            "implementation": "CUDAFusion skin_vertices_from_voxel_knn_kernel + rasterize_triangles_z_kernel + "
+                              "resolve_rasterized_triangles_kernel with the pipeline's memsets, rebuilt for sm_100a "
+                              "with --use_fast_math (oracle/_ref/libcfref_raster.so)",
+            "l2": "flushed between steps (256 MiB write)",
+            "parallelism": "single GPU (rank 0 of the launch)",
+        },
+        "cpu_baseline": {"value": value, "unit": "ms", "cores": 1, "kind": "reference",
+                         "sample": "the reference path is CUDA: the prediction timed on the GPU, one host thread"},
+        "e2e": {"value": statistics.median(e2e), "unit": "ms", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(P * 28 + frame.meta["vertices"] * 12 + P * 8)},
+        "clocks": clocks,
+    }
+
+
 def run_reference(args, world, rank, local):
     import torch
 
@@ -907,9 +1117,10 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-start comparison")
     ap.add_argument("--no-precision", action="store_true", help="skip the 8192-node precision study")
     ap.add_argument("--pcg-mode", type=int, default=0, help="0 auto, 1 grid-wide, 2 single cluster, 3 streaming")
-    ap.add_argument("--workload", default="frame", choices=["frame", "batch", "learned", "corr"],
+    ap.add_argument("--workload", default="frame", choices=["frame", "batch", "learned", "corr", "raster"],
                     help="frame: the headline line; batch / learned: the batched-solve and learned-start "
-                         "measurements alone; corr: the projective correspondence search")
+                         "measurements alone; corr: the projective correspondence search; raster: the "
+                         "live-surface prediction (mesh skinning + rasterisation)")
     ap.add_argument("--problems", type=int, default=64, help="problems of --workload batch")
     ap.add_argument("--frames", type=int, default=300, help="frames of --workload learned")
     args = ap.parse_args()
@@ -918,6 +1129,10 @@ def main():
     try:
         if args.impl == "reference" and args.workload == "corr":
             line = run_reference_corr(args, world, rank, local)
+        elif args.impl == "reference" and args.workload == "raster":
+            line = run_reference_raster(args, world, rank, local)
+        elif args.workload == "raster":
+            line = run_raster(args, world, rank, local)
         elif args.impl == "reference":
             line = run_reference(args, world, rank, local)
         elif args.workload == "corr":

@@ -82,6 +82,12 @@ EXPORTS = [
     "cf_compute_pixel_knn",
     "cf_corr_search_launch_count",
     "cf_corr_search_set_chunks",
+    "cf_skin_mesh_vertices",
+    "cf_raster_create",
+    "cf_raster_destroy",
+    "cf_rasterize_live_surface",
+    "cf_raster_launch_count",
+    "cf_predict_live_surface",
     "cf_get_version",
     "cf_last_cuda_error",
 ]
@@ -149,6 +155,12 @@ class CorrFrameArgs(ctypes.Structure):
         ("pixel_knn_out", ctypes.c_void_p),
         ("pixel_knn_w_out", ctypes.c_void_p),
     ]
+
+
+class VoxelGrid(ctypes.Structure):
+    """cf_voxel_grid: the canonical grid's origin, voxel size and dims."""
+
+    _fields_ = [("origin", ctypes.c_float * 3), ("voxel_size", ctypes.c_float), ("dims", ctypes.c_int * 3)]
 
 
 class SolveStats(ctypes.Structure):
@@ -249,6 +261,14 @@ def lib():
         L.cf_compute_pixel_knn.argtypes = [vp, i, i, vp, vp, ctypes.c_longlong, vp, vp, vp]
         L.cf_corr_search_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
         L.cf_corr_search_set_chunks.argtypes = [vp, i]
+        L.cf_skin_mesh_vertices.argtypes = [vp, vp, i, ctypes.POINTER(VoxelGrid), vp, vp, i, vp, vp, vp]
+        L.cf_raster_create.argtypes = [i, i, ctypes.POINTER(vp)]
+        L.cf_raster_destroy.argtypes = [vp]
+        L.cf_rasterize_live_surface.argtypes = [vp, vp, vp, vp, i, i, ctypes.POINTER(Camera), ctypes.POINTER(Mat4),
+                                                ctypes.POINTER(VoxelGrid), vp, vp, vp, vp]
+        L.cf_raster_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+        L.cf_predict_live_surface.argtypes = [vp, vp, vp, vp, i, i, vp, vp, i, vp, vp, ctypes.POINTER(Camera),
+                                              ctypes.POINTER(Mat4), ctypes.POINTER(VoxelGrid), vp, vp, vp, vp]
         L.cf_get_version.argtypes = [ctypes.POINTER(i)] * 3
         L.cf_last_cuda_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
         for name in EXPORTS:

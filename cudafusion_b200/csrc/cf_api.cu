@@ -1759,6 +1759,113 @@ cf_status cf_corr_search_launch_count(const cf_corr_search* h, long long* launch
   return CF_OK;
 }
 
+cf_status cf_skin_mesh_vertices(const float* d_canonical, float* d_warped, int num_vertices, const cf_voxel_grid* grid,
+                                const cf_deform_node* d_nodes, const cf_dual_quat* d_transforms, int num_nodes,
+                                const int* d_voxel_knn, const float* d_voxel_knn_w, void* stream) {
+  if (num_vertices < 0 || num_nodes < 0 || !grid) return CF_ERR_INVALID_ARG;
+  if (num_vertices == 0) return CF_OK;
+  if (!d_canonical || !d_warped) return CF_ERR_INVALID_ARG;
+  if (!(grid->voxel_size > 0.f) || grid->dims[0] < 0 || grid->dims[1] < 0 || grid->dims[2] < 0)
+    return CF_ERR_INVALID_ARG;
+  if ((long long)grid->dims[0] * grid->dims[1] * grid->dims[2] > (1LL << 31) / CF_K_NEIGHBORS) return CF_ERR_CAPACITY;
+  CF_TRY(launch_mesh_skin(d_canonical, d_warped, num_vertices, grid, d_nodes, d_transforms, num_nodes, d_voxel_knn,
+                          d_voxel_knn_w, (cudaStream_t)stream));
+  return CF_OK;
+}
+
+struct cf_raster {
+  int max_w = 0, max_h = 0;
+  unsigned long long* ztri = nullptr;  // per pixel: depth bits << 32 | triangle, all ones = empty
+  float4* cache = nullptr;             // per triangle: projection, area, face normal (48 B)
+  int cache_cap = 0;                   // triangles the cache holds
+  bool dirty = false;                  // a call failed after the buffer may have been written
+  long long launches = 0;
+};
+
+cf_status cf_raster_create(int max_width, int max_height, cf_raster** out) {
+  if (!out) return CF_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (max_width <= 0 || max_height <= 0) return CF_ERR_INVALID_ARG;
+  if ((long long)max_width * max_height > (1LL << 30)) return CF_ERR_CAPACITY;
+  cf_raster* h = new cf_raster();
+  h->max_w = max_width;
+  h->max_h = max_height;
+  const size_t P = (size_t)max_width * max_height;
+  cudaError_t e = dalloc(&h->ztri, P);
+  if (e == cudaSuccess) e = cudaMemset(h->ztri, 0xff, P * sizeof(unsigned long long));
+  if (e != cudaSuccess) {
+    cudaFree(h->ztri);
+    delete h;
+    return from_cuda(e);
+  }
+  *out = h;
+  return CF_OK;
+}
+
+cf_status cf_raster_destroy(cf_raster* h) {
+  if (!h) return CF_OK;
+  cudaFree(h->ztri);
+  cudaFree(h->cache);
+  delete h;
+  return CF_OK;
+}
+
+cf_status cf_rasterize_live_surface(cf_raster* h, const float* d_canonical, const float* d_warped,
+                                    const int* d_triangles, int num_vertices, int num_triangles, const cf_camera* cam,
+                                    const cf_mat4* T_cam_world, const cf_voxel_grid* grid, float* d_live_vertices,
+                                    float* d_live_normals, int* d_hit_voxel_idx, void* stream) {
+  if (!h || !cam || !T_cam_world || !grid || num_vertices < 0 || num_triangles < 0) return CF_ERR_INVALID_ARG;
+  if (cam->width < 0 || cam->height < 0) return CF_ERR_INVALID_ARG;
+  if (cam->width > h->max_w || cam->height > h->max_h) return CF_ERR_CAPACITY;
+  if ((long long)cam->width * cam->height == 0) return CF_OK;
+  if (!d_live_vertices || !d_live_normals || !d_hit_voxel_idx) return CF_ERR_INVALID_ARG;
+  if (num_triangles > 0 && (!d_canonical || !d_warped || !d_triangles)) return CF_ERR_INVALID_ARG;
+  if (!(grid->voxel_size > 0.f) || grid->dims[0] < 0 || grid->dims[1] < 0 || grid->dims[2] < 0)
+    return CF_ERR_INVALID_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (num_triangles > h->cache_cap) {  // grows with the mesh (synchronous allocation)
+    CF_TRY(cudaStreamSynchronize(s));
+    cudaFree(h->cache);
+    h->cache = nullptr;
+    h->cache_cap = 0;
+    CF_TRY(dalloc(&h->cache, (size_t)num_triangles * 3));
+    h->cache_cap = num_triangles;
+  }
+  if (h->dirty) {
+    CF_TRY(cudaMemsetAsync(h->ztri, 0xff, (size_t)h->max_w * h->max_h * sizeof(unsigned long long), s));
+    h->dirty = false;
+  }
+  const cudaError_t e = launch_raster(d_canonical, d_warped, d_triangles, num_vertices, num_triangles, cam,
+                                      T_cam_world, grid, h->ztri, h->cache, d_live_vertices, d_live_normals,
+                                      d_hit_voxel_idx, s, &h->launches);
+  if (e != cudaSuccess) {
+    h->dirty = true;
+    return from_cuda(e);
+  }
+  return CF_OK;
+}
+
+cf_status cf_predict_live_surface(cf_raster* h, const float* d_canonical, float* d_warped, const int* d_triangles,
+                                  int num_vertices, int num_triangles, const cf_deform_node* d_nodes,
+                                  const cf_dual_quat* d_transforms, int num_nodes, const int* d_voxel_knn,
+                                  const float* d_voxel_knn_w, const cf_camera* cam, const cf_mat4* T_cam_world,
+                                  const cf_voxel_grid* grid, float* d_live_vertices, float* d_live_normals,
+                                  int* d_hit_voxel_idx, void* stream) {
+  if (!h) return CF_ERR_INVALID_ARG;
+  cf_status st = cf_skin_mesh_vertices(d_canonical, d_warped, num_vertices, grid, d_nodes, d_transforms, num_nodes,
+                                       d_voxel_knn, d_voxel_knn_w, stream);
+  if (st != CF_OK) return st;
+  if (num_vertices > 0) h->launches += 1;
+  return cf_rasterize_live_surface(h, d_canonical, d_warped, d_triangles, num_vertices, num_triangles, cam,
+                                   T_cam_world, grid, d_live_vertices, d_live_normals, d_hit_voxel_idx, stream);
+}
+
+cf_status cf_raster_launch_count(const cf_raster* h, long long* launches) {
+  if (!h || !launches) return CF_ERR_INVALID_ARG;
+  *launches = h->launches;
+  return CF_OK;
+}
+
 cf_status cf_get_version(int* major, int* minor, int* patch) {
   if (major) *major = 0;
   if (minor) *minor = 1;

@@ -185,6 +185,34 @@ __device__ __forceinline__ DQ twist_update(DQ T, const float* dx, float max_rot,
   return dq_mul(dq_from_twist(tw), T);
 }
 
+// warp_point (se3_math.cuh:450-510) centring each node DQ on the fly: node
+// ids outside 0..N-1 and weights below 1e-8 are skipped; no weight left
+// copies the point.
+__device__ __forceinline__ float3 skin_point_centered(float3 p, const int* ids, const float* ws,
+                                                      const cf_deform_node* __restrict__ nodes,
+                                                      const cf_dual_quat* __restrict__ T, int N) {
+  float4 br = make_float4(0.f, 0.f, 0.f, 0.f), bd = make_float4(0.f, 0.f, 0.f, 0.f);
+  float wsum = 0.f;
+  for (int k = 0; k < kK; k++) {
+    int nid = ids[k];
+    float wk = ws[k];
+    if (nid < 0 || nid >= N || wk < 1e-8f) continue;
+    DQ d = dq_centered(load_dq_cg(T + nid), node_pos(nodes, nid));
+    if (qdot(d.r, br) < 0.f) {
+      d.r.x = -d.r.x; d.r.y = -d.r.y; d.r.z = -d.r.z; d.r.w = -d.r.w;
+      d.d.x = -d.d.x; d.d.y = -d.d.y; d.d.z = -d.d.z; d.d.w = -d.d.w;
+    }
+    br.x += wk * d.r.x; br.y += wk * d.r.y; br.z += wk * d.r.z; br.w += wk * d.r.w;
+    bd.x += wk * d.d.x; bd.y += wk * d.d.y; bd.z += wk * d.d.z; bd.w += wk * d.d.w;
+    wsum += wk;
+  }
+  if (wsum < 1e-8f) return p;
+  DQ b;
+  b.r = br;
+  b.d = bd;
+  return dq_transform_point(dq_normalize(b), p);
+}
+
 // se3_math.cuh:450-510 with the per-node plain DQs (dq_centered of each node)
 // computed once per GN iteration instead of once per (point, node).
 __device__ __forceinline__ float3 blend_warp(float3 p, int4 ids, float4 ws, const cf_dual_quat* plain, int N) {

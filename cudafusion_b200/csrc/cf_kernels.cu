@@ -688,29 +688,8 @@ __global__ void skin_points_kernel(const float* __restrict__ pts, const int* __r
                                    const cf_dual_quat* __restrict__ T, int N, float* out) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= M) return;
-  float3 p = f3(pts[3 * c], pts[3 * c + 1], pts[3 * c + 2]);
-  float4 br = make_float4(0.f, 0.f, 0.f, 0.f), bd = make_float4(0.f, 0.f, 0.f, 0.f);
-  float wsum = 0.f;
-  for (int k = 0; k < kK; k++) {
-    int nid = ids[4 * c + k];
-    float wk = ws[4 * c + k];
-    if (nid < 0 || nid >= N || wk < 1e-8f) continue;
-    DQ d = dq_centered(load_dq_cg(T + nid), node_pos(nodes, nid));
-    if (qdot(d.r, br) < 0.f) {
-      d.r.x = -d.r.x; d.r.y = -d.r.y; d.r.z = -d.r.z; d.r.w = -d.r.w;
-      d.d.x = -d.d.x; d.d.y = -d.d.y; d.d.z = -d.d.z; d.d.w = -d.d.w;
-    }
-    br.x += wk * d.r.x; br.y += wk * d.r.y; br.z += wk * d.r.z; br.w += wk * d.r.w;
-    bd.x += wk * d.d.x; bd.y += wk * d.d.y; bd.z += wk * d.d.z; bd.w += wk * d.d.w;
-    wsum += wk;
-  }
-  float3 o = p;
-  if (wsum >= 1e-8f) {
-    DQ b;
-    b.r = br;
-    b.d = bd;
-    o = dq_transform_point(dq_normalize(b), p);
-  }
+  const float3 o = skin_point_centered(f3(pts[3 * c], pts[3 * c + 1], pts[3 * c + 2]), ids + 4 * c, ws + 4 * c,
+                                       nodes, T, N);
   out[3 * c] = o.x;
   out[3 * c + 1] = o.y;
   out[3 * c + 2] = o.z;

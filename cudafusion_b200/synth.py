@@ -795,3 +795,108 @@ def corr_frame(
                   depth_coverage=float((depth > 0).mean()), num_voxels=V, num_nodes=int(node_pos.shape[0]),
                   bend_deg=bend_deg, est_bend_deg=est_bend_deg),
     )
+
+
+@dataclass
+class MeshFrame:
+    """The inputs of one live-surface prediction
+    (DynamicFusionPipeline::rasterize_deformed_mesh_live_surface,
+    include/fusion_app.h:1216-1318): the canonical mesh, its warp (analytic
+    and by the deformation graph), the camera and the canonical voxel grid
+    with the voxels' node lists."""
+
+    width: int
+    height: int
+    cam: np.ndarray  # float32[4]: fx, fy, cx, cy
+    canonical: np.ndarray  # float32[V, 3]
+    warped: np.ndarray  # float32[V, 3]: the articulated mesh (exact warp)
+    triangles: np.ndarray  # int32[T, 3]
+    T_cam_world: np.ndarray  # float32[4, 4]
+    grid_origin: np.ndarray  # float32[3]
+    voxel_size: float
+    dims: np.ndarray  # int32[3]
+    voxel_knn: np.ndarray  # int32[V_grid, 4]
+    voxel_knn_w: np.ndarray  # float32[V_grid, 4]
+    nodes: np.ndarray  # NODE_DTYPE[N]
+    transforms: np.ndarray  # DQ_DTYPE[N]: the articulation as centred node DQs
+    meta: dict = field(default_factory=dict)
+
+
+def _tube_mesh(joint, radius, s0, s1, n_theta, n_axial):
+    th = np.linspace(0.0, 2 * np.pi, n_theta, endpoint=False)
+    s = np.linspace(s0, s1, n_axial + 1)
+    S, TH = np.meshgrid(s, th, indexing="ij")
+    v = np.stack([joint[0] + S, joint[1] + radius * np.cos(TH), joint[2] + radius * np.sin(TH)], -1).reshape(-1, 3)
+    i, j = np.meshgrid(np.arange(n_axial), np.arange(n_theta), indexing="ij")
+    a = i * n_theta + j
+    b = i * n_theta + (j + 1) % n_theta
+    c = (i + 1) * n_theta + j
+    d = (i + 1) * n_theta + (j + 1) % n_theta
+    tri = np.concatenate([np.stack([a, c, b], -1).reshape(-1, 3), np.stack([b, c, d], -1).reshape(-1, 3)])
+    return v, tri
+
+
+def mesh_frame(width=640, height=480, n_theta=256, n_axial=160, bend_deg=30.0, cam_rot_deg=0.6,
+               cam_trans=(0.003, -0.002, 0.002), voxel_size=0.004, num_nodes=None, seed=13):
+    """The two-cylinder surface (radii 6 and 5 cm, lengths 8 and 9 cm, joint
+    at z = 0.14 m) as a triangle mesh: two tubes of n_theta x n_axial quads
+    each, 4 * n_theta * n_axial triangles in all.  `warped` bends the second
+    tube by `bend_deg` about the joint; the deformation graph (nodes sampled
+    from the canonical vertices, 4-NN voxel lists as in
+    src/warp_field.cu:379-404) carries the same articulation as centred node
+    DQs.  Intrinsics scale with width from fx = fy = 570.342 at 640 x 480."""
+    rng = np.random.default_rng(seed)
+    s = width / 640.0
+    fx = fy = 570.342 * s
+    cx, cy = width / 2.0, height / 2.0
+    joint = np.array([0.0, 0.0, 0.14])
+    v1, t1 = _tube_mesh(joint, 0.06, -0.08, 0.0, n_theta, n_axial)
+    v2, t2 = _tube_mesh(joint, 0.05, 0.0, 0.09, n_theta, n_axial)
+    canon = np.concatenate([v1, v2])
+    tris = np.concatenate([t1, t2 + v1.shape[0]]).astype(np.int32)
+    on2 = np.zeros(canon.shape[0], bool)
+    on2[v1.shape[0]:] = True
+    q = _rot_y(np.deg2rad(bend_deg))
+    warped = canon.copy()
+    warped[on2] = joint + _qrotate(np.broadcast_to(q, (int(on2.sum()), 4)), canon[on2] - joint)
+
+    axis = rng.normal(size=3)
+    axis /= np.linalg.norm(axis)
+    R = _rotmat(quat_from_rotvec(axis * np.deg2rad(cam_rot_deg)))
+    T_cw = np.eye(4)
+    T_cw[:3, :3] = R
+    T_cw[:3, 3] = np.asarray(cam_trans, np.float64)
+
+    lo = (canon.min(0) - 2 * voxel_size).astype(np.float32)
+    dims = (np.ceil((canon.max(0) - lo) / voxel_size).astype(np.int64) + 3).astype(np.int32)
+    # the vertices' voxels in FP32, as the skinning kernel finds them
+    ijk = np.floor((canon.astype(np.float32) - lo) / np.float32(voxel_size)).astype(np.int64)
+    vidx = (ijk[:, 2] * dims[1] + ijk[:, 1]) * dims[0] + ijk[:, 0]
+    if num_nodes is None:
+        num_nodes = 2048
+    num_nodes = min(num_nodes, max(4, canon.shape[0] // 4))
+    sel, h = _blue_noise_subsample(canon, num_nodes, rng)
+    node_pos = canon[sel]
+    nb, nw, kc = _graph(node_pos, h)
+    nrm = np.zeros_like(node_pos)
+    nodes = _make_nodes(node_pos, nrm, h, nb, nw, kc)
+    used = np.unique(vidx)
+    centers = lo + (np.stack([used % dims[0], (used // dims[0]) % dims[1], used // (dims[0] * dims[1])], -1)
+                    + 0.5) * voxel_size
+    ids, ws = _skin_weights(centers, node_pos, h)
+    G = int(np.prod(dims.astype(np.int64)))
+    voxel_knn = np.full((G, K_NEIGHBORS), -1, np.int32)
+    voxel_knn_w = np.zeros((G, K_NEIGHBORS), np.float32)
+    voxel_knn[used] = ids
+    voxel_knn_w[used] = ws
+    node_on2 = node_pos[:, 0] > joint[0]
+    qn = np.where(node_on2[:, None], np.broadcast_to(q, (len(node_pos), 4)), np.array([0.0, 0.0, 0.0, 1.0]))
+    tn = _qrotate(qn, node_pos - joint) + joint - node_pos
+    return MeshFrame(
+        width=width, height=height, cam=np.array([fx, fy, cx, cy], np.float32),
+        canonical=canon.astype(np.float32), warped=warped.astype(np.float32), triangles=tris,
+        T_cam_world=T_cw.astype(np.float32), grid_origin=lo.astype(np.float32), voxel_size=float(voxel_size),
+        dims=dims, voxel_knn=voxel_knn, voxel_knn_w=voxel_knn_w, nodes=nodes, transforms=centred_dq(qn, tn),
+        meta=dict(kind="cylinders-mesh", seed=seed, width=width, height=height, vertices=int(canon.shape[0]),
+                  triangles=int(tris.shape[0]), grid_voxels=G, num_nodes=int(node_pos.shape[0]),
+                  bend_deg=bend_deg))

@@ -499,6 +499,74 @@ CF_API cf_status cf_corr_search_launch_count(const cf_corr_search* h, long long*
  * the SM count).  Results do not depend on it. */
 CF_API cf_status cf_corr_search_set_chunks(cf_corr_search* h, int chunks);
 
+/* ------------------------------------------------------------------------ */
+/* Live-surface prediction: the deformed mesh rasterised into the live maps */
+/* the correspondence search reads.                                         */
+/* DynamicFusionPipeline::rasterize_deformed_mesh_live_surface,             */
+/* include/fusion_app.h:1216-1318: skin_vertices_from_voxel_knn_kernel       */
+/* (src/skinning_kernels.cu:29-63), rasterize_triangles_z_kernel and         */
+/* resolve_rasterized_triangles_kernel (src/mesh_raster_kernels.cu:76-200). */
+/* ------------------------------------------------------------------------ */
+
+/* The canonical voxel grid (TSDFParams origin / voxel_size / dims,
+ * include/types.h): voxel (x, y, z) has index (z * dims[1] + y) * dims[0] + x. */
+typedef struct cf_voxel_grid {
+  float origin[3];
+  float voxel_size;
+  int dims[3];
+} cf_voxel_grid;
+
+/* skin_vertices_from_voxel_knn_kernel: each canonical vertex is warped by the
+ * CF_K_NEIGHBORS nodes of the voxel it lies in (warp_point,
+ * include/se3_math.cuh:450-510); a vertex outside the grid, or with no nodes
+ * at all (num_nodes == 0 or no voxel tables), is copied.  d_voxel_knn /
+ * d_voxel_knn_w hold CF_K_NEIGHBORS entries per voxel of the grid.
+ * Asynchronous on `stream`. */
+CF_API cf_status cf_skin_mesh_vertices(const float* d_canonical, float* d_warped, int num_vertices,
+                                       const cf_voxel_grid* grid, const cf_deform_node* d_nodes,
+                                       const cf_dual_quat* d_transforms, int num_nodes, const int* d_voxel_knn,
+                                       const float* d_voxel_knn_w, void* stream);
+
+/* Opaque raster handle: owns the 64-bit depth/triangle buffer of the largest
+ * frame (8 B per pixel) and a per-triangle set-up cache (48 B per triangle,
+ * allocated by the first call with a larger mesh, which then synchronises
+ * `stream`). */
+typedef struct cf_raster cf_raster;
+CF_API cf_status cf_raster_create(int max_width, int max_height, cf_raster** out);
+CF_API cf_status cf_raster_destroy(cf_raster* h);
+
+/* The rasterisation and resolve of rasterize_deformed_mesh_live_surface: the
+ * triangles (int3, indices into both vertex arrays) of the warped mesh are
+ * projected with T_cam_world and cam; each pixel keeps the nearest triangle
+ * covering its centre (ties: the lower triangle index); the pixel's live
+ * vertex is the warped triangle interpolated at the centre, its normal the
+ * warped face normal, and its hit voxel the voxel of the canonical triangle
+ * interpolated there (-1 outside the grid).  Writes every pixel of the
+ * cam->width x cam->height maps (no hit: zero vertex and normal, voxel -1).
+ * FP32 with fused multiply-add accumulation and IEEE division and square
+ * roots (the reference's build uses approximate ones: results agree to
+ * rounding).  Asynchronous on `stream`. */
+CF_API cf_status cf_rasterize_live_surface(cf_raster* h, const float* d_canonical, const float* d_warped,
+                                           const int* d_triangles, int num_vertices, int num_triangles,
+                                           const cf_camera* cam, const cf_mat4* T_cam_world,
+                                           const cf_voxel_grid* grid, float* d_live_vertices,
+                                           float* d_live_normals, int* d_hit_voxel_idx, void* stream);
+
+/* rasterize_deformed_mesh_live_surface once the mesh is extracted: the
+ * canonical vertices skinned into d_warped (cf_skin_mesh_vertices), then
+ * rasterised and resolved (cf_rasterize_live_surface), on one stream.
+ * Asynchronous on `stream`. */
+CF_API cf_status cf_predict_live_surface(cf_raster* h, const float* d_canonical, float* d_warped, const int* d_triangles,
+                                         int num_vertices, int num_triangles, const cf_deform_node* d_nodes,
+                                         const cf_dual_quat* d_transforms, int num_nodes, const int* d_voxel_knn,
+                                         const float* d_voxel_knn_w, const cf_camera* cam,
+                                         const cf_mat4* T_cam_world, const cf_voxel_grid* grid,
+                                         float* d_live_vertices, float* d_live_normals, int* d_hit_voxel_idx,
+                                         void* stream);
+
+/* Kernel launches made through the handle since its creation. */
+CF_API cf_status cf_raster_launch_count(const cf_raster* h, long long* launches);
+
 /* Library / device information. */
 CF_API cf_status cf_get_version(int* major, int* minor, int* patch);
 CF_API cf_status cf_last_cuda_error(char* buf, size_t len);

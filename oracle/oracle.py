@@ -249,3 +249,47 @@ def compute_pixel_knn(hit_voxel_idx, voxel_knn, voxel_knn_w):
     pw = np.zeros((P, 4), np.float32)
     f(_p(hit), P, _p(vk), _p(vw), vk.shape[0], _p(pk), _p(pw))
     return pk, pw
+
+
+# ---- live-surface rasterisation (oracle/cf_oracle_raster.c) ----
+
+
+def rasterize(frame, warped=None, width=None, height=None):
+    """rasterize_triangles_z_kernel + resolve_rasterized_triangles_kernel
+    (src/mesh_raster_kernels.cu:76-200) of `frame` (a synth.MeshFrame) with
+    its warped vertices (or `warped`).  Returns (live vertices f32[P,3],
+    live normals f32[P,3], hit voxel int32[P], depth keys uint64[P])."""
+    L = lib()
+    f = L.cfo_rasterize
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int] * 4 + [ctypes.c_void_p] * 8
+    W = frame.width if width is None else width
+    H = frame.height if height is None else height
+    canon = _f32(frame.canonical)
+    wv = _f32(frame.warped if warped is None else warped)
+    tris = np.ascontiguousarray(frame.triangles, np.int32)
+    cam, cw = _f32(frame.cam), _f32(frame.T_cam_world)
+    grid = np.array(list(frame.grid_origin) + [frame.voxel_size], np.float32)
+    dims = np.ascontiguousarray(frame.dims, np.int32)
+    P = W * H
+    lv = np.zeros((P, 3), np.float32)
+    ln = np.zeros((P, 3), np.float32)
+    hit = np.zeros(P, np.int32)
+    z = np.zeros(P, np.uint64)
+    f(_p(canon), _p(wv), _p(tris), canon.shape[0], tris.shape[0], W, H, _p(cam), _p(cw), _p(grid), _p(dims),
+      _p(lv), _p(ln), _p(hit), _p(z))
+    return lv, ln, hit, z
+
+
+def voxel_of_points(points, grid_origin, voxel_size, dims):
+    """The canonical voxel of each point (src/skinning_kernels.cu:13-24), -1 outside."""
+    L = lib()
+    f = L.cfo_voxel_of_points
+    f.restype = None
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    pts = _f32(points)
+    grid = np.array(list(grid_origin) + [voxel_size], np.float32)
+    dims = np.ascontiguousarray(dims, np.int32)
+    out = np.zeros(pts.shape[0], np.int32)
+    f(_p(pts), pts.shape[0], _p(grid), _p(dims), _p(out))
+    return out

@@ -1,0 +1,177 @@
+"""Live-surface prediction on the B200 (cf_skin_mesh_vertices,
+cf_rasterize_live_surface) against the CPU oracle
+(oracle/cf_oracle_raster.c, which follows src/mesh_raster_kernels.cu:76-200
+triangle by triangle) and against the reference's own kernels
+(oracle/_ref/libcfref_raster.so).
+
+Rasterisation against the oracle is bit-for-bit: the live vertices, normals
+and hit voxels of every pixel, given the same warped vertices.  Skinning is
+FP32 DQ blending against the oracle's FP32 restatement within 2e-6 (the solve's
+skinning bar).  Against the reference's build (--use_fast_math) the bar is
+agreement to rounding: the same pixels hit on >= 99.5 %, and on >= 99 % of
+those the same triangle (vertex within 1e-5 m and normal within 1e-4) with the
+same hit voxel on >= 99 % of them."""
+import dataclasses
+
+import numpy as np
+import pytest
+import torch
+
+from cudafusion_b200 import synth
+from cudafusion_b200.raster import DeviceMesh, LiveSurfaceRaster, skin_mesh
+
+pytestmark = pytest.mark.gpu
+
+
+def run_gpu(frame, warped=None, raster=None):
+    m = DeviceMesh(frame)
+    r = raster or LiveSurfaceRaster(frame.width, frame.height)
+    w = None if warped is None else torch.from_numpy(np.ascontiguousarray(warped, np.float32).reshape(-1)).cuda()
+    r.rasterize(m, w)
+    torch.cuda.synchronize()
+    return r.maps(frame.width * frame.height), r
+
+
+def check_exact(oracle, frame, warped=None, raster=None):
+    (lv, ln, hit), r = run_gpu(frame, warped, raster)
+    olv, oln, ohit, _ = oracle.rasterize(frame, warped)
+    assert np.array_equal(hit, ohit), np.nonzero(hit != ohit)[0][:5]
+    assert np.array_equal(lv.view(np.uint32), olv.view(np.uint32))
+    assert np.array_equal(ln.view(np.uint32), oln.view(np.uint32))
+    return lv, ln, hit, r
+
+
+@pytest.mark.parametrize("case", [(96, 72, 48, 24, 30.0, 0.6), (80, 60, 24, 12, 10.0, 2.0),
+                                  (64, 48, 160, 80, 45.0, 1.0), (37, 23, 32, 16, 20.0, 0.3)],
+                         ids=["coarse", "very-coarse", "sub-pixel", "ragged"])
+def test_small_meshes_bit_exact(oracle, case):
+    w, h, nt, na, bend, rot = case
+    f = synth.mesh_frame(w, h, n_theta=nt, n_axial=na, bend_deg=bend, cam_rot_deg=rot, seed=71)
+    lv, ln, hit, _ = check_exact(oracle, f)
+    assert (np.linalg.norm(lv, axis=1) > 0).mean() > 0.5
+
+
+def test_full_frame_bit_exact(oracle):
+    f = synth.mesh_frame(seed=72)
+    lv, ln, hit, _ = check_exact(oracle, f)
+    assert (hit >= 0).mean() > 0.95
+    # the live points lie on the warped surface: unit normals, depth in range
+    on = np.linalg.norm(lv, axis=1) > 0
+    assert np.allclose(np.linalg.norm(ln[on], axis=1), 1.0, atol=1e-5)
+
+
+def test_degenerate_triangles(oracle):
+    f = synth.mesh_frame(64, 48, n_theta=32, n_axial=16, seed=73)
+    tris = f.triangles.copy()
+    tris[::7, 1] = tris[::7, 0]  # zero area
+    tris[3::11, 2] = -1  # invalid index
+    tris[5::13, 0] = f.canonical.shape[0] + 2  # out of range
+    w = f.warped.copy()
+    w[::29, 2] = -0.5  # behind the camera
+    extra = np.array([[0, 1, 2]], np.int32)  # a triangle spanning the image
+    big = np.concatenate([w, np.array([[-5.0, -5.0, 1.0], [5.0, -5.0, 1.0], [0.0, 5.0, 1.0]], np.float32)])
+    canon = np.concatenate([f.canonical, big[-3:]])
+    g = dataclasses.replace(f, triangles=np.concatenate([tris, extra + w.shape[0]]), warped=big, canonical=canon)
+    check_exact(oracle, g)
+
+
+def test_empty_mesh_and_buffer_reset(oracle):
+    f = synth.mesh_frame(64, 48, n_theta=32, n_axial=16, seed=74)
+    r = LiveSurfaceRaster(64, 48)
+    a = check_exact(oracle, f, raster=r)
+    # an empty mesh right after a full one: the depth buffer was reset
+    g = dataclasses.replace(f, triangles=np.zeros((0, 3), np.int32))
+    lv, ln, hit, _ = check_exact(oracle, g, raster=r)
+    assert np.all(hit == -1) and not lv.any() and not ln.any()
+    b = check_exact(oracle, f, raster=r)
+    assert np.array_equal(a[2], b[2]) and np.array_equal(a[0], b[0])
+
+
+def test_skin_mesh_matches_oracle(oracle):
+    f = synth.mesh_frame(64, 48, n_theta=64, n_axial=32, seed=75)
+    m = DeviceMesh(f)
+    out = skin_mesh(m).cpu().numpy().reshape(-1, 3)
+    vox = oracle.voxel_of_points(f.canonical, f.grid_origin, f.voxel_size, f.dims)
+    assert np.all(vox >= 0)
+    ids = f.voxel_knn[vox]
+    ws = f.voxel_knn_w[vox]
+    want = oracle.skin(f.canonical, ids, ws, f.nodes, f.transforms, precision="f32")
+    assert np.abs(out - want).max() < 2e-6
+    # the graph reproduces the articulation away from the joint
+    far = np.abs(f.canonical[:, 0]) > 0.02
+    assert np.abs(out[far] - f.warped[far]).max() < 2e-3
+
+
+def test_predict_chain_bit_exact(oracle):
+    """skin + rasterise: the rasterised maps are the oracle's on the skinned
+    vertices, bit for bit."""
+    f = synth.mesh_frame(96, 72, n_theta=64, n_axial=32, seed=76)
+    m = DeviceMesh(f)
+    r = LiveSurfaceRaster(96, 72)
+    warped = r.predict(m)
+    torch.cuda.synchronize()
+    lv, ln, hit = r.maps(96 * 72)
+    olv, oln, ohit, _ = oracle.rasterize(f, warped.cpu().numpy().reshape(-1, 3))
+    assert np.array_equal(hit, ohit)
+    assert np.array_equal(lv.view(np.uint32), olv.view(np.uint32))
+    assert np.array_equal(ln.view(np.uint32), oln.view(np.uint32))
+
+
+def test_raster_feeds_the_correspondence_search():
+    """The chain: the rasterised live maps and voxels into the correspondence
+    search against a depth frame rendered from the same surface: nearly every
+    hit pixel pairs with a point within a millimetre of its plane."""
+    from cudafusion_b200.corr import CorrespondenceSearch, CorrParams, DeviceCorrFrame
+
+    f = synth.mesh_frame(160, 120, n_theta=128, n_axial=64, seed=77)
+    m = DeviceMesh(f)
+    r = LiveSurfaceRaster(160, 120)
+    r.rasterize(m)
+    torch.cuda.synchronize()
+    lv, ln, hit = r.maps(160 * 120)
+    # depth = the camera-frame z of the live surface, normals facing the camera
+    T = f.T_cam_world.astype(np.float64)
+    vc = lv.astype(np.float64) @ T[:3, :3].T + T[:3, 3]
+    on = np.linalg.norm(lv, axis=1) > 0
+    depth = np.where(on, vc[:, 2], 0.0).astype(np.float32)
+    nc = ln.astype(np.float64) @ T[:3, :3].T
+    nc = np.where((np.sum(nc * vc, -1) > 0)[:, None], -nc, nc)
+    cf = synth.corr_frame(64, 48, seed=1)
+    G = int(np.prod(f.dims))
+    pk = np.where(hit[:, None] >= 0, f.voxel_knn[np.maximum(hit, 0) % G], -1).astype(np.int32)
+    pw = np.where(hit[:, None] >= 0, f.voxel_knn_w[np.maximum(hit, 0) % G], 0).astype(np.float32)
+    frame = dataclasses.replace(cf, width=160, height=120, cam=f.cam, live_vertices=lv, live_normals=ln,
+                                depth=depth, depth_normals=(nc * on[:, None]).astype(np.float32),
+                                T_cam_world=f.T_cam_world, T_world_cam=np.linalg.inv(T).astype(np.float32),
+                                hit_voxel_idx=hit, voxel_knn=f.voxel_knn, voxel_knn_w=f.voxel_knn_w,
+                                pixel_knn=pk, pixel_knn_w=pw)
+    s = CorrespondenceSearch(160, 120)
+    n = s.find_correspondences(DeviceCorrFrame(frame), CorrParams(0.01, 0.0, 0.0, 2), use_voxels=True)
+    recs = s.records(160 * 120)
+    assert n > 0.95 * on.sum()
+    v = recs["valid"] == 1
+    pd = np.abs(np.sum((recs["dst"][v] - recs["src"][v]) * recs["normal"][v], -1))
+    assert np.percentile(pd, 99) < 1e-3
+
+
+def test_against_reference_kernels():
+    import ref_raster
+
+    if not ref_raster.available():
+        pytest.skip("oracle/_ref/libcfref_raster.so not built (needs the CUDAFusion sources)")
+    f = synth.mesh_frame(seed=78)
+    (lv, ln, hit), _ = run_gpu(f)
+    ref = ref_raster.RefRaster(f, with_graph=False)
+    ref.run(skin=False)
+    rlv, rln, rhit, _, rz = ref.download()
+    ref.close()
+    on, ron = np.linalg.norm(lv, axis=1) > 0, np.linalg.norm(rlv, axis=1) > 0
+    flag = float(np.mean(on == ron))
+    both = on & ron
+    # the same triangle: the same point and the same face normal (a pixel centre
+    # on a shared edge may go to either neighbour under a last-bit difference)
+    same = both & (np.linalg.norm(lv - rlv, axis=1) < 1e-5) & (np.abs(ln - rln).max(axis=1) < 1e-4)
+    frac = float(same.sum()) / max(int(both.sum()), 1)
+    print(f"hit pixels {int(on.sum())} vs {int(ron.sum())}: flags agree {flag:.5f}, same triangle {frac:.5f}")
+    assert flag >= 0.995 and frac >= 0.99
+    assert np.mean(hit[same] == rhit[same]) > 0.99
