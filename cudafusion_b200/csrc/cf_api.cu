@@ -1776,8 +1776,10 @@ cf_status cf_skin_mesh_vertices(const float* d_canonical, float* d_warped, int n
 struct cf_raster {
   int max_w = 0, max_h = 0;
   unsigned long long* ztri = nullptr;  // per pixel: depth bits << 32 | triangle, all ones = empty
-  float4* cache = nullptr;             // per triangle: projection, area, face normal (48 B)
-  int cache_cap = 0;                   // triangles the cache holds
+  float4* cache = nullptr;             // per triangle: projection, area, normal, corners (112 B)
+  int* big = nullptr;                  // triangles whose boxes exceed 64 pixels
+  int* big_count = nullptr;            // their number (reset by the resolve)
+  int cache_cap = 0;                   // triangles the cache and the list hold
   bool dirty = false;                  // a call failed after the buffer may have been written
   long long launches = 0;
 };
@@ -1793,8 +1795,11 @@ cf_status cf_raster_create(int max_width, int max_height, cf_raster** out) {
   const size_t P = (size_t)max_width * max_height;
   cudaError_t e = dalloc(&h->ztri, P);
   if (e == cudaSuccess) e = cudaMemset(h->ztri, 0xff, P * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = dalloc(&h->big_count, 1);
+  if (e == cudaSuccess) e = cudaMemset(h->big_count, 0, sizeof(int));
   if (e != cudaSuccess) {
     cudaFree(h->ztri);
+    cudaFree(h->big_count);
     delete h;
     return from_cuda(e);
   }
@@ -1806,6 +1811,8 @@ cf_status cf_raster_destroy(cf_raster* h) {
   if (!h) return CF_OK;
   cudaFree(h->ztri);
   cudaFree(h->cache);
+  cudaFree(h->big);
+  cudaFree(h->big_count);
   delete h;
   return CF_OK;
 }
@@ -1826,18 +1833,22 @@ cf_status cf_rasterize_live_surface(cf_raster* h, const float* d_canonical, cons
   if (num_triangles > h->cache_cap) {  // grows with the mesh (synchronous allocation)
     CF_TRY(cudaStreamSynchronize(s));
     cudaFree(h->cache);
+    cudaFree(h->big);
     h->cache = nullptr;
+    h->big = nullptr;
     h->cache_cap = 0;
-    CF_TRY(dalloc(&h->cache, (size_t)num_triangles * 3));
+    CF_TRY(dalloc(&h->cache, (size_t)num_triangles * 7));
+    CF_TRY(dalloc(&h->big, (size_t)num_triangles));
     h->cache_cap = num_triangles;
   }
   if (h->dirty) {
     CF_TRY(cudaMemsetAsync(h->ztri, 0xff, (size_t)h->max_w * h->max_h * sizeof(unsigned long long), s));
+    CF_TRY(cudaMemsetAsync(h->big_count, 0, sizeof(int), s));
     h->dirty = false;
   }
   const cudaError_t e = launch_raster(d_canonical, d_warped, d_triangles, num_vertices, num_triangles, cam,
-                                      T_cam_world, grid, h->ztri, h->cache, d_live_vertices, d_live_normals,
-                                      d_hit_voxel_idx, s, &h->launches);
+                                      T_cam_world, grid, h->ztri, h->cache, h->big, h->big_count, d_live_vertices,
+                                      d_live_normals, d_hit_voxel_idx, s, &h->launches);
   if (e != cudaSuccess) {
     h->dirty = true;
     return from_cuda(e);

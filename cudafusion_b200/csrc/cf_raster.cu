@@ -19,12 +19,14 @@
 // operations, so the two agree bit for bit.
 //
 // Launches per frame: mesh_skin_kernel (one thread per vertex, when the caller
-// skins), raster_kernel (one thread per triangle; it stores each drawn
-// triangle's projection, area and face normal for the resolve, and tests a
-// pixel centre against each edge without dividing unless the edge value lies
-// within a narrow band of the threshold), resolve_kernel (one thread per
-// pixel; it writes every pixel and resets the depth buffer for the next
-// frame, which replaces the reference's three memsets).
+// skins); raster_kernel (one thread per triangle: the set-up, the record the
+// resolve reads, and the pixels of a box of up to 64; a larger box goes to a
+// list); raster_big_kernel (one warp per listed triangle, its pixels shared
+// out over the lanes); resolve_kernel (one thread per pixel; it writes every pixel
+// and resets the depth buffer and the list for the next frame, which replaces
+// the reference's three memsets).  A pixel centre is tested against each edge
+// without dividing unless the edge value lies within a narrow band of the
+// threshold.
 #include <cmath>
 
 #include "cf_device.cuh"
@@ -161,73 +163,154 @@ __device__ __forceinline__ bool rs_out(const RsEdgeTest& g, float e, float area)
   return __fdiv_rn(e, area) < -1e-5f;
 }
 
-__global__ void __launch_bounds__(256) raster_kernel(const float* __restrict__ warped, const int3* __restrict__ tris,
-                                                     int V, int NT, const RasterConsts k,
-                                                     unsigned long long* __restrict__ ztri,
-                                                     float4* __restrict__ cache) {
-  const int ti = blockIdx.x * blockDim.x + threadIdx.x;
-  if (ti >= NT) return;
+// The per-triangle record the raster leaves for the resolve: the projected
+// corners, the area, the face normal and the warped and canonical corners,
+// 7 float4 (112 B), so that a pixel's owner is one record away.
+constexpr int kRsRec = 7;
+constexpr int kRsSmallBox = 64;  // boxes up to this many pixels: one thread; larger: one warp
+
+// A drawn triangle's set-up in registers.
+struct RsTri {
+  float2 p0, p1, p2;
+  float area, lo, hi, z0, z1, z2;
+  int min_u, min_v, bw, bh;
+};
+
+// The reference's per-pixel test and depth-key atomic for pixel (x, y) of
+// triangle ti (src/mesh_raster_kernels.cu:112-131), the edge tests without
+// division outside the threshold band.
+__device__ __forceinline__ void rs_fragment(const RsTri& r, int ti, int x, int y, const RasterConsts& k,
+                                            unsigned long long* __restrict__ ztri) {
+  const float2 q = make_float2(__fadd_rn((float)x, 0.5f), __fadd_rn((float)y, 0.5f));
+  const float e0 = rs_edge(r.p1, r.p2, q), e1 = rs_edge(r.p2, r.p0, q), e2 = rs_edge(r.p0, r.p1, q);
+  RsEdgeTest g;
+  g.lo = r.lo;
+  g.hi = r.hi;
+  g.pos = r.area > 0.f;
+  if (rs_out(g, e0, r.area) || rs_out(g, e1, r.area) || rs_out(g, e2, r.area)) return;
+  const float z = rs_lerp3(__fdiv_rn(e0, r.area), __fdiv_rn(e1, r.area), __fdiv_rn(e2, r.area), r.z0, r.z1, r.z2);
+  if (!(z > 0.f) || !isfinite(z)) return;
+  atomicMin(ztri + (size_t)y * k.W + x, ((unsigned long long)__float_as_uint(z) << 32) | (unsigned)ti);
+}
+
+// Set-up of triangle ti (rasterize_triangles_z_kernel up to the pixel loop,
+// src/mesh_raster_kernels.cu:86-110); false when it draws nothing.  A drawn
+// triangle's record goes to the cache (when given).
+__device__ __forceinline__ bool rs_setup(int ti, const float* __restrict__ canon, const float* __restrict__ warped,
+                                         const int3* __restrict__ tris, int V, const RasterConsts& k,
+                                         float4* __restrict__ cache, RsTri& r) {
   const int3 t = tris[ti];
-  if (!rs_valid_tri(t, V)) return;
   float3 wc[3], cc[3];
   float2 p[3];
   float area = 0.f;
-  if (!rs_project(k, warped, t, wc, cc, p, area)) return;
-  const int min_u = max(0, __float2int_rd(fminf(p[0].x, fminf(p[1].x, p[2].x))));
+  if (!rs_valid_tri(t, V) || !rs_project(k, warped, t, wc, cc, p, area)) return false;
+  r.min_u = max(0, __float2int_rd(fminf(p[0].x, fminf(p[1].x, p[2].x))));
   const int max_u = min(k.W - 1, __float2int_ru(fmaxf(p[0].x, fmaxf(p[1].x, p[2].x))));
-  const int min_v = max(0, __float2int_rd(fminf(p[0].y, fminf(p[1].y, p[2].y))));
+  r.min_v = max(0, __float2int_rd(fminf(p[0].y, fminf(p[1].y, p[2].y))));
   const int max_v = min(k.H - 1, __float2int_ru(fmaxf(p[0].y, fmaxf(p[1].y, p[2].y))));
-  if (min_u > max_u || min_v > max_v) return;
+  if (r.min_u > max_u || r.min_v > max_v) return false;
   const float3 fn = rs_normalize(rs_cross(rs_sub(wc[1], wc[0]), rs_sub(wc[2], wc[0])));
-  if (rs_norm(fn) < 1e-6f) return;
-  // the triangle's set-up for the resolve (only a triangle that reaches here
-  // can own a pixel)
-  cache[3 * (size_t)ti] = make_float4(p[0].x, p[0].y, p[1].x, p[1].y);
-  cache[3 * (size_t)ti + 1] = make_float4(p[2].x, p[2].y, area, fn.x);
-  cache[3 * (size_t)ti + 2] = make_float4(fn.y, fn.z, 0.f, 0.f);
+  if (rs_norm(fn) < 1e-6f) return false;
+  if (cache) {
+    const float3 c0 = rs_ld3(canon, t.x), c1 = rs_ld3(canon, t.y), c2 = rs_ld3(canon, t.z);
+    float4* rec = cache + (size_t)kRsRec * ti;
+    rec[0] = make_float4(p[0].x, p[0].y, p[1].x, p[1].y);
+    rec[1] = make_float4(p[2].x, p[2].y, area, fn.x);
+    rec[2] = make_float4(fn.y, fn.z, wc[0].x, wc[0].y);
+    rec[3] = make_float4(wc[0].z, wc[1].x, wc[1].y, wc[1].z);
+    rec[4] = make_float4(wc[2].x, wc[2].y, wc[2].z, c0.x);
+    rec[5] = make_float4(c0.y, c0.z, c1.x, c1.y);
+    rec[6] = make_float4(c1.z, c2.x, c2.y, c2.z);
+  }
   const RsEdgeTest g = rs_edge_test(area);
-  for (int y = min_v; y <= max_v; ++y)
-    for (int x = min_u; x <= max_u; ++x) {
-      const float2 q = make_float2(__fadd_rn((float)x, 0.5f), __fadd_rn((float)y, 0.5f));
-      const float e0 = rs_edge(p[1], p[2], q), e1 = rs_edge(p[2], p[0], q), e2 = rs_edge(p[0], p[1], q);
-      if (rs_out(g, e0, area) || rs_out(g, e1, area) || rs_out(g, e2, area)) continue;
-      const float z = rs_lerp3(__fdiv_rn(e0, area), __fdiv_rn(e1, area), __fdiv_rn(e2, area), cc[0].z, cc[1].z,
-                               cc[2].z);
-      if (z <= 0.f || !isfinite(z)) continue;
-      const unsigned long long packed = ((unsigned long long)__float_as_uint(z) << 32) | (unsigned)ti;
-      atomicMin(ztri + (size_t)y * k.W + x, packed);
-    }
+  r.p0 = p[0];
+  r.p1 = p[1];
+  r.p2 = p[2];
+  r.area = area;
+  r.lo = g.lo;
+  r.hi = g.hi;
+  r.z0 = cc[0].z;
+  r.z1 = cc[1].z;
+  r.z2 = cc[2].z;
+  r.bw = max_u - r.min_u + 1;
+  r.bh = max_v - r.min_v + 1;
+  return true;
 }
 
-__global__ void __launch_bounds__(256) resolve_kernel(const float* __restrict__ canon, const float* __restrict__ warped,
-                                                      const int3* __restrict__ tris, int V, const RasterConsts k,
-                                                      unsigned long long* __restrict__ ztri, const float4* __restrict__ cache,
-                                                      float* __restrict__ lv, float* __restrict__ ln, int* __restrict__ hit) {
+// One thread per triangle: a box of up to kRsSmallBox pixels is drawn here;
+// a larger one goes to the big list for raster_big_kernel.
+__global__ void __launch_bounds__(256) raster_kernel(const float* __restrict__ canon, const float* __restrict__ warped,
+                                                     const int3* __restrict__ tris, int V, int NT,
+                                                     const RasterConsts k, unsigned long long* __restrict__ ztri,
+                                                     float4* __restrict__ cache, int* __restrict__ big,
+                                                     int* __restrict__ big_count) {
+  const int ti = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ti >= NT) return;
+  RsTri r;
+  if (!rs_setup(ti, canon, warped, tris, V, k, cache, r)) return;
+  if (r.bw * r.bh > kRsSmallBox) {
+    big[atomicAdd(big_count, 1)] = ti;
+    return;
+  }
+  for (int y = r.min_v; y < r.min_v + r.bh; ++y)
+    for (int x = r.min_u; x < r.min_u + r.bw; ++x) rs_fragment(r, ti, x, y, k, ztri);
+}
+
+// The big list, one warp per triangle: every lane repeats the set-up (the
+// same operations, so the same values) and the lanes stride over the box's
+// pixels.  The 64-bit min is order-free: the keys equal a sequential pass's.
+__global__ void __launch_bounds__(256) raster_big_kernel(const float* __restrict__ canon,
+                                                         const float* __restrict__ warped,
+                                                         const int3* __restrict__ tris, int V, const RasterConsts k,
+                                                         unsigned long long* __restrict__ ztri,
+                                                         const int* __restrict__ big,
+                                                         const int* __restrict__ big_count) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  const int n = *big_count;
+  for (int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < n; w += warps) {
+    const int ti = big[w];
+    RsTri r;
+    if (!rs_setup(ti, canon, warped, tris, V, k, nullptr, r)) continue;  // drew in raster_kernel: cannot fail
+    const int cnt = r.bw * r.bh;
+    const float inv_w = 1.f / (float)r.bw;
+    for (int idx = lane; idx < cnt; idx += 32) {
+      int row = __float2int_rz((float)idx * inv_w);
+      if (row * r.bw > idx) --row;
+      if ((row + 1) * r.bw <= idx) ++row;
+      rs_fragment(r, ti, r.min_u + (idx - row * r.bw), r.min_v + row, k, ztri);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) resolve_kernel(const RasterConsts k, unsigned long long* __restrict__ ztri,
+                                                      const float4* __restrict__ cache, float* __restrict__ lv,
+                                                      float* __restrict__ ln, int* __restrict__ hit,
+                                                      int* __restrict__ big_count) {
   const int px = blockIdx.x * blockDim.x + threadIdx.x;
+  if (px == 0) *big_count = 0;  // the big list is consumed: ready for the next frame
   if (px >= k.W * k.H) return;
   const unsigned long long packed = ztri[px];
   ztri[px] = kRsEmpty;  // ready for the next frame
   float3 v = make_float3(0.f, 0.f, 0.f), n = v;
   int h = -1;
   if (packed != kRsEmpty) {
-    // the owner passed the raster's tests, so its set-up is in the cache:
-    // the projection, area and face normal resolve_rasterized_triangles_kernel
-    // recomputes (src/mesh_raster_kernels.cu:172-187)
+    // the owner's record: the projection, area, face normal and corners that
+    // resolve_rasterized_triangles_kernel recomputes (src/mesh_raster_kernels.cu:162-199)
     const int ti = (int)(packed & 0xffffffffull);
-    const int3 t = tris[ti];
-    const float4 c0v = cache[3 * (size_t)ti], c1v = cache[3 * (size_t)ti + 1], c2v = cache[3 * (size_t)ti + 2];
-    const float2 p[3] = {make_float2(c0v.x, c0v.y), make_float2(c0v.z, c0v.w), make_float2(c1v.x, c1v.y)};
-    const float area = c1v.z;
+    const float4* rec = cache + (size_t)kRsRec * ti;
+    const float4 r0 = rec[0], r1 = rec[1];
+    const float2 p[3] = {make_float2(r0.x, r0.y), make_float2(r0.z, r0.w), make_float2(r1.x, r1.y)};
+    const float area = r1.z;
     float w0, w1, w2;
     const int y = px / k.W, x = px - y * k.W;
     if (rs_bary(p, area, make_float2(__fadd_rn((float)x, 0.5f), __fadd_rn((float)y, 0.5f)), w0, w1, w2)) {
-      const float3 wc[3] = {rs_ld3(warped, t.x), rs_ld3(warped, t.y), rs_ld3(warped, t.z)};
-      v = make_float3(rs_lerp3(w0, w1, w2, wc[0].x, wc[1].x, wc[2].x), rs_lerp3(w0, w1, w2, wc[0].y, wc[1].y, wc[2].y),
-                      rs_lerp3(w0, w1, w2, wc[0].z, wc[1].z, wc[2].z));
-      n = make_float3(c1v.w, c2v.x, c2v.y);
-      const float3 c0 = rs_ld3(canon, t.x), c1 = rs_ld3(canon, t.y), c2 = rs_ld3(canon, t.z);
-      h = rs_voxel(k, make_float3(rs_lerp3(w0, w1, w2, c0.x, c1.x, c2.x), rs_lerp3(w0, w1, w2, c0.y, c1.y, c2.y),
-                                  rs_lerp3(w0, w1, w2, c0.z, c1.z, c2.z)));
+      const float4 r2 = rec[2], r3 = rec[3], r4 = rec[4], r5 = rec[5], r6 = rec[6];
+      v = make_float3(rs_lerp3(w0, w1, w2, r2.z, r3.y, r4.x), rs_lerp3(w0, w1, w2, r2.w, r3.z, r4.y),
+                      rs_lerp3(w0, w1, w2, r3.x, r3.w, r4.z));
+      n = make_float3(r1.w, r2.x, r2.y);
+      h = rs_voxel(k, make_float3(rs_lerp3(w0, w1, w2, r4.w, r5.z, r6.y), rs_lerp3(w0, w1, w2, r5.x, r5.w, r6.z),
+                                  rs_lerp3(w0, w1, w2, r5.y, r6.x, r6.w)));
     }
   }
   lv[3 * px] = v.x;
@@ -272,17 +355,26 @@ cudaError_t launch_mesh_skin(const float* canon, float* warped, int V, const cf_
 
 cudaError_t launch_raster(const float* canon, const float* warped, const int* tris, int V, int NT,
                           const cf_camera* cam, const cf_mat4* Tcw, const cf_voxel_grid* grid,
-                          unsigned long long* ztri, float4* cache, float* lv, float* ln, int* hit, cudaStream_t s,
-                          long long* launches) {
+                          unsigned long long* ztri, float4* cache, int* big, int* big_count, float* lv, float* ln,
+                          int* hit, cudaStream_t s, long long* launches) {
   const RasterConsts k = raster_consts(cam, Tcw, grid);
   const int P = k.W * k.H;
   if (P == 0) return cudaSuccess;
   const int3* t3 = reinterpret_cast<const int3*>(tris);
   if (NT > 0) {
-    raster_kernel<<<(NT + 255) / 256, 256, 0, s>>>(warped, t3, V, NT, k, ztri, cache);
-    *launches += 1;
+    // the big list is at most NT long; its kernel strides over it, one warp per
+    // triangle, with a grid of 8 CTAs of 8 warps per SM
+    static int sms_times_8 = 0;
+    if (sms_times_8 == 0) {
+      int dev = 0, sms = 148;
+      if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      sms_times_8 = 8 * sms;
+    }
+    raster_kernel<<<(NT + 255) / 256, 256, 0, s>>>(canon, warped, t3, V, NT, k, ztri, cache, big, big_count);
+    raster_big_kernel<<<sms_times_8, 256, 0, s>>>(canon, warped, t3, V, k, ztri, big, big_count);
+    *launches += 2;
   }
-  resolve_kernel<<<(P + 255) / 256, 256, 0, s>>>(canon, warped, t3, V, k, ztri, cache, lv, ln, hit);
+  resolve_kernel<<<(P + 255) / 256, 256, 0, s>>>(k, ztri, cache, lv, ln, hit, big_count);
   *launches += 1;
   return cudaGetLastError();
 }

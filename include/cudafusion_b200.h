@@ -528,9 +528,9 @@ CF_API cf_status cf_skin_mesh_vertices(const float* d_canonical, float* d_warped
                                        const float* d_voxel_knn_w, void* stream);
 
 /* Opaque raster handle: owns the 64-bit depth/triangle buffer of the largest
- * frame (8 B per pixel) and a per-triangle set-up cache (48 B per triangle,
- * allocated by the first call with a larger mesh, which then synchronises
- * `stream`). */
+ * frame (8 B per pixel) and a per-triangle record and list (116 B per
+ * triangle, allocated by the first call with a larger mesh, which then
+ * synchronises `stream`). */
 typedef struct cf_raster cf_raster;
 CF_API cf_status cf_raster_create(int max_width, int max_height, cf_raster** out);
 CF_API cf_status cf_raster_destroy(cf_raster* h);
