@@ -2,7 +2,7 @@
 (oracle/_ref/libcfref_corr.so: kernels/tsdf_kernels.cu unmodified, built for
 sm_100a with the reference's flags, driven by oracle/ref_corr_harness.cu).
 
-TEST / BASELINE INFRASTRUCTURE ONLY: used by the GPU parity tests, by
+TEST AND REFERENCE-ARM INFRASTRUCTURE ONLY: used by the GPU parity tests, by
 tests/golden/make_corr_golden.py and by `bench.py --impl reference
 --workload corr`.  Needs a GPU.
 """

@@ -1,7 +1,7 @@
 // ref_corr_harness.cu — thin driver of the reference's own correspondence
 // search, linked with the unmodified kernels/tsdf_kernels.cu (oracle/Makefile
 // target `ref`, built for sm_100a with --use_fast_math as the reference
-// ships).  TEST / BASELINE INFRASTRUCTURE ONLY: used by the GPU parity tests,
+// ships).  TEST AND REFERENCE-ARM INFRASTRUCTURE ONLY: used by the GPU parity tests,
 // by the script that makes the golden fixtures and by
 // `bench.py --impl reference --workload corr`.
 //

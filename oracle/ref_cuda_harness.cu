@@ -1,7 +1,7 @@
 // ref_cuda_harness.cu — thin driver of the reference's own CUDA solver,
 // linked with the unmodified kernels/solver_kernels.cu and src/warp_field.cu
 // (oracle/Makefile target `ref`, built for sm_100a with --use_fast_math as the
-// reference ships).  TEST / BASELINE INFRASTRUCTURE ONLY: used by the GPU
+// reference ships).  TEST AND REFERENCE-ARM INFRASTRUCTURE ONLY: used by the GPU
 // parity tests and by `bench.py --impl reference`.
 //
 // Per GN iteration it does what the reference pipeline does around the solve

@@ -3,7 +3,7 @@
 src/skinning_kernels.cu unmodified, built for sm_100a with the reference's
 flags, driven by oracle/ref_raster_harness.cu).
 
-TEST / BASELINE INFRASTRUCTURE ONLY: used by the GPU parity tests, by
+TEST AND REFERENCE-ARM INFRASTRUCTURE ONLY: used by the GPU parity tests, by
 tests/golden/make_raster_golden.py and by `bench.py --impl reference
 --workload raster`.  Needs a GPU.
 """

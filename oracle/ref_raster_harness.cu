@@ -1,7 +1,7 @@
 // ref_raster_harness.cu — thin driver of the reference's own live-surface
 // prediction, linked with the unmodified src/mesh_raster_kernels.cu and
 // src/skinning_kernels.cu (oracle/Makefile target `ref`, built for sm_100a
-// with --use_fast_math as the reference ships).  TEST / BASELINE
+// with --use_fast_math as the reference ships).  TEST AND REFERENCE-ARM
 // INFRASTRUCTURE ONLY: used by the GPU parity tests, by the script that makes
 // the golden fixtures and by `bench.py --impl reference --workload raster`.
 //
