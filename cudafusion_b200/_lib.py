@@ -88,6 +88,10 @@ EXPORTS = [
     "cf_rasterize_live_surface",
     "cf_raster_launch_count",
     "cf_predict_live_surface",
+    "cf_validate_update",
+    "cf_scale_delta",
+    "cf_correspondence_rmse",
+    "cf_line_search",
     "cf_get_version",
     "cf_last_cuda_error",
 ]
@@ -161,6 +165,26 @@ class VoxelGrid(ctypes.Structure):
     """cf_voxel_grid: the canonical grid's origin, voxel size and dims."""
 
     _fields_ = [("origin", ctypes.c_float * 3), ("voxel_size", ctypes.c_float), ("dims", ctypes.c_int * 3)]
+
+
+class UpdateStats(ctypes.Structure):
+    """cf_update_stats: the increment's validation statistics and decision."""
+
+    _fields_ = [("rot_sum", ctypes.c_double), ("trans_sum", ctypes.c_double), ("eff_rot_sum", ctypes.c_double),
+                ("eff_trans_sum", ctypes.c_double), ("rot_max", ctypes.c_float), ("trans_max", ctypes.c_float),
+                ("eff_rot_max", ctypes.c_float), ("eff_trans_max", ctypes.c_float), ("finite", ctypes.c_int),
+                ("num_nodes", ctypes.c_int), ("iter_ok", ctypes.c_int), ("pad_", ctypes.c_int)]
+
+
+class LineSearchParams(ctypes.Structure):
+    _fields_ = [("update_scale", ctypes.c_float), ("max_update_rot", ctypes.c_float),
+                ("max_update_trans", ctypes.c_float), ("max_dx_mean", ctypes.c_float),
+                ("min_valid_corrs", ctypes.c_int), ("pad_", ctypes.c_int)]
+
+
+CF_RMSE_BLOCKS = 296
+CF_LINE_SEARCH_TRIALS = 10
+CF_LINE_SEARCH_SCRATCH = 2 * CF_RMSE_BLOCKS + 3 * CF_LINE_SEARCH_TRIALS
 
 
 class SolveStats(ctypes.Structure):
@@ -267,6 +291,15 @@ def lib():
         L.cf_rasterize_live_surface.argtypes = [vp, vp, vp, vp, i, i, ctypes.POINTER(Camera), ctypes.POINTER(Mat4),
                                                 ctypes.POINTER(VoxelGrid), vp, vp, vp, vp]
         L.cf_raster_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+        L.cf_validate_update.argtypes = [vp, i, ctypes.POINTER(LineSearchParams), ctypes.POINTER(UpdateStats), vp]
+        L.cf_scale_delta.argtypes = [vp, i, f, f, f, vp, vp]
+        L.cf_correspondence_rmse.argtypes = [vp, i, vp, vp, vp]
+        L.cf_line_search.argtypes = [vp, vp, vp, vp, vp, i, i, ctypes.POINTER(VoxelGrid), vp, vp, i, vp, vp, vp,
+                                     ctypes.POINTER(LineSearchParams), ctypes.POINTER(CorrFrameArgs),
+                                     ctypes.POINTER(Camera), ctypes.POINTER(Mat4), ctypes.POINTER(Mat4),
+                                     ctypes.POINTER(CorrParams), vp, vp, ctypes.c_double, i, vp, vp, vp,
+                                     ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double),
+                                     ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int), vp]
         L.cf_predict_live_surface.argtypes = [vp, vp, vp, vp, i, i, vp, vp, i, vp, vp, ctypes.POINTER(Camera),
                                               ctypes.POINTER(Mat4), ctypes.POINTER(VoxelGrid), vp, vp, vp, vp]
         L.cf_get_version.argtypes = [ctypes.POINTER(i)] * 3

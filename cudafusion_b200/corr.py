@@ -50,6 +50,29 @@ def _mat4(m):
     return _lib.Mat4((ctypes.c_float * 16)(*a.tolist()))
 
 
+def frame_args(frame, use_voxels=False, pixel_knn_out=None):
+    """cf_corr_frame for a DeviceCorrFrame: the per-pixel node lists, or the
+    hit voxels with the voxel tables (use_voxels); pixel_knn_out = (ids,
+    weights) tensors for the gathered lists (voxel path)."""
+    f = _lib.CorrFrameArgs()
+    f.live_vertices = frame.live_vertices.data_ptr()
+    f.live_normals = frame.live_normals.data_ptr()
+    f.depth = frame.depth.data_ptr()
+    f.depth_normals = frame.depth_normals.data_ptr()
+    if use_voxels:
+        f.hit_voxel_idx = frame.hit_voxel_idx.data_ptr()
+        f.voxel_knn = frame.voxel_knn.data_ptr()
+        f.voxel_knn_w = frame.voxel_knn_w.data_ptr()
+        f.num_voxels = frame.num_voxels
+        if pixel_knn_out is not None:
+            f.pixel_knn_out = pixel_knn_out[0].data_ptr()
+            f.pixel_knn_w_out = pixel_knn_out[1].data_ptr()
+    else:
+        f.pixel_knn = frame.pixel_knn.data_ptr()
+        f.pixel_knn_w = frame.pixel_knn_w.data_ptr()
+    return f
+
+
 class DeviceCorrFrame:
     """The device-resident inputs of one search: a synth.CorrFrame's arrays as
     torch tensors (row-major over height x width)."""
@@ -116,22 +139,7 @@ class CorrespondenceSearch:
         pixel_knn_out (voxel path): also write the gathered lists to
         self.pixel_knn / self.pixel_knn_w."""
         params = params or CorrParams()
-        f = _lib.CorrFrameArgs()
-        f.live_vertices = frame.live_vertices.data_ptr()
-        f.live_normals = frame.live_normals.data_ptr()
-        f.depth = frame.depth.data_ptr()
-        f.depth_normals = frame.depth_normals.data_ptr()
-        if use_voxels:
-            f.hit_voxel_idx = frame.hit_voxel_idx.data_ptr()
-            f.voxel_knn = frame.voxel_knn.data_ptr()
-            f.voxel_knn_w = frame.voxel_knn_w.data_ptr()
-            f.num_voxels = frame.num_voxels
-            if pixel_knn_out:
-                f.pixel_knn_out = self.pixel_knn.data_ptr()
-                f.pixel_knn_w_out = self.pixel_knn_w.data_ptr()
-        else:
-            f.pixel_knn = frame.pixel_knn.data_ptr()
-            f.pixel_knn_w = frame.pixel_knn_w.data_ptr()
+        f = frame_args(frame, use_voxels, (self.pixel_knn, self.pixel_knn_w) if pixel_knn_out else None)
         cam = frame.camera()
         check(_lib.lib().cf_find_correspondences(self._h, ctypes.byref(f), ctypes.byref(cam),
                                                  ctypes.byref(_mat4(frame.T_cam_world)),

@@ -1877,6 +1877,170 @@ cf_status cf_raster_launch_count(const cf_raster* h, long long* launches) {
   return CF_OK;
 }
 
+// ---- update validation and line search -------------------------------------
+
+namespace {
+// device scratch of cf_validate_update: sums (4 doubles), maxima (4 floats as
+// bits), the finite flag; one set per process, calls serialised by g_ls_mu
+__device__ double g_ls_sums[4];
+__device__ unsigned g_ls_max[4];
+__device__ int g_ls_finite;
+std::mutex g_ls_mu;
+}  // namespace
+
+cf_status cf_validate_update(const float* d_delta_x, int num_nodes, const cf_line_search_params* params,
+                             cf_update_stats* stats, void* stream) {
+  if (!params || !stats || num_nodes < 0 || (num_nodes > 0 && !d_delta_x)) return CF_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lock(g_ls_mu);
+  cudaStream_t s = (cudaStream_t)stream;
+  void *sums = nullptr, *maxima = nullptr, *finite = nullptr;
+  CF_TRY(cudaGetSymbolAddress(&sums, g_ls_sums));
+  CF_TRY(cudaGetSymbolAddress(&maxima, g_ls_max));
+  CF_TRY(cudaGetSymbolAddress(&finite, g_ls_finite));
+  const int one = 1;
+  CF_TRY(cudaMemsetAsync(sums, 0, 4 * sizeof(double), s));
+  CF_TRY(cudaMemsetAsync(maxima, 0, 4 * sizeof(unsigned), s));
+  CF_TRY(cudaMemcpyAsync(finite, &one, sizeof(int), cudaMemcpyHostToDevice, s));
+  CF_TRY(launch_update_stats(d_delta_x, num_nodes, params->update_scale, params->max_update_rot,
+                             params->max_update_trans, (double*)sums, (unsigned*)maxima, (int*)finite, s));
+  double hs[4];
+  unsigned hm[4];
+  int hf = 1;
+  CF_TRY(cudaMemcpyAsync(hs, sums, sizeof(hs), cudaMemcpyDeviceToHost, s));
+  CF_TRY(cudaMemcpyAsync(hm, maxima, sizeof(hm), cudaMemcpyDeviceToHost, s));
+  CF_TRY(cudaMemcpyAsync(&hf, finite, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CF_TRY(cudaStreamSynchronize(s));
+  cf_update_stats& st = *stats;
+  st.rot_sum = hs[0];
+  st.trans_sum = hs[1];
+  st.eff_rot_sum = hs[2];
+  st.eff_trans_sum = hs[3];
+  float mx[4];
+  memcpy(mx, hm, sizeof(mx));
+  st.rot_max = mx[0];
+  st.trans_max = mx[1];
+  st.eff_rot_max = mx[2];
+  st.eff_trans_max = mx[3];
+  st.finite = hf;
+  st.num_nodes = num_nodes;
+  st.pad_ = 0;
+  // the acceptance of fusion_app.h:460-489
+  const float n1 = (float)(num_nodes > 1 ? num_nodes : 1);
+  const float eff_rot_mean = (float)st.eff_rot_sum / n1, eff_trans_mean = (float)st.eff_trans_sum / n1;
+  const float ur = params->update_scale;
+  const float reject_rot = params->max_update_rot > 0.f ? 5.0f * params->max_update_rot : INFINITY;
+  const float reject_trans = params->max_update_trans > 0.f ? 5.0f * params->max_update_trans : INFINITY;
+  const bool bad_spike = (ur * st.rot_max > reject_rot) || (ur * st.trans_max > reject_trans);
+  const bool mean_ok = (params->max_dx_mean <= 0.f) ||
+                       (eff_rot_mean <= params->max_dx_mean && eff_trans_mean <= params->max_dx_mean);
+  st.iter_ok = hf && std::isfinite(eff_rot_mean) && std::isfinite(eff_trans_mean) && std::isfinite(st.eff_rot_max) &&
+               std::isfinite(st.eff_trans_max) && st.eff_rot_max < reject_rot && st.eff_trans_max < reject_trans &&
+               mean_ok && !bad_spike;
+  return CF_OK;
+}
+
+cf_status cf_scale_delta(const float* d_delta_x, int num_nodes, float max_rot, float max_trans, float scale,
+                         float* d_out, void* stream) {
+  if (num_nodes < 0) return CF_ERR_INVALID_ARG;
+  if (num_nodes == 0) return CF_OK;
+  if (!d_delta_x || !d_out) return CF_ERR_INVALID_ARG;
+  CF_TRY(launch_scale_delta(d_delta_x, num_nodes, max_rot, max_trans, scale, d_out, (cudaStream_t)stream));
+  return CF_OK;
+}
+
+cf_status cf_correspondence_rmse(const cf_correspondence* d_corrs, int num_corrs, double* d_partials, double* d_out,
+                                 void* stream) {
+  if (num_corrs < 0 || !d_partials || !d_out || (num_corrs > 0 && !d_corrs)) return CF_ERR_INVALID_ARG;
+  CF_TRY(launch_corr_rmse(d_corrs, num_corrs, d_partials, d_out, nullptr, (cudaStream_t)stream));
+  return CF_OK;
+}
+
+cf_status cf_line_search(cf_raster* raster, cf_corr_search* search, const float* d_mesh_canonical,
+                         float* d_mesh_warped, const int* d_mesh_triangles, int num_vertices, int num_triangles,
+                         const cf_voxel_grid* grid, const cf_deform_node* d_nodes, cf_dual_quat* d_transforms,
+                         int num_nodes, const int* d_voxel_knn, const float* d_voxel_knn_w, const float* d_delta_x,
+                         const cf_line_search_params* params, cf_corr_frame* frame, const cf_camera* cam,
+                         const cf_mat4* T_cam_world, const cf_mat4* T_world_cam, const cf_corr_params* corr_params,
+                         cf_correspondence* d_corrs, int* d_num_valid, double base_rmse, int base_valid,
+                         cf_dual_quat* d_scratch_transforms, float* d_scratch_delta, double* d_scratch_rmse,
+                         float* best_scale, double* best_rmse, double* trial_rmse, int* trial_valid, void* stream) {
+  if (!raster || !search || !params || !frame || !cam || !T_cam_world || !T_world_cam || !corr_params ||
+      !best_scale || !best_rmse || num_nodes < 0)
+    return CF_ERR_INVALID_ARG;
+  *best_scale = 0.f;
+  *best_rmse = base_rmse;
+  for (int t = 0; t < CF_LINE_SEARCH_TRIALS; ++t) {
+    if (trial_rmse) trial_rmse[t] = NAN;
+    if (trial_valid) trial_valid[t] = -1;
+  }
+  // fusion_app.h:496-497: no line search without a step or a finite base
+  if (!(params->update_scale > 0.f) || !std::isfinite(base_rmse)) return CF_OK;
+  if (!d_transforms || !d_delta_x || !d_scratch_transforms || !d_scratch_delta || !d_scratch_rmse || !d_corrs ||
+      !d_num_valid || frame->d_pixel_knn || !frame->d_hit_voxel_idx || !frame->d_live_vertices ||
+      !frame->d_live_normals)
+    return CF_ERR_INVALID_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const float u = params->update_scale;
+  const float scales[CF_LINE_SEARCH_TRIALS] = {u,          0.5f * u,    0.25f * u,  0.125f * u, 0.0625f * u,
+                                               -0.0625f * u, -0.125f * u, -0.25f * u, -0.5f * u,  -u};
+  const size_t tbytes = (size_t)num_nodes * sizeof(cf_dual_quat);
+  const int P = cam->width * cam->height;
+  float* lv = const_cast<float*>(frame->d_live_vertices);
+  float* ln = const_cast<float*>(frame->d_live_normals);
+  int* hit = const_cast<int*>(frame->d_hit_voxel_idx);
+  double* partials = d_scratch_rmse;
+  double* slots = d_scratch_rmse + 2 * CF_RMSE_BLOCKS;
+  cf_status st = CF_OK;
+  // one trial, or the final application: restore, scale, apply, predict, search
+  auto apply = [&](float scale) -> cf_status {
+    cf_status r = from_cuda(cudaMemcpyAsync(d_transforms, d_scratch_transforms, tbytes, cudaMemcpyDeviceToDevice, s));
+    if (r == CF_OK) r = cf_scale_delta(d_delta_x, num_nodes, params->max_update_rot, params->max_update_trans, scale,
+                                       d_scratch_delta, stream);
+    if (r == CF_OK) r = cf_warp_apply_twist(d_transforms, d_scratch_delta, num_nodes, params->max_update_rot,
+                                            params->max_update_trans, 1.0f, stream);
+    if (r == CF_OK) r = cf_predict_live_surface(raster, d_mesh_canonical, d_mesh_warped, d_mesh_triangles,
+                                                num_vertices, num_triangles, d_nodes, d_transforms, num_nodes,
+                                                d_voxel_knn, d_voxel_knn_w, cam, T_cam_world, grid, lv, ln, hit,
+                                                stream);
+    if (r == CF_OK) r = cf_find_correspondences(search, frame, cam, T_cam_world, T_world_cam, corr_params, d_corrs,
+                                                d_num_valid, nullptr, stream);
+    return r;
+  };
+  CF_TRY(cudaMemcpyAsync(d_scratch_transforms, d_transforms, tbytes, cudaMemcpyDeviceToDevice, s));  // save
+  for (int t = 0; t < CF_LINE_SEARCH_TRIALS && st == CF_OK; ++t) {
+    st = apply(scales[t]);
+    if (st == CF_OK) st = from_cuda(launch_corr_rmse(d_corrs, P, partials, slots + 3 * t, d_num_valid, s));
+  }
+  if (st != CF_OK) {
+    cudaMemcpyAsync(d_transforms, d_scratch_transforms, tbytes, cudaMemcpyDeviceToDevice, s);
+    return st;
+  }
+  double h[3 * CF_LINE_SEARCH_TRIALS];
+  CF_TRY(cudaMemcpyAsync(h, slots, sizeof(h), cudaMemcpyDeviceToHost, s));
+  CF_TRY(cudaStreamSynchronize(s));
+  // the acceptance of each trial (fusion_app.h:575-582)
+  const int need = (int)(0.75f * (float)base_valid);
+  for (int t = 0; t < CF_LINE_SEARCH_TRIALS; ++t) {
+    const double sum = h[3 * t], wsum = h[3 * t + 1];
+    const int valid = (int)h[3 * t + 2];
+    const double rmse = wsum > 0.0 ? std::sqrt(sum / wsum) : INFINITY;
+    if (trial_rmse) trial_rmse[t] = rmse;
+    if (trial_valid) trial_valid[t] = valid;
+    if (valid >= params->min_valid_corrs && valid >= need && std::isfinite(rmse) && rmse < *best_rmse) {
+      *best_rmse = rmse;
+      *best_scale = scales[t];
+    }
+  }
+  if (*best_scale == 0.f) {  // fusion_app.h:586-592: restore and stop; the maps stay the last trial's
+    CF_TRY(cudaMemcpyAsync(d_transforms, d_scratch_transforms, tbytes, cudaMemcpyDeviceToDevice, s));
+  } else {
+    st = apply(*best_scale);
+    if (st != CF_OK) return st;
+  }
+  CF_TRY(cudaStreamSynchronize(s));
+  return CF_OK;
+}
+
 cf_status cf_get_version(int* major, int* minor, int* patch) {
   if (major) *major = 0;
   if (minor) *minor = 1;

@@ -249,6 +249,13 @@ struct CorrScratch {
   int sms;
 };
 int corr_pick_chunks(int tiles, int sms, int radius, int W, int H);
+// cf_linesearch.cu: the GN step's acceptance
+cudaError_t launch_update_stats(const float* dx, int N, float update_scale, float max_rot, float max_trans,
+                                double* sums, unsigned* maxima, int* finite, cudaStream_t s);
+cudaError_t launch_scale_delta(const float* dx, int N, float max_rot, float max_trans, float scale, float* out,
+                               cudaStream_t s);
+cudaError_t launch_corr_rmse(const cf_correspondence* corrs, int M, double* partials, double* out, const int* valid,
+                             cudaStream_t s);
 // cf_raster.cu: live-surface prediction
 cudaError_t launch_mesh_skin(const float* canon, float* warped, int V, const cf_voxel_grid* grid,
                              const cf_deform_node* nodes, const cf_dual_quat* T, int N, const int* vk, const float* vw,

@@ -567,6 +567,98 @@ CF_API cf_status cf_predict_live_surface(cf_raster* h, const float* d_canonical,
 /* Kernel launches made through the handle since its creation. */
 CF_API cf_status cf_raster_launch_count(const cf_raster* h, long long* launches);
 
+/* ------------------------------------------------------------------------ */
+/* Update validation and line search: the GN step's acceptance.             */
+/* The body of DynamicFusionPipeline's GN loop after the solve,             */
+/* include/fusion_app.h:409-641, with correspondence_rmse (:1331-1350) and  */
+/* upload_scaled_delta_x (:1352-1375), kept on the device.                 */
+/* ------------------------------------------------------------------------ */
+
+/* Per-node increment statistics of the validation (fusion_app.h:409-490):
+ * rn = |dx[0:3]|, tn = |dx[3:6]|; the raw and the scaled-and-clamped
+ * (er = min(update_scale rn, max_rot), et likewise) sums and maxima, summed
+ * in FP64 on the device (the reference sums in FP32 in node order). */
+typedef struct cf_update_stats {
+  double rot_sum, trans_sum, eff_rot_sum, eff_trans_sum;
+  float rot_max, trans_max, eff_rot_max, eff_trans_max;
+  int finite;    /* every rn and tn finite */
+  int num_nodes;
+  int iter_ok;   /* the reference's acceptance of the increment (:480-489) */
+  int pad_;
+} cf_update_stats;
+
+/* The validation's thresholds and the line search's parameters (the
+ * pipeline's params_: update_scale, max_update_rot, max_update_trans,
+ * max_dx_mean, min_valid_corrs). */
+typedef struct cf_line_search_params {
+  float update_scale;
+  float max_update_rot;
+  float max_update_trans;
+  float max_dx_mean;
+  int min_valid_corrs;
+  int pad_;
+} cf_line_search_params;
+
+/* The validation statistics and decision for d_delta_x [6*num_nodes]
+ * (synchronises `stream`). */
+CF_API cf_status cf_validate_update(const float* d_delta_x, int num_nodes, const cf_line_search_params* params,
+                                    cf_update_stats* stats, void* stream);
+
+/* upload_scaled_delta_x (fusion_app.h:1352-1375) on the device: per node the
+ * rotation part scaled by min(1, max_rot / |w|) and the translation part by
+ * min(1, max_trans / |v|) (a bound <= 0 leaves it), both times `scale`. */
+CF_API cf_status cf_scale_delta(const float* d_delta_x, int num_nodes, float max_rot, float max_trans, float scale,
+                                float* d_out, void* stream);
+
+/* correspondence_rmse (fusion_app.h:1331-1350) on the device: over the
+ * records with valid set and weight > 0, r = n . (src - dst) in FP64 (the
+ * difference in FP32), sum w r^2 and sum w; d_out[0] = sum, d_out[1] = wsum
+ * (device doubles, overwritten).  RMSE = sqrt(sum / wsum), +inf when wsum is
+ * 0.  The sums run per block over fixed slices and then in block order, so
+ * a result does not depend on scheduling.  d_partials: 2 x CF_RMSE_BLOCKS
+ * device doubles of scratch.  Asynchronous on `stream`. */
+#define CF_RMSE_BLOCKS 296
+CF_API cf_status cf_correspondence_rmse(const cf_correspondence* d_corrs, int num_corrs, double* d_partials,
+                                        double* d_out, void* stream);
+
+#define CF_LINE_SEARCH_TRIALS 10
+/* device doubles of cf_line_search's d_scratch_rmse */
+#define CF_LINE_SEARCH_SCRATCH (2 * CF_RMSE_BLOCKS + 3 * CF_LINE_SEARCH_TRIALS)
+
+/* The line search of fusion_app.h:493-641 for one GN iteration, on the
+ * device.  With update_scale <= 0 or a non-finite base_rmse it does nothing
+ * (best_scale 0), as the reference breaks there.  Otherwise, for each of the
+ * ten trial scales (update_scale x 1, 1/2, 1/4, 1/8, 1/16 and their
+ * negatives) the saved transforms are restored, the scaled increment applied
+ * (cf_scale_delta, then cf_warp_apply_twist with the clamps and scale 1), the
+ * mesh re-predicted (cf_predict_live_surface into frame's live maps and hit
+ * voxels), the correspondences searched again (cf_find_correspondences into
+ * d_corrs / d_num_valid, the node lists gathered from frame's voxel tables)
+ * and their RMSE reduced (cf_correspondence_rmse).  A trial is kept when its
+ * valid count reaches min_valid_corrs and (int)(0.75 base_valid) and its
+ * RMSE is finite and below the best so far (starting at base_rmse).  The
+ * ten trials are enqueued without synchronising and read back once.  Then
+ * the saved transforms are restored and, when a trial was kept, its
+ * increment applied and the mesh and correspondences predicted and searched
+ * again for it; when none was, the maps and records stay the last trial's,
+ * as in the reference.  d_transforms holds the warp on entry and the
+ * accepted warp on exit; d_scratch_transforms (num_nodes), d_scratch_delta
+ * (6 num_nodes) and d_scratch_rmse (CF_LINE_SEARCH_SCRATCH doubles) are the
+ * caller's device scratch.  *best_scale = 0 means no update; trial_rmse /
+ * trial_valid (CF_LINE_SEARCH_TRIALS each, may be NULL) receive every
+ * trial's result.  Synchronises `stream`. */
+CF_API cf_status cf_line_search(cf_raster* raster, cf_corr_search* search, const float* d_mesh_canonical,
+                                float* d_mesh_warped, const int* d_mesh_triangles, int num_vertices,
+                                int num_triangles, const cf_voxel_grid* grid, const cf_deform_node* d_nodes,
+                                cf_dual_quat* d_transforms, int num_nodes, const int* d_voxel_knn,
+                                const float* d_voxel_knn_w, const float* d_delta_x,
+                                const cf_line_search_params* params, cf_corr_frame* frame, const cf_camera* cam,
+                                const cf_mat4* T_cam_world, const cf_mat4* T_world_cam,
+                                const cf_corr_params* corr_params, cf_correspondence* d_corrs, int* d_num_valid,
+                                double base_rmse, int base_valid, cf_dual_quat* d_scratch_transforms,
+                                float* d_scratch_delta, double* d_scratch_rmse, float* best_scale,
+                                double* best_rmse, double* trial_rmse, int* trial_valid, void* stream);
+
 /* Library / device information. */
 CF_API cf_status cf_get_version(int* major, int* minor, int* patch);
 CF_API cf_status cf_last_cuda_error(char* buf, size_t len);

@@ -293,3 +293,45 @@ def voxel_of_points(points, grid_origin, voxel_size, dims):
     out = np.zeros(pts.shape[0], np.int32)
     f(_p(pts), pts.shape[0], _p(grid), _p(dims), _p(out))
     return out
+
+
+# ---- the GN step's acceptance (oracle/cf_oracle_ls.c) ----
+
+
+def scale_delta(dx, max_rot, max_trans, scale):
+    """upload_scaled_delta_x (include/fusion_app.h:1352-1375)."""
+    L = lib()
+    f = L.cfo_scale_delta
+    f.restype = None
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_void_p]
+    d = _f32(dx).reshape(-1)
+    out = np.zeros_like(d)
+    f(_p(d), d.size // 6, max_rot, max_trans, scale, _p(out))
+    return out
+
+
+def update_stats(dx, update_scale, max_rot, max_trans):
+    """The increment statistics (include/fusion_app.h:427-458): (sums f64[4], maxima f32[4], finite)."""
+    L = lib()
+    f = L.cfo_update_stats
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_void_p,
+                  ctypes.c_void_p]
+    d = _f32(dx).reshape(-1)
+    sums = np.zeros(4, np.float64)
+    maxima = np.zeros(4, np.float32)
+    fin = f(_p(d), d.size // 6, update_scale, max_rot, max_trans, _p(sums), _p(maxima))
+    return sums, maxima, bool(fin)
+
+
+def corr_rmse(recs):
+    """correspondence_rmse (include/fusion_app.h:1331-1350): (sum w r^2, sum w, rmse)."""
+    L = lib()
+    f = L.cfo_corr_rmse
+    f.restype = None
+    f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    r = np.ascontiguousarray(recs)
+    out = np.zeros(2, np.float64)
+    f(_p(r), r.shape[0], _p(out))
+    rmse = float(np.sqrt(out[0] / out[1])) if out[1] > 0 else float("inf")
+    return float(out[0]), float(out[1]), rmse
