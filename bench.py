@@ -1022,6 +1022,142 @@ def run_reference_raster(args, world, rank, local):
     }
 
 
+LS_METRIC = "ms per GN-step line search (10 trials of predict + search + RMSE), 640x480, stock search radius 50"
+
+
+def run_linesearch(args, world, rank, local):
+    """`--workload linesearch`: the GN step's ten-trial line search
+    (include/fusion_app.h:493-641) on the 640x480 two-cylinder mesh (depth
+    from the mesh bent 30 deg, warp at 24 deg, a small random increment), the
+    stock search thresholds.  Compared with the same trials driven the
+    reference's way: a host loop that downloads every correspondence record
+    per trial and sums the RMSE on the host (this library's kernels, the
+    reference's data flow)."""
+    import ctypes
+    import dataclasses
+
+    import torch
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    from cudafusion_b200 import _lib, synth
+    from cudafusion_b200.corr import CorrespondenceSearch, CorrParams, DeviceCorrFrame
+    from cudafusion_b200.linesearch import LineSearch, LineSearchParams, scale_delta
+    from cudafusion_b200.raster import DeviceMesh, LiveSurfaceRaster
+
+    if rank != 0:
+        return None
+    W, H = 640, 480
+    P = W * H
+    true = synth.mesh_frame(W, H, bend_deg=30.0, seed=13)
+    est = synth.mesh_frame(W, H, bend_deg=24.0, seed=13)
+    raster = LiveSurfaceRaster(W, H)
+    raster.rasterize(DeviceMesh(true))
+    torch.cuda.synchronize()
+    lv, ln, _ = raster.maps(P)
+    T = true.T_cam_world.astype(np.float64)
+    vc = lv.astype(np.float64) @ T[:3, :3].T + T[:3, 3]
+    on = np.linalg.norm(lv, axis=1) > 0
+    nc = ln.astype(np.float64) @ T[:3, :3].T
+    nc = np.where((np.sum(nc * vc, -1) > 0)[:, None], -nc, nc) * on[:, None]
+    cf = synth.corr_frame(64, 48, seed=1)
+    frame = dataclasses.replace(
+        cf, width=W, height=H, cam=est.cam, live_vertices=np.zeros((P, 3), np.float32),
+        live_normals=np.zeros((P, 3), np.float32), depth=np.where(on, vc[:, 2], 0.0).astype(np.float32),
+        depth_normals=nc.astype(np.float32), T_cam_world=est.T_cam_world,
+        T_world_cam=np.linalg.inv(T).astype(np.float32), hit_voxel_idx=np.full(P, -1, np.int32),
+        voxel_knn=est.voxel_knn, voxel_knn_w=est.voxel_knn_w, pixel_knn=np.zeros((P, 4), np.int32),
+        pixel_knn_w=np.zeros((P, 4), np.float32))
+    N = est.nodes.shape[0]
+    dx = (np.random.default_rng(13).normal(size=(N, 6)) * [0.01, 0.01, 0.01, 0.003, 0.003, 0.003]).astype(np.float32)
+    mesh = DeviceMesh(est)
+    dframe = DeviceCorrFrame(frame)
+    search = CorrespondenceSearch(W, H)
+    cprm = CorrParams()
+    lp = LineSearchParams(update_scale=1.0, max_update_rot=MAX_ROT, max_update_trans=MAX_TRANS, min_valid_corrs=100)
+    d_dx = torch.from_numpy(dx.reshape(-1).copy()).cuda()
+    T0 = mesh.transforms.clone()
+    warped = torch.empty_like(mesh.canonical)
+
+    def host_flow():
+        """The reference's loop: per trial restore, scale, twist, predict,
+        search, download the records, RMSE on the host."""
+        out = []
+        u = lp.update_scale
+        for sc in (u, 0.5 * u, 0.25 * u, 0.125 * u, 0.0625 * u, -0.0625 * u, -0.125 * u, -0.25 * u, -0.5 * u, -u):
+            Tt = T0.clone()
+            sd = scale_delta(d_dx, N, lp.max_update_rot, lp.max_update_trans, sc)
+            _lib.check(_lib.lib().cf_warp_apply_twist(ctypes.c_void_p(Tt.data_ptr()), ctypes.c_void_p(sd.data_ptr()),
+                                                      N, lp.max_update_rot, lp.max_update_trans, 1.0, None), "twist")
+            mesh.transforms = Tt
+            raster.predict(mesh, warped)
+            dframe.live_vertices.copy_(raster.live_vertices[: 3 * P])
+            dframe.live_normals.copy_(raster.live_normals[: 3 * P])
+            dframe.hit_voxel_idx.copy_(raster.hit_voxel_idx[:P])
+            n = search.find_correspondences(dframe, cprm, use_voxels=True)
+            out.append((n, O.corr_rmse(search.records(P))[2]))
+        mesh.transforms = T0.clone()
+        return out
+
+    base = host_flow()[4]  # a valid, finite base: the smallest positive trial's
+    base_valid, base_rmse = base[0], base[1] * 1.0001
+    ls = LineSearch(N)
+
+    def device_flow():
+        Tls = T0.clone()
+        return ls.run(raster, search, mesh, dframe, Tls, d_dx, base_rmse, base_valid, lp, cprm, warped)
+
+    for _ in range(args.warmup):
+        device_flow()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    sampler = ClockSampler(local)
+    sampler.start()
+    dev_ms = []
+    for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = device_flow()
+        dev_ms.append((time.perf_counter() - t0) * 1e3)
+    clocks = sampler.stop()
+    host_ms = []
+    for _ in range(max(2, min(args.steps, 4))):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        host_flow()
+        host_ms.append((time.perf_counter() - t0) * 1e3)
+    value = statistics.median(dev_ms)
+    return {
+        "metric": LS_METRIC,
+        "value": value,
+        "unit": "ms",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": value,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": f"two-cylinder mesh ({est.meta['vertices']} vertices, {est.meta['triangles']} triangles, "
+                        f"{N} nodes) at {W}x{H}, depth from the 30 deg bend, warp at 24 deg; search radius 50",
+            "timing": "wall clock around the call (it synchronises once, at its read-back); L2 flushed before each",
+            "best_scale": res["best_scale"], "trial_valid": res["trial_valid"],
+        },
+        "reference_data_flow_ms": statistics.median(host_ms),
+        "reference_data_flow": "the same trials driven as the reference's host loop: a synchronous call per step, "
+                               "the 23 MB of records downloaded per trial and the RMSE summed on the host",
+        "cpu_baseline": None,
+        "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 3 * 8 * 10},
+        "gpu_launches": None,
+        "clocks": clocks,
+    }
+
+
 def run_reference(args, world, rank, local):
     import torch
 
@@ -1117,10 +1253,12 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-start comparison")
     ap.add_argument("--no-precision", action="store_true", help="skip the 8192-node precision study")
     ap.add_argument("--pcg-mode", type=int, default=0, help="0 auto, 1 grid-wide, 2 single cluster, 3 streaming")
-    ap.add_argument("--workload", default="frame", choices=["frame", "batch", "learned", "corr", "raster"],
+    ap.add_argument("--workload", default="frame",
+                    choices=["frame", "batch", "learned", "corr", "raster", "linesearch"],
                     help="frame: the headline line; batch / learned: the batched-solve and learned-start "
                          "measurements alone; corr: the projective correspondence search; raster: the "
-                         "live-surface prediction (mesh skinning + rasterisation)")
+                         "live-surface prediction (mesh skinning + rasterisation); linesearch: the GN step's "
+                         "ten-trial line search")
     ap.add_argument("--problems", type=int, default=64, help="problems of --workload batch")
     ap.add_argument("--frames", type=int, default=300, help="frames of --workload learned")
     args = ap.parse_args()
@@ -1131,6 +1269,13 @@ def main():
             line = run_reference_corr(args, world, rank, local)
         elif args.impl == "reference" and args.workload == "raster":
             line = run_reference_raster(args, world, rank, local)
+        elif args.impl == "reference" and args.workload == "linesearch":
+            line = {"impl": "reference", "unavailable": "the reference's line search is host code inside "
+                    "DynamicFusionPipeline (include/fusion_app.h:493-641), which needs OpenCV, Open3D and yaml-cpp "
+                    "to build; bench.py --workload linesearch reports the same trials driven the reference's way "
+                    "as reference_data_flow_ms"}
+        elif args.workload == "linesearch":
+            line = run_linesearch(args, world, rank, local)
         elif args.workload == "raster":
             line = run_raster(args, world, rank, local)
         elif args.impl == "reference":
