@@ -1,7 +1,11 @@
 // cudafusion_b200.hpp — C++ drop-in for CUDAFusion's solve-path classes.
 //
-//   cudafusion_b200::GaussNewtonSolver   include/solver.h:10-89
-//   cudafusion_b200::WarpField           include/warp_field.h:12-126 (solve-path subset)
+//   cudafusion_b200::GaussNewtonSolver     include/solver.h:10-89
+//   cudafusion_b200::WarpField             include/warp_field.h:12-126 (solve-path subset)
+//   cudafusion_b200::CorrespondenceSearch  DynamicFusionPipeline::find_correspondences,
+//                                          include/fusion_app.h:1791-1845
+//   cudafusion_b200::LiveSurfaceRaster     DynamicFusionPipeline::rasterize_deformed_mesh_live_surface,
+//                                          include/fusion_app.h:1216-1318 (after the mesh extraction)
 //
 // Header-only, on top of the C ABI (cudafusion_b200.h, link libcfb200.so).
 // The classes keep the reference's constructor and method signatures and
@@ -253,6 +257,83 @@ class WarpField {
   DQ* d_Tprev_ = nullptr;
   std::vector<Node> h_nodes_;
   std::vector<DQ> h_T_;
+};
+
+// The projective correspondence search on the pipeline's own buffers.  Cam,
+// M4 and Corr are the caller's CameraIntrinsics, Mat4 and Correspondence.
+class CorrespondenceSearch {
+ public:
+  CorrespondenceSearch(int max_width, int max_height) {
+    check(cf_corr_search_create(max_width, max_height, &h_), "CorrespondenceSearch");
+  }
+  ~CorrespondenceSearch() { cf_corr_search_destroy(h_); }
+  CorrespondenceSearch(const CorrespondenceSearch&) = delete;
+  CorrespondenceSearch& operator=(const CorrespondenceSearch&) = delete;
+
+  // find_correspondences: searches, synchronises and returns the valid count
+  // (d_stats, when given, receives the six debug counters).
+  template <class Cam, class M4, class Corr>
+  int find_correspondences(const cf_corr_frame& frame, const Cam& cam, const M4& T_cam_world, const M4& T_world_cam,
+                           const cf_corr_params& params, Corr* d_corrs, int* d_num_valid, int* d_stats = nullptr) {
+    static_assert(sizeof(Cam) == sizeof(cf_camera) && sizeof(M4) == sizeof(cf_mat4) &&
+                      sizeof(Corr) == sizeof(cf_correspondence),
+                  "CameraIntrinsics / Mat4 / Correspondence layouts");
+    check(cf_find_correspondences(h_, &frame, reinterpret_cast<const cf_camera*>(&cam),
+                                  reinterpret_cast<const cf_mat4*>(&T_cam_world),
+                                  reinterpret_cast<const cf_mat4*>(&T_world_cam), &params,
+                                  reinterpret_cast<cf_correspondence*>(d_corrs), d_num_valid, d_stats, nullptr),
+          "find_correspondences");
+    int n = 0;
+    check_cuda(cudaMemcpy(&n, d_num_valid, sizeof(int), cudaMemcpyDeviceToHost), "find_correspondences");
+    return n;
+  }
+  cf_corr_search* handle() { return h_; }
+
+ private:
+  static void check_cuda(cudaError_t e, const char* where) {
+    if (e != cudaSuccess) check(CF_ERR_CUDA, where);
+  }
+  cf_corr_search* h_ = nullptr;
+};
+
+// The live-surface prediction: mesh skinning, rasterisation and resolve into
+// the pipeline's live maps.  Node / DQ / Cam / M4 are the caller's
+// DeformNode, DualQuat, CameraIntrinsics and Mat4; vertices are float3.
+class LiveSurfaceRaster {
+ public:
+  LiveSurfaceRaster(int max_width, int max_height) {
+    check(cf_raster_create(max_width, max_height, &h_), "LiveSurfaceRaster");
+  }
+  ~LiveSurfaceRaster() { cf_raster_destroy(h_); }
+  LiveSurfaceRaster(const LiveSurfaceRaster&) = delete;
+  LiveSurfaceRaster& operator=(const LiveSurfaceRaster&) = delete;
+
+  // rasterize_deformed_mesh_live_surface after the mesh is extracted;
+  // synchronises, as the reference does.
+  template <class V3, class I3, class Node, class DQ, class Cam, class M4>
+  void predict(const V3* d_canonical, V3* d_warped, const I3* d_triangles, int num_vertices, int num_triangles,
+               const Node* d_nodes, const DQ* d_transforms, int num_nodes, const int* d_voxel_knn,
+               const float* d_voxel_knn_w, const Cam& cam, const M4& T_cam_world, const cf_voxel_grid& grid,
+               V3* d_live_vertices, V3* d_live_normals, int* d_hit_voxel_idx) {
+    static_assert(sizeof(V3) == 3 * sizeof(float) && sizeof(I3) == 3 * sizeof(int), "float3 / int3");
+    static_assert(sizeof(Node) == sizeof(cf_deform_node) && sizeof(DQ) == sizeof(cf_dual_quat) &&
+                      sizeof(Cam) == sizeof(cf_camera) && sizeof(M4) == sizeof(cf_mat4),
+                  "DeformNode / DualQuat / CameraIntrinsics / Mat4 layouts");
+    check(cf_predict_live_surface(h_, reinterpret_cast<const float*>(d_canonical), reinterpret_cast<float*>(d_warped),
+                                  reinterpret_cast<const int*>(d_triangles), num_vertices, num_triangles,
+                                  reinterpret_cast<const cf_deform_node*>(d_nodes),
+                                  reinterpret_cast<const cf_dual_quat*>(d_transforms), num_nodes, d_voxel_knn,
+                                  d_voxel_knn_w, reinterpret_cast<const cf_camera*>(&cam),
+                                  reinterpret_cast<const cf_mat4*>(&T_cam_world), &grid,
+                                  reinterpret_cast<float*>(d_live_vertices), reinterpret_cast<float*>(d_live_normals),
+                                  d_hit_voxel_idx, nullptr),
+          "rasterize_deformed_mesh_live_surface");
+    if (cudaDeviceSynchronize() != cudaSuccess) check(CF_ERR_CUDA, "rasterize_deformed_mesh_live_surface");
+  }
+  cf_raster* handle() { return h_; }
+
+ private:
+  cf_raster* h_ = nullptr;
 };
 
 }  // namespace cudafusion_b200

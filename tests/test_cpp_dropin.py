@@ -84,3 +84,21 @@ def test_dropin_loop_matches_python_mirror(exe, tmp_path):
     e0, e1 = (float(v) for v in r.stdout.split()[1:3])
     assert e0 == pytest.approx(st["energy_initial"], rel=1e-12)
     assert e1 == pytest.approx(st["energy_final"], rel=1e-12)
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-device error path")
+def test_frontend_classes_compile_and_fail_loudly_without_gpu(cflib, tmp_path):
+    """CorrespondenceSearch and LiveSurfaceRaster compile against the
+    reference's type layouts (-Wall -Werror) and, with no GPU, throw
+    CF_ERR_NO_DEVICE from their constructors."""
+    out = str(tmp_path / "dropin_frontend")
+    src = os.path.join(ROOT, "tests", "cpp", "dropin_frontend.cpp")
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+           "-I", os.path.join(CUDA, "include"), src, "-o", out, "-L", LIBDIR, "-lcfb200",
+           f"-Wl,-rpath,{LIBDIR}", "-L", os.path.join(CUDA, "lib64"), "-lcudart",
+           f"-Wl,-rpath,{os.path.join(CUDA, 'lib64')}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([out, "nodev"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stdout + r.stderr
+
