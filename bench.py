@@ -1022,6 +1022,244 @@ def run_reference_raster(args, world, rank, local):
     }
 
 
+TSDF_METRIC = "ms per warped TSDF integration, 256^3 x 6 mm volume, 640x480 depth, gated at 3 optimisations"
+TSDF_MIN_OPT = 3
+
+
+def tsdf_workload():
+    """The reference's volume (256^3 voxels of 6 mm from (-0.768, -0.768,
+    0.5), truncation 3 cm, decay 0.9, cap 50) with a bumpy surface 1.1 m in
+    front of the 640x480 camera; a 1728-node graph on the surface warps by up
+    to 3 deg / 1 cm; voxels within 6 voxels of the surface hold node lists;
+    the prior volume and the optimisation counts (0..6) cover 15 voxels
+    either side of it."""
+    from cudafusion_b200 import synth
+
+    return synth.tsdf_frame(knn_band_voxels=6, invalid_frac=0.002, seed=21)
+
+
+def run_tsdf(args, world, rank, local):
+    """`--workload tsdf`: TSDFVolume::integrate warped and gated, as
+    DynamicFusionPipeline runs it after the solve (include/fusion_app.h:655-666)."""
+    import torch
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from cudafusion_b200 import _lib
+    from cudafusion_b200.solver import to_device
+    from cudafusion_b200.tsdf import TSDFVolume, TsdfParams
+
+    f = tsdf_workload()
+    p = f.params
+    prm = TsdfParams(dims=tuple(int(v) for v in p["dims"]), voxel_size=p["voxel_size"], truncation=p["truncation"],
+                     origin=tuple(float(v) for v in p["origin"]), decay_alpha=p["decay_alpha"],
+                     max_weight=p["max_weight"])
+    vol = TSDFVolume(prm)
+    vol.voxels.copy_(torch.from_numpy(f.voxels.view(np.uint8).reshape(-1).copy()))
+    V = vol.n
+    depth = torch.from_numpy(f.depth.copy()).cuda()
+    nodes, T = to_device(f.nodes), to_device(f.transforms)
+    N = f.nodes.shape[0]
+    knn = torch.from_numpy(f.voxel_knn.reshape(-1).copy()).cuda()
+    knn_w = torch.from_numpy(f.voxel_knn_w.reshape(-1).copy()).cuda()
+    counts = torch.from_numpy(f.counts.copy()).cuda()
+    fx, fy, cx, cy = (float(v) for v in f.cam)
+    cam = _lib.Camera(fx, fy, cx, cy, f.width, f.height)
+    pose = f.camera_pose
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    side = torch.cuda.Stream()
+
+    def one():
+        vol.integrate(depth, cam, pose, nodes, T, N, knn, knn_w, counts, TSDF_MIN_OPT, stream=side)
+
+    before = vol.fields().clone()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(side):
+        one()
+    side.synchronize()
+    updated = int((vol.fields() != before).any(dim=1).sum().item())
+    del before
+    with torch.cuda.stream(side):
+        for _ in range(args.warmup):
+            flush.fill_(1)
+            one()
+    side.synchronize()
+    gated_in = int((counts >= TSDF_MIN_OPT).sum().item())
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    sampler = ClockSampler(local) if rank == 0 else None
+    barrier(world)
+    if sampler:
+        sampler.start()
+    t_wall = time.perf_counter()
+    with torch.cuda.stream(side):
+        for k in range(args.steps):
+            flush.fill_(1)
+            evs[k][0].record(side)
+            one()
+            evs[k][1].record(side)
+    side.synchronize()
+    barrier(world)
+    t_wall = time.perf_counter() - t_wall
+    clocks = sampler.stop() if sampler else None
+    value = replica_value(sum(a.elapsed_time(b) for a, b in evs), args.steps, world)
+
+    # end to end through the public API: the frame's depth and node
+    # transforms from pinned host memory (the volume, the voxel node lists and
+    # the counts stay on the device, as the pipeline keeps them), the
+    # integration, and the volume's centre voxel read back
+    h_depth = torch.from_numpy(f.depth.copy()).pin_memory()
+    h_T = T.cpu().pin_memory()
+    h_out = torch.empty(3, dtype=torch.float32).pin_memory()
+    mid = (V // 2)
+    e2e_times = []
+    barrier(world)
+    with torch.cuda.stream(side):
+        for _ in range(max(3, min(args.steps, 10))):
+            flush.fill_(1)
+            side.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(side)
+            depth.copy_(h_depth, non_blocking=True)
+            T.copy_(h_T, non_blocking=True)
+            one()
+            h_out.copy_(vol.fields()[mid], non_blocking=True)
+            b.record(side)
+            side.synchronize()
+            e2e_times.append(a.elapsed_time(b))
+    e2e_ms = replica_value(sum(e2e_times), len(e2e_times), world)
+    if rank != 0:
+        return None
+    hbm, peak_kind = peaks()
+    # bytes moved at least once: every voxel's count; the node lists and
+    # weights of the voxels that pass the gate; tsdf + weight read and written
+    # for the voxels updated (the depth map and the nodes stay in L2)
+    alg_bytes = 4 * V + 32 * gated_in + 16 * updated
+    achieved = alg_bytes / (value * 1e-3) / 1e9
+    traffic = load_traffic("tsdf_integrate_kernel")
+    cpu = None
+    if not args.no_cpu_baseline:
+        import oracle as O
+
+        plane = int(p["dims"][0]) * int(p["dims"][1])
+        z0, z1 = 116, 124  # 8 planes through the surface
+        lo, hi = z0 * plane, z1 * plane
+        vox = f.voxels.copy()
+        cam_t = (fx, fy, cx, cy, f.width, f.height)
+        t0 = time.perf_counter()
+        cen = O.tsdf_centres(p["dims"], p["origin"], p["voxel_size"], lo, hi)
+        sel = np.nonzero(f.counts[lo:hi] >= TSDF_MIN_OPT)[0]
+        live = cen.copy()
+        live[sel] = O.skin(cen[sel], f.voxel_knn[lo + sel], f.voxel_knn_w[lo + sel], f.nodes, f.transforms,
+                           precision="f32")
+        O.tsdf_integrate(vox, p, f.depth, cam_t, pose, live=live, counts=f.counts, gate=True, min_opt=TSDF_MIN_OPT,
+                         lo=lo, hi=hi)
+        dt = time.perf_counter() - t0
+        cpu = {"value": dt * 1e3 * V / (hi - lo), "unit": "ms", "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": f"8 of 256 z-planes through the surface ({hi - lo} voxels, "
+                         f"{int((f.counts[lo:hi] >= TSDF_MIN_OPT).sum())} past the gate) by the C oracle (FP32 "
+                         "skinning of the gated voxels with OpenMP, the integration on one thread), scaled by "
+                         "voxels to the full volume (the surface planes are the dense ones: an upper bound)"}
+    return {
+        "metric": TSDF_METRIC,
+        "value": value,
+        "unit": "ms",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": value * world,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": f"warped TSDF integration of a {'x'.join(str(int(v)) for v in p['dims'])} volume "
+                        f"({V} voxels, {gated_in} past the gate, {updated} updated) by a {N}-node graph, "
+                        f"{f.width}x{f.height} depth",
+            "l2": "flushed between steps (256 MiB write)",
+            "parallelism": f"replicas x{world}",
+        },
+        "roofline": {"kernel": "tsdf_integrate_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": value,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "note": "two launches per integration (the per-node plain DQs, then the volume)"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(h_depth.numel() * 4 + h_T.numel()),
+                "d2h_bytes_per_step": 12},
+        "gpu_launches": 2 * args.steps,
+        "gpu_launches_per_step": 2,
+        "clocks": clocks,
+        "wall_s_timed_region": t_wall,
+    }
+
+
+def run_reference_tsdf(args, world, rank, local):
+    """`--impl reference --workload tsdf`: the reference's own
+    TSDFVolume::integrate (src/tsdf_volume.cu:23-60, tsdf_integrate_kernel)
+    on the same volume and frame."""
+    import torch
+
+    if rank != 0:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_tsdf
+
+    if not ref_tsdf.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libcfref_tsdf.so was not built "
+                "(needs the reference sources: make -C oracle ref)"}
+    f = tsdf_workload()
+    ref = ref_tsdf.RefTsdf(f, warp=True, gate=True)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    def one():
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        return ref.integrate(TSDF_MIN_OPT)
+
+    for _ in range(args.warmup):
+        one()
+    sampler = ClockSampler(local)
+    sampler.start()
+    times = [one() for _ in range(args.steps)]
+    clocks = sampler.stop()
+    value = sum(times) / len(times)
+    e2e = []
+    for _ in range(max(3, min(args.steps, 5))):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        one()
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    ref.close()
+    return {
+        "impl": "reference",
+        "metric": TSDF_METRIC,
+        "value": value,
+        "unit": "ms",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": value,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": "warped TSDF integration of a 256x256x256 volume by a 1728-node graph, 640x480 depth",
+            "implementation": "CUDAFusion TSDFVolume::integrate (tsdf_integrate_kernel on 8x8 blocks), rebuilt for "
+                              "sm_100a with --use_fast_math (oracle/_ref/libcfref_tsdf.so)",
+            "l2": "flushed between steps (256 MiB write)",
+            "parallelism": "single GPU (rank 0 of the launch)",
+        },
+        "cpu_baseline": {"value": value, "unit": "ms", "cores": 1, "kind": "reference",
+                         "sample": "the reference path is CUDA: the integration timed on the GPU, one host thread"},
+        "e2e": {"value": statistics.median(e2e), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clocks,
+    }
+
+
 LS_METRIC = "ms per GN-step line search (10 trials of predict + search + RMSE), 640x480, stock search radius 50"
 
 
@@ -1254,11 +1492,11 @@ def main():
     ap.add_argument("--no-precision", action="store_true", help="skip the 8192-node precision study")
     ap.add_argument("--pcg-mode", type=int, default=0, help="0 auto, 1 grid-wide, 2 single cluster, 3 streaming")
     ap.add_argument("--workload", default="frame",
-                    choices=["frame", "batch", "learned", "corr", "raster", "linesearch"],
+                    choices=["frame", "batch", "learned", "corr", "raster", "linesearch", "tsdf"],
                     help="frame: the headline line; batch / learned: the batched-solve and learned-start "
                          "measurements alone; corr: the projective correspondence search; raster: the "
                          "live-surface prediction (mesh skinning + rasterisation); linesearch: the GN step's "
-                         "ten-trial line search")
+                         "ten-trial line search; tsdf: the warped TSDF integration")
     ap.add_argument("--problems", type=int, default=64, help="problems of --workload batch")
     ap.add_argument("--frames", type=int, default=300, help="frames of --workload learned")
     args = ap.parse_args()
@@ -1274,6 +1512,10 @@ def main():
                     "DynamicFusionPipeline (include/fusion_app.h:493-641), which needs OpenCV, Open3D and yaml-cpp "
                     "to build; bench.py --workload linesearch reports the same trials driven the reference's way "
                     "as reference_data_flow_ms"}
+        elif args.impl == "reference" and args.workload == "tsdf":
+            line = run_reference_tsdf(args, world, rank, local)
+        elif args.workload == "tsdf":
+            line = run_tsdf(args, world, rank, local)
         elif args.workload == "linesearch":
             line = run_linesearch(args, world, rank, local)
         elif args.workload == "raster":

@@ -92,6 +92,11 @@ EXPORTS = [
     "cf_scale_delta",
     "cf_correspondence_rmse",
     "cf_line_search",
+    "cf_tsdf_reset",
+    "cf_tsdf_world_to_camera",
+    "cf_tsdf_integrate",
+    "cf_tsdf_warp_voxel_centres",
+    "cf_mark_optimized_voxels",
     "cf_get_version",
     "cf_last_cuda_error",
 ]
@@ -180,6 +185,13 @@ class LineSearchParams(ctypes.Structure):
     _fields_ = [("update_scale", ctypes.c_float), ("max_update_rot", ctypes.c_float),
                 ("max_update_trans", ctypes.c_float), ("max_dx_mean", ctypes.c_float),
                 ("min_valid_corrs", ctypes.c_int), ("pad_", ctypes.c_int)]
+
+
+class TsdfParams(ctypes.Structure):
+    """cf_tsdf_params: TSDFVolume::Params (include/tsdf_volume.h:10-19)."""
+
+    _fields_ = [("dims", ctypes.c_int * 3), ("voxel_size", ctypes.c_float), ("truncation", ctypes.c_float),
+                ("origin", ctypes.c_float * 3), ("decay_alpha", ctypes.c_float), ("max_weight", ctypes.c_float)]
 
 
 CF_RMSE_BLOCKS = 296
@@ -302,6 +314,12 @@ def lib():
                                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int), vp]
         L.cf_predict_live_surface.argtypes = [vp, vp, vp, vp, i, i, vp, vp, i, vp, vp, ctypes.POINTER(Camera),
                                               ctypes.POINTER(Mat4), ctypes.POINTER(VoxelGrid), vp, vp, vp, vp]
+        L.cf_tsdf_reset.argtypes = [vp, ctypes.c_longlong, vp]
+        L.cf_tsdf_world_to_camera.argtypes = [ctypes.POINTER(Mat4), ctypes.POINTER(Mat4)]
+        L.cf_tsdf_integrate.argtypes = [vp, ctypes.POINTER(TsdfParams), vp, ctypes.POINTER(Camera),
+                                        ctypes.POINTER(Mat4), vp, vp, i, vp, vp, vp, i, vp, vp]
+        L.cf_tsdf_warp_voxel_centres.argtypes = [vp, ctypes.POINTER(TsdfParams), vp, vp, i, vp, vp, vp, vp]
+        L.cf_mark_optimized_voxels.argtypes = [vp, vp, i, ctypes.POINTER(ctypes.c_int * 3), i, vp, vp, vp]
         L.cf_get_version.argtypes = [ctypes.POINTER(i)] * 3
         L.cf_last_cuda_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
         for name in EXPORTS:

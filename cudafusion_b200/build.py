@@ -11,7 +11,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcfb200.so")
 SOURCES = ["cf_api.cu", "cf_kernels.cu", "cf_assemble.cu", "cf_pcg_grid.cu", "cf_pcg_cluster.cu", "cf_pcg_stream.cu",
            "cf_mpnn.cu", "cf_noalloc.cu", "cf_corr.cu",
-           "cf_raster.cu", "cf_linesearch.cu"]
+           "cf_raster.cu", "cf_linesearch.cu", "cf_tsdf.cu"]
 HEADERS = ["cf_device.cuh", "cf_internal.h", os.path.join("..", "..", "include", "cudafusion_b200.h")]
 
 NVCC_FLAGS = [

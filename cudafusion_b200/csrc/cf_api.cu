@@ -2041,6 +2041,127 @@ cf_status cf_line_search(cf_raster* raster, cf_corr_search* search, const float*
   return CF_OK;
 }
 
+// ---- warped TSDF integration ----
+
+namespace {
+
+bool tsdf_voxels(const cf_tsdf_params* p, unsigned* V) {
+  if (!p) return false;
+  long long n = 1;
+  for (int a = 0; a < 3; ++a) {
+    if (p->dims[a] < 0) return false;
+    n *= p->dims[a];
+    if (n >= (1LL << 31)) return false;
+  }
+  *V = (unsigned)n;
+  return true;
+}
+
+// src/tsdf_volume.cu:34-50: R^T and -(R^T t), each sum of products taken left
+// to right with every product and sum rounded (the reference's host build).
+void world_to_camera(const cf_mat4& pose, float* rows) {
+  float m[3][4];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) m[i][j] = pose.m[j][i];
+  for (int i = 0; i < 3; ++i) {
+    volatile float a = m[i][0] * pose.m[0][3];
+    volatile float b = m[i][1] * pose.m[1][3];
+    volatile float c = m[i][2] * pose.m[2][3];
+    volatile float ab = a + b;
+    volatile float abc = ab + c;
+    m[i][3] = -abc;
+  }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 4; ++j) rows[4 * i + j] = m[i][j];
+}
+
+}  // namespace
+
+cf_status cf_tsdf_reset(cf_tsdf_voxel* d_voxels, long long num_voxels, void* stream) {
+  if (num_voxels < 0 || num_voxels >= (1LL << 31) || (num_voxels > 0 && !d_voxels)) return CF_ERR_INVALID_ARG;
+  CF_TRY(launch_tsdf_init(d_voxels, (unsigned)num_voxels, (cudaStream_t)stream));
+  return CF_OK;
+}
+
+cf_status cf_tsdf_world_to_camera(const cf_mat4* camera_pose, cf_mat4* T_cam_world) {
+  if (!camera_pose || !T_cam_world) return CF_ERR_INVALID_ARG;
+  float rows[12];
+  world_to_camera(*camera_pose, rows);
+  cf_mat4 out;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 4; ++j) out.m[i][j] = rows[4 * i + j];
+  out.m[3][0] = out.m[3][1] = out.m[3][2] = 0.f;
+  out.m[3][3] = 1.f;
+  *T_cam_world = out;
+  return CF_OK;
+}
+
+cf_status cf_tsdf_integrate(cf_tsdf_voxel* d_voxels, const cf_tsdf_params* params, const float* d_depth,
+                            const cf_camera* cam, const cf_mat4* camera_pose, const cf_deform_node* d_nodes,
+                            const cf_dual_quat* d_transforms, int num_nodes, const int* d_voxel_knn,
+                            const float* d_voxel_knn_w, const int* d_voxel_opt_counts, int min_opt_count,
+                            cf_dual_quat* d_scratch_plain, void* stream) {
+  unsigned V = 0;
+  if (!tsdf_voxels(params, &V) || !cam || !camera_pose || num_nodes < 0) return CF_ERR_INVALID_ARG;
+  if (V == 0) return CF_OK;
+  if (!d_voxels || !d_depth || cam->width < 0 || cam->height < 0) return CF_ERR_INVALID_ARG;
+  if ((reinterpret_cast<uintptr_t>(d_voxels) | reinterpret_cast<uintptr_t>(d_depth)) & 3u) return CF_ERR_INVALID_ARG;
+  // TSDFVolume::integrate: use_warp = (nodes != nullptr && num_nodes > 0)
+  const bool warp = d_nodes != nullptr && num_nodes > 0;
+  if (warp) {
+    if (!d_transforms || !d_voxel_knn || !d_voxel_knn_w || !d_scratch_plain) return CF_ERR_INVALID_ARG;
+    if ((reinterpret_cast<uintptr_t>(d_voxel_knn) | reinterpret_cast<uintptr_t>(d_voxel_knn_w) |
+         reinterpret_cast<uintptr_t>(d_transforms) | reinterpret_cast<uintptr_t>(d_scratch_plain)) & 15u)
+      return CF_ERR_INVALID_ARG;
+    if (d_voxel_opt_counts && (reinterpret_cast<uintptr_t>(d_voxel_opt_counts) & 3u)) return CF_ERR_INVALID_ARG;
+  }
+  float rows[12];
+  world_to_camera(*camera_pose, rows);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (warp) CF_TRY(launch_tsdf_plain(d_nodes, d_transforms, d_scratch_plain, num_nodes, s));
+  CF_TRY(launch_tsdf_integrate(reinterpret_cast<float*>(d_voxels), params, d_depth, cam, rows,
+                               warp ? d_voxel_knn : nullptr, warp ? d_voxel_knn_w : nullptr,
+                               warp ? d_scratch_plain : nullptr, warp ? num_nodes : 0,
+                               warp ? d_voxel_opt_counts : nullptr, min_opt_count, s));
+  return CF_OK;
+}
+
+cf_status cf_tsdf_warp_voxel_centres(float* d_points, const cf_tsdf_params* params, const cf_deform_node* d_nodes,
+                                     const cf_dual_quat* d_transforms, int num_nodes, const int* d_voxel_knn,
+                                     const float* d_voxel_knn_w, cf_dual_quat* d_scratch_plain, void* stream) {
+  unsigned V = 0;
+  if (!tsdf_voxels(params, &V) || num_nodes < 0) return CF_ERR_INVALID_ARG;
+  if (V == 0) return CF_OK;
+  if (!d_points) return CF_ERR_INVALID_ARG;
+  const bool warp = d_nodes != nullptr && num_nodes > 0;
+  if (warp && (!d_transforms || !d_voxel_knn || !d_voxel_knn_w || !d_scratch_plain ||
+               ((reinterpret_cast<uintptr_t>(d_voxel_knn) | reinterpret_cast<uintptr_t>(d_voxel_knn_w) |
+                 reinterpret_cast<uintptr_t>(d_transforms) | reinterpret_cast<uintptr_t>(d_scratch_plain)) & 15u)))
+    return CF_ERR_INVALID_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (warp) CF_TRY(launch_tsdf_plain(d_nodes, d_transforms, d_scratch_plain, num_nodes, s));
+  CF_TRY(launch_tsdf_centres(d_points, params, warp ? d_voxel_knn : nullptr, warp ? d_voxel_knn_w : nullptr,
+                             warp ? d_scratch_plain : nullptr, warp ? num_nodes : 0, s));
+  return CF_OK;
+}
+
+cf_status cf_mark_optimized_voxels(const cf_correspondence* d_corrs, const int* d_canonical_vidx, int num_pixels,
+                                   const int dims[3], int frame_id, int* d_voxel_opt_counts, int* d_voxel_opt_frame,
+                                   void* stream) {
+  if (!dims || num_pixels < 0) return CF_ERR_INVALID_ARG;
+  long long n = 1;
+  for (int a = 0; a < 3; ++a) {
+    if (dims[a] <= 0) return CF_ERR_INVALID_ARG;
+    n *= dims[a];
+    if (n >= (1LL << 31)) return CF_ERR_INVALID_ARG;
+  }
+  if (num_pixels == 0) return CF_OK;
+  if (!d_corrs || !d_canonical_vidx || !d_voxel_opt_counts || !d_voxel_opt_frame) return CF_ERR_INVALID_ARG;
+  CF_TRY(launch_mark_optimized(d_corrs, d_canonical_vidx, num_pixels, dims, frame_id, d_voxel_opt_counts,
+                               d_voxel_opt_frame, (cudaStream_t)stream));
+  return CF_OK;
+}
+
 cf_status cf_get_version(int* major, int* minor, int* patch) {
   if (major) *major = 0;
   if (minor) *minor = 1;

@@ -256,6 +256,16 @@ cudaError_t launch_scale_delta(const float* dx, int N, float max_rot, float max_
                                cudaStream_t s);
 cudaError_t launch_corr_rmse(const cf_correspondence* corrs, int M, double* partials, double* out, const int* valid,
                              cudaStream_t s);
+cudaError_t launch_tsdf_plain(const cf_deform_node* nodes, const cf_dual_quat* T, cf_dual_quat* plain, int N,
+                              cudaStream_t s);
+cudaError_t launch_tsdf_integrate(float* vox, const cf_tsdf_params* p, const float* depth, const cf_camera* cam,
+                                  const float* cw, const int* knn, const float* knn_w, const cf_dual_quat* plain,
+                                  int N, const int* counts, int min_opt, cudaStream_t s);
+cudaError_t launch_tsdf_centres(float* out, const cf_tsdf_params* p, const int* knn, const float* knn_w,
+                                const cf_dual_quat* plain, int N, cudaStream_t s);
+cudaError_t launch_mark_optimized(const cf_correspondence* corrs, const int* vidx, int P, const int dims[3],
+                                  int frame, int* counts, int* frames, cudaStream_t s);
+cudaError_t launch_tsdf_init(cf_tsdf_voxel* vox, unsigned V, cudaStream_t s);
 // cf_raster.cu: live-surface prediction
 cudaError_t launch_mesh_skin(const float* canon, float* warped, int V, const cf_voxel_grid* grid,
                              const cf_deform_node* nodes, const cf_dual_quat* T, int N, const int* vk, const float* vw,

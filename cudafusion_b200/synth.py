@@ -900,3 +900,128 @@ def mesh_frame(width=640, height=480, n_theta=256, n_axial=160, bend_deg=30.0, c
         meta=dict(kind="cylinders-mesh", seed=seed, width=width, height=height, vertices=int(canon.shape[0]),
                   triangles=int(tris.shape[0]), grid_voxels=G, num_nodes=int(node_pos.shape[0]),
                   bend_deg=bend_deg))
+
+
+@dataclass
+class TsdfFrame:
+    """The inputs of one warped TSDF integration (TSDFVolume::integrate,
+    src/tsdf_volume.cu:23-60, as DynamicFusionPipeline calls it,
+    include/fusion_app.h:655-666): the volume's parameters and prior state,
+    the depth frame and camera pose, the deformation graph with every voxel's
+    node list, and the voxels' optimisation counts."""
+
+    params: dict  # dims, origin, voxel_size, truncation, decay_alpha, max_weight
+    width: int
+    height: int
+    cam: np.ndarray  # float32[4]: fx, fy, cx, cy
+    camera_pose: np.ndarray  # float32[4, 4]: camera -> world
+    depth: np.ndarray  # float32[H * W], metres; 0 = none
+    voxels: np.ndarray  # float32[V, 3]: tsdf, weight, colour bytes
+    nodes: np.ndarray  # NODE_DTYPE[N]
+    transforms: np.ndarray  # DQ_DTYPE[N]: node-centred
+    voxel_knn: np.ndarray  # int32[V, 4]
+    voxel_knn_w: np.ndarray  # float32[V, 4]
+    counts: np.ndarray  # int32[V]
+    meta: dict = field(default_factory=dict)
+
+
+def tsdf_frame(width=640, height=480, dims=(256, 256, 256), extent=1.536, origin=(-0.768, -0.768, 0.5),
+               truncation_voxels=5.0, nodes_xy=(48, 36), knn_band_voxels=None, cam_rot_deg=0.8,
+               cam_trans=(0.004, -0.003, 0.002), warp_rot_deg=3.0, warp_trans=0.01, holes=True, invalid_frac=0.0,
+               seed=21):
+    """A depth frame of a smooth bumpy surface about 1.1 m in front of the
+    camera, inside a volume of `dims` voxels spanning `extent` metres along x
+    from `origin` (the reference's 256^3 x 6 mm at the defaults).  The camera
+    pose is a small rigid motion.  Nodes sit on the surface on a
+    nodes_xy lattice of pixels, warped by a smooth field of rotations up to
+    warp_rot_deg and translations up to warp_trans; every voxel within
+    knn_band_voxels of the surface (all voxels when None) holds its 4 nearest
+    nodes weighted as src/warp_field.cu:379-404.  The prior volume holds the
+    truncated surface distance with random weights in the band; counts are
+    random 0..6 in the band and 0 elsewhere.  invalid_frac of the depth
+    pixels are NaN or negative; `holes` zeroes two rectangles."""
+    rng = np.random.default_rng(seed)
+    dims = np.asarray(dims, np.int32)
+    vs = float(np.float32(extent / float(dims[0])))
+    trunc = float(np.float32(truncation_voxels * vs))
+    s = width / 640.0
+    fx = fy = 570.342 * s
+    cx, cy = width / 2.0, height / 2.0
+    u, v = np.meshgrid(np.arange(width, dtype=np.float64), np.arange(height, dtype=np.float64))
+    z = 1.1 + 0.12 * np.sin(2 * np.pi * 1.5 * u / width) * np.cos(2 * np.pi * v / height) + 0.06 * (u / width)
+    depth = z.copy()
+    if holes:
+        depth[height // 5: height // 5 + height // 8, width // 6: width // 6 + width // 7] = 0.0
+        depth[3 * height // 5: 3 * height // 5 + height // 10, 3 * width // 5: 3 * width // 5 + width // 9] = 0.0
+    depth = depth.reshape(-1)
+    if invalid_frac > 0:
+        bad = rng.random(depth.size) < invalid_frac
+        depth[bad] = np.where(rng.random(int(bad.sum())) < 0.5, np.nan, -0.5)
+    axis = rng.normal(size=3)
+    axis /= np.linalg.norm(axis)
+    pose = np.eye(4)
+    pose[:3, :3] = _rotmat(quat_from_rotvec(axis * np.deg2rad(cam_rot_deg)))
+    pose[:3, 3] = cam_trans
+    # surface points (world) and the nodes on a pixel lattice
+    pc = np.stack([z * (u - cx) / fx, z * (v - cy) / fy, z], -1)
+    nu, nv = nodes_xy
+    iu = np.linspace(0.04 * width, 0.96 * width, nu).astype(int)
+    iv = np.linspace(0.04 * height, 0.96 * height, nv).astype(int)
+    npc = pc[iv[:, None], iu[None, :]].reshape(-1, 3)
+    node_pos = npc @ pose[:3, :3].T + pose[:3, 3]
+    spacing = np.median(np.linalg.norm(np.diff(pc[iv[nv // 2], iu], axis=0), axis=-1))
+    h = 1.5 * spacing
+    nb, nw, kc = _graph(node_pos, h)
+    nodes = _make_nodes(node_pos, np.zeros_like(node_pos), h, nb, nw, kc)
+    rv = _smooth_field(rng, node_pos, np.deg2rad(warp_rot_deg), 0.5)
+    tn = _smooth_field(rng, node_pos, warp_trans, 0.5)
+    transforms = centred_dq(quat_from_rotvec(rv), tn)
+    # voxel centres (float64; the generator's own), their camera depth and
+    # the surface distance along the ray through their pixel
+    V = int(np.prod(dims.astype(np.int64)))
+    org = np.asarray(origin, np.float64)
+    knn = np.full((V, K_NEIGHBORS), -1, np.int32)
+    knn_w = np.zeros((V, K_NEIGHBORS), np.float32)
+    vox = np.zeros((V, 3), np.float32)
+    vox[:, 0] = 1.0
+    vox.view(np.uint32)[:, 2] = 0x00808080
+    counts = np.zeros(V, np.int32)
+    Rcw = pose[:3, :3].T
+    tcw = -Rcw @ pose[:3, 3]
+    tree = cKDTree(node_pos)
+    plane = int(dims[0]) * int(dims[1])
+    gx, gy = np.meshgrid(np.arange(dims[0]), np.arange(dims[1]))
+    gx, gy = gx.reshape(-1), gy.reshape(-1)
+    band = None if knn_band_voxels is None else knn_band_voxels * vs
+    for zi in range(int(dims[2])):
+        c = np.stack([org[0] + (gx + 0.5) * vs, org[1] + (gy + 0.5) * vs,
+                      np.full(gx.shape, org[2] + (zi + 0.5) * vs)], -1)
+        p = c @ Rcw.T + tcw
+        with np.errstate(divide="ignore", invalid="ignore"):
+            pu = np.rint(fx * p[:, 0] / p[:, 2] + cx)
+            pv = np.rint(fy * p[:, 1] / p[:, 2] + cy)
+        ok = (p[:, 2] > 0) & (pu >= 0) & (pu < width) & (pv >= 0) & (pv < height)
+        sdf = np.full(gx.shape, np.inf)
+        idx = (np.where(ok, pv, 0) * width + np.where(ok, pu, 0)).astype(np.int64)
+        sdf[ok] = z.reshape(-1)[idx[ok]] - p[ok, 2]
+        near = np.abs(sdf) < band if band is not None else np.ones(gx.shape, bool)
+        sl = slice(zi * plane, (zi + 1) * plane)
+        if near.any():
+            ids, ws = _skin_weights(c[near], node_pos, h, tree)
+            knn[sl][near] = ids
+            knn_w[sl][near] = ws
+        inb = np.abs(sdf) < 3 * trunc
+        if inb.any():
+            vt = vox[sl]
+            vt[inb, 0] = np.clip(sdf[inb] / trunc, -1.0, 1.0)
+            vt[inb, 1] = rng.uniform(0.0, 50.0, int(inb.sum()))
+            vox[sl] = vt
+            ct = counts[sl]
+            ct[inb] = rng.integers(0, 7, int(inb.sum()))
+            counts[sl] = ct
+    params = dict(dims=dims, origin=np.asarray(origin, np.float32), voxel_size=vs, truncation=trunc,
+                  decay_alpha=0.9, max_weight=50.0)
+    return TsdfFrame(params=params, width=width, height=height, cam=np.array([fx, fy, cx, cy], np.float32),
+                     camera_pose=pose.astype(np.float32), depth=depth.astype(np.float32), voxels=vox, nodes=nodes,
+                     transforms=transforms, voxel_knn=knn, voxel_knn_w=knn_w, counts=counts,
+                     meta=dict(node_radius=h, band_voxels=int((counts > 0).sum())))

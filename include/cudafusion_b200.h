@@ -659,6 +659,80 @@ CF_API cf_status cf_line_search(cf_raster* raster, cf_corr_search* search, const
                                 float* d_scratch_delta, double* d_scratch_rmse, float* best_scale,
                                 double* best_rmse, double* trial_rmse, int* trial_valid, void* stream);
 
+/* ------------------------------------------------------------------------ */
+/* Warped TSDF integration: TSDFVolume::integrate (src/tsdf_volume.cu:23-60,  */
+/* include/tsdf_volume.h:27-35) with tsdf_integrate_kernel                    */
+/* (kernels/tsdf_kernels.cu:85-174), and the gate's counts,                   */
+/* mark_optimized_voxels (include/fusion_app.h:1321-1328,                     */
+/* kernels/tsdf_kernels.cu:606-650).                                          */
+/* ------------------------------------------------------------------------ */
+
+/* TSDFVoxel, include/types.h:168-176 (12 bytes; a new voxel is tsdf 1,
+ * weight 0, colour 128 128 128). */
+typedef struct cf_tsdf_voxel {
+  float tsdf;
+  float weight;
+  uint8_t color[3];
+  uint8_t pad;
+} cf_tsdf_voxel;
+
+/* TSDFVolume::Params, include/tsdf_volume.h:10-19 (stock: 256^3, 0.006 m,
+ * truncation 0.03 m, origin (-0.768, -0.768, 0.5), decay 0.9, cap 50).
+ * Voxel (x, y, z) has index (z * dims[1] + y) * dims[0] + x and centre
+ * origin + (v + 0.5) voxel_size. */
+typedef struct cf_tsdf_params {
+  int dims[3];
+  float voxel_size;
+  float truncation;
+  float origin[3];
+  float decay_alpha; /* the old weight is multiplied by this before an update */
+  float max_weight;  /* the updated weight is capped here */
+} cf_tsdf_params;
+
+/* The TSDFVolume constructor's initial state (src/tsdf_volume.cu:11-19) for
+ * num_voxels voxels.  Asynchronous on `stream`. */
+CF_API cf_status cf_tsdf_reset(cf_tsdf_voxel* d_voxels, long long num_voxels, void* stream);
+
+/* T_cam_world as TSDFVolume::integrate forms it from camera_pose (the
+ * transposed rotation and -R^T t, src/tsdf_volume.cu:34-50); the bottom row
+ * is 0 0 0 1. */
+CF_API cf_status cf_tsdf_world_to_camera(const cf_mat4* camera_pose, cf_mat4* T_cam_world);
+
+/* TSDFVolume::integrate: the depth map (cam->width x cam->height, metres,
+ * <= 0 = none) is fused into d_voxels (params->dims voxels) seen from
+ * camera_pose (camera -> world).  With nodes (d_nodes, d_transforms and
+ * num_nodes > 0) each voxel centre is warped by the CF_K_NEIGHBORS entries of
+ * its d_voxel_knn / d_voxel_knn_w lists (both 16-byte aligned) and, when
+ * d_voxel_opt_counts is given, a voxel whose count is below min_opt_count is
+ * skipped; without nodes the integration is rigid (KinectFusion) and the
+ * lists and counts are not read.  d_scratch_plain holds num_nodes dual
+ * quaternions of the caller's device scratch (may be NULL without nodes).
+ * Only tsdf and weight are written.  The volume must have fewer than 2^31
+ * voxels.  FP32 with IEEE division (the reference's build uses approximate
+ * division: results agree to rounding).  Asynchronous on `stream`. */
+CF_API cf_status cf_tsdf_integrate(cf_tsdf_voxel* d_voxels, const cf_tsdf_params* params, const float* d_depth,
+                                   const cf_camera* cam, const cf_mat4* camera_pose, const cf_deform_node* d_nodes,
+                                   const cf_dual_quat* d_transforms, int num_nodes, const int* d_voxel_knn,
+                                   const float* d_voxel_knn_w, const int* d_voxel_opt_counts, int min_opt_count,
+                                   cf_dual_quat* d_scratch_plain, void* stream);
+
+/* The warped voxel centres cf_tsdf_integrate projects (3 floats per voxel,
+ * index order into d_points); with num_nodes == 0 the canonical centres.
+ * Asynchronous on `stream`. */
+CF_API cf_status cf_tsdf_warp_voxel_centres(float* d_points, const cf_tsdf_params* params,
+                                            const cf_deform_node* d_nodes, const cf_dual_quat* d_transforms,
+                                            int num_nodes, const int* d_voxel_knn, const float* d_voxel_knn_w,
+                                            cf_dual_quat* d_scratch_plain, void* stream);
+
+/* mark_optimized_voxels_kernel: every pixel with a valid correspondence of
+ * weight > 0 and a canonical voxel d_canonical_vidx[px] >= 0 marks the voxels
+ * of the 3x3x3 block around it inside the grid (dims): a voxel whose
+ * d_voxel_opt_frame differs from frame_id takes frame_id and its
+ * d_voxel_opt_counts rises by one.  Asynchronous on `stream`. */
+CF_API cf_status cf_mark_optimized_voxels(const cf_correspondence* d_corrs, const int* d_canonical_vidx,
+                                          int num_pixels, const int dims[3], int frame_id,
+                                          int* d_voxel_opt_counts, int* d_voxel_opt_frame, void* stream);
+
 /* Library / device information. */
 CF_API cf_status cf_get_version(int* major, int* minor, int* patch);
 CF_API cf_status cf_last_cuda_error(char* buf, size_t len);

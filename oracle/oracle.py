@@ -335,3 +335,81 @@ def corr_rmse(recs):
     f(_p(r), r.shape[0], _p(out))
     rmse = float(np.sqrt(out[0] / out[1])) if out[1] > 0 else float("inf")
     return float(out[0]), float(out[1]), rmse
+
+
+# ---- warped TSDF integration (oracle/cf_oracle_tsdf.c) ----
+
+
+def _tsdf_fn(name, restype, argtypes):
+    f = getattr(lib(), name)
+    f.restype = restype
+    f.argtypes = argtypes
+    return f
+
+
+def tsdf_reset(num_voxels):
+    """The TSDFVolume constructor's voxels (src/tsdf_volume.cu:11-19): float32 (n, 3), the third
+    column the colour bytes 128 128 128 0."""
+    vox = np.zeros((num_voxels, 3), np.float32)
+    _tsdf_fn("cfo_tsdf_reset", None, [ctypes.c_void_p, ctypes.c_longlong])(_p(vox), num_voxels)
+    return vox
+
+
+def tsdf_world_to_camera(camera_pose):
+    """T_cam_world as src/tsdf_volume.cu:34-50 forms it: a 4x4 float32 matrix."""
+    pose = np.ascontiguousarray(camera_pose, np.float32)
+    rows = np.zeros(12, np.float32)
+    _tsdf_fn("cfo_tsdf_world_to_camera", None, [ctypes.c_void_p, ctypes.c_void_p])(_p(pose), _p(rows))
+    out = np.eye(4, dtype=np.float32)
+    out[:3] = rows.reshape(3, 4)
+    return out
+
+
+def tsdf_centres(dims, origin, voxel_size, lo=0, hi=None):
+    """The centres of voxels [lo, hi) (kernels/tsdf_kernels.cu:117-121), float32 (n, 3)."""
+    dims = np.ascontiguousarray(dims, np.int32)
+    hi = int(np.prod(dims.astype(np.int64))) if hi is None else hi
+    org = np.ascontiguousarray(origin, np.float32)
+    out = np.zeros((hi - lo, 3), np.float32)
+    _tsdf_fn("cfo_tsdf_centres", None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, ctypes.c_longlong,
+                                        ctypes.c_longlong, ctypes.c_void_p])(_p(dims), _p(org), voxel_size, lo, hi,
+                                                                              _p(out))
+    return out
+
+
+def tsdf_integrate(vox, params, depth, cam, camera_pose, live=None, counts=None, gate=False, min_opt=0, lo=0,
+                   hi=None):
+    """tsdf_integrate_kernel (kernels/tsdf_kernels.cu:85-174) over voxels [lo, hi) of `vox`
+    (float32 (n, 3), updated in place).  params = dict(dims, origin, voxel_size, truncation,
+    decay_alpha, max_weight); cam = (fx, fy, cx, cy, width, height); live = the warped centres of
+    the range (None: rigid).  Returns the number of voxels updated."""
+    dims = np.ascontiguousarray(params["dims"], np.int32)
+    hi = vox.shape[0] if hi is None else hi
+    org = np.ascontiguousarray(params["origin"], np.float32)
+    rows = np.ascontiguousarray(tsdf_world_to_camera(camera_pose)[:3].reshape(-1))
+    c = np.array(cam[:4], np.float32)
+    d = np.ascontiguousarray(depth, np.float32).reshape(-1)
+    lv = None if live is None else np.ascontiguousarray(live, np.float32)
+    cn = None if counts is None else np.ascontiguousarray(counts, np.int32)
+    assert vox.dtype == np.float32 and vox.flags.c_contiguous
+    f = _tsdf_fn("cfo_tsdf_integrate", ctypes.c_longlong,
+                 [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_void_p,
+                  ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                  ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_longlong, ctypes.c_longlong])
+    return f(_p(vox), _p(dims), _p(org), params["voxel_size"], params["truncation"], _p(d), int(cam[4]), int(cam[5]),
+             _p(c), _p(rows), _p(lv), _p(cn), int(bool(gate)), min_opt, params["decay_alpha"], params["max_weight"],
+             lo, hi)
+
+
+def mark_optimized_voxels(recs, vidx_map, dims, frame, counts, frames):
+    """mark_optimized_voxels_kernel (kernels/tsdf_kernels.cu:606-650) on the correspondence records;
+    counts and frames (int32) are updated in place."""
+    valid = np.ascontiguousarray(recs["valid"], np.uint8)
+    weight = np.ascontiguousarray(recs["weight"], np.float32)
+    vm = np.ascontiguousarray(vidx_map, np.int32)
+    dims = np.ascontiguousarray(dims, np.int32)
+    assert counts.dtype == np.int32 and frames.dtype == np.int32
+    _tsdf_fn("cfo_mark_optimized_voxels", None,
+             [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+              ctypes.c_void_p, ctypes.c_void_p])(_p(valid), _p(weight), _p(vm), vm.size, _p(dims), frame, _p(counts),
+                                                 _p(frames))
