@@ -336,4 +336,69 @@ class LiveSurfaceRaster {
   cf_raster* h_ = nullptr;
 };
 
+// TSDFVolume::integrate (src/tsdf_volume.cu:23-60) over a volume the caller
+// owns (TSDFVolume::device_data(), the reference's 12-byte TSDFVoxel), and
+// DynamicFusionPipeline::mark_optimized_voxels (include/fusion_app.h:1321-1328).
+// Holds the per-node scratch of up to max_nodes dual quaternions; synchronises,
+// as the reference does.
+class TSDFIntegrator {
+ public:
+  explicit TSDFIntegrator(int max_nodes) : cap_(max_nodes) {
+    if (max_nodes < 0) check(CF_ERR_INVALID_ARG, "TSDFIntegrator");
+    int devices = 0;
+    if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0) {
+      cudaGetLastError();
+      check(CF_ERR_NO_DEVICE, "TSDFIntegrator");
+    }
+    if (cap_ > 0 && cudaMalloc(&plain_, sizeof(cf_dual_quat) * (size_t)cap_) != cudaSuccess) {
+      cudaGetLastError();
+      check(CF_ERR_OOM, "TSDFIntegrator");
+    }
+  }
+  ~TSDFIntegrator() { cudaFree(plain_); }
+  TSDFIntegrator(const TSDFIntegrator&) = delete;
+  TSDFIntegrator& operator=(const TSDFIntegrator&) = delete;
+
+  // Params = TSDFVolume::Params (include/tsdf_volume.h:10-19); nodes == nullptr
+  // or num_nodes == 0 integrates rigidly.
+  template <class Voxel, class Params, class Cam, class M4, class Node = cf_deform_node, class DQ = cf_dual_quat>
+  void integrate(Voxel* d_voxels, const Params& params, const float* d_depth, const Cam& cam, const M4& camera_pose,
+                 const Node* d_nodes = nullptr, const DQ* d_transforms = nullptr, int num_nodes = 0,
+                 const int* d_voxel_knn = nullptr, const float* d_voxel_knn_w = nullptr,
+                 const int* d_voxel_opt_counts = nullptr, int min_opt_count = 0) {
+    static_assert(sizeof(Voxel) == sizeof(cf_tsdf_voxel) && sizeof(Params) == sizeof(cf_tsdf_params),
+                  "TSDFVoxel / TSDFVolume::Params layouts");
+    static_assert(sizeof(Node) == sizeof(cf_deform_node) && sizeof(DQ) == sizeof(cf_dual_quat) &&
+                      sizeof(Cam) == sizeof(cf_camera) && sizeof(M4) == sizeof(cf_mat4),
+                  "DeformNode / DualQuat / CameraIntrinsics / Mat4 layouts");
+    if (d_nodes && num_nodes > cap_) check(CF_ERR_CAPACITY, "TSDFVolume::integrate");
+    check(cf_tsdf_integrate(reinterpret_cast<cf_tsdf_voxel*>(d_voxels),
+                            reinterpret_cast<const cf_tsdf_params*>(&params), d_depth,
+                            reinterpret_cast<const cf_camera*>(&cam), reinterpret_cast<const cf_mat4*>(&camera_pose),
+                            reinterpret_cast<const cf_deform_node*>(d_nodes),
+                            reinterpret_cast<const cf_dual_quat*>(d_transforms), num_nodes, d_voxel_knn,
+                            d_voxel_knn_w, d_voxel_opt_counts, min_opt_count, plain_, nullptr),
+          "TSDFVolume::integrate");
+    if (cudaDeviceSynchronize() != cudaSuccess) check(CF_ERR_CUDA, "TSDFVolume::integrate");
+  }
+
+  // mark_optimized_voxels_kernel; Dims = int3.
+  template <class Corr, class Dims>
+  static void mark_optimized_voxels(const Corr* d_corrs, const int* d_canonical_vidx, int num_pixels,
+                                    const Dims& dims, int frame_id, int* d_voxel_opt_counts,
+                                    int* d_voxel_opt_frame) {
+    static_assert(sizeof(Corr) == sizeof(cf_correspondence) && sizeof(Dims) == 3 * sizeof(int),
+                  "Correspondence / int3 layouts");
+    check(cf_mark_optimized_voxels(reinterpret_cast<const cf_correspondence*>(d_corrs), d_canonical_vidx, num_pixels,
+                                   reinterpret_cast<const int*>(&dims), frame_id, d_voxel_opt_counts,
+                                   d_voxel_opt_frame, nullptr),
+          "mark_optimized_voxels");
+    if (cudaDeviceSynchronize() != cudaSuccess) check(CF_ERR_CUDA, "mark_optimized_voxels");
+  }
+
+ private:
+  int cap_ = 0;
+  cf_dual_quat* plain_ = nullptr;
+};
+
 }  // namespace cudafusion_b200

@@ -88,9 +88,9 @@ def test_dropin_loop_matches_python_mirror(exe, tmp_path):
 
 @pytest.mark.skipif(has_gpu(), reason="checks the no-device error path")
 def test_frontend_classes_compile_and_fail_loudly_without_gpu(cflib, tmp_path):
-    """CorrespondenceSearch and LiveSurfaceRaster compile against the
-    reference's type layouts (-Wall -Werror) and, with no GPU, throw
-    CF_ERR_NO_DEVICE from their constructors."""
+    """CorrespondenceSearch, LiveSurfaceRaster and TSDFIntegrator compile
+    against the reference's type layouts (-Wall -Werror) and, with no GPU,
+    throw CF_ERR_NO_DEVICE from their constructors."""
     out = str(tmp_path / "dropin_frontend")
     src = os.path.join(ROOT, "tests", "cpp", "dropin_frontend.cpp")
     cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
