@@ -196,3 +196,25 @@ def test_oracle_against_reference_golden(oracle):
             assert np.array_equal(c, g[f"c{k}_mark_counts{j + 1}"]) and np.array_equal(fr, g[f"c{k}_mark_frames{j + 1}"])
         k += 1
     assert k >= 2
+
+
+def test_voxel_range_matches_full_volume(oracle):
+    """Integrating voxels [lo, hi) with that range's centres (the form the
+    full-volume GPU test and the CPU baseline use) gives the full run's
+    values there and leaves the rest alone."""
+    f = synth.tsdf_frame(96, 72, dims=(40, 32, 28), nodes_xy=(6, 5), invalid_frac=0.01, seed=67)
+    cen = oracle.tsdf_centres(f.params["dims"], f.params["origin"], f.params["voxel_size"])
+    live = oracle.skin(cen, f.voxel_knn, f.voxel_knn_w, f.nodes, f.transforms, precision="f32")
+    full = f.voxels.copy()
+    oracle.tsdf_integrate(full, f.params, f.depth, _cam(f), f.camera_pose, live=live, counts=f.counts, gate=True,
+                          min_opt=3)
+    plane = 40 * 32
+    lo, hi = 13 * plane, 17 * plane + 5
+    part = f.voxels.copy()
+    n = oracle.tsdf_integrate(part, f.params, f.depth, _cam(f), f.camera_pose, live=live[lo:hi], counts=f.counts,
+                              gate=True, min_opt=3, lo=lo, hi=hi)
+    assert n > 0
+    assert np.array_equal(part[lo:hi].view(np.uint32), full[lo:hi].view(np.uint32))
+    assert np.array_equal(part[:lo], f.voxels[:lo]) and np.array_equal(part[hi:], f.voxels[hi:])
+    assert np.array_equal(oracle.tsdf_centres(f.params["dims"], f.params["origin"], f.params["voxel_size"], lo, hi),
+                          cen[lo:hi])
