@@ -218,3 +218,15 @@ def test_voxel_range_matches_full_volume(oracle):
     assert np.array_equal(part[:lo], f.voxels[:lo]) and np.array_equal(part[hi:], f.voxels[hi:])
     assert np.array_equal(oracle.tsdf_centres(f.params["dims"], f.params["origin"], f.params["voxel_size"], lo, hi),
                           cen[lo:hi])
+
+
+def test_camera_facing_away_updates_nothing(oracle):
+    """Every voxel behind the camera (z <= 0) is skipped: a pose turned 180
+    degrees about y leaves the volume as it was; an empty range does nothing."""
+    f = synth.tsdf_frame(96, 72, dims=(40, 32, 28), nodes_xy=(6, 5), seed=68)
+    pose = f.camera_pose.copy()
+    pose[:3, :3] = pose[:3, :3] @ np.diag([-1.0, 1.0, -1.0]).astype(np.float32)
+    vox = f.voxels.copy()
+    assert oracle.tsdf_integrate(vox, f.params, f.depth, _cam(f), pose) == 0
+    assert np.array_equal(vox, f.voxels)
+    assert oracle.tsdf_integrate(vox, f.params, f.depth, _cam(f), f.camera_pose, lo=5, hi=5) == 0
