@@ -35,11 +35,21 @@ METRIC = "ms/GN solve at 2k nodes/300k corr, learned-init vs plain at equal ener
 L2_FLUSH_BYTES = 256 << 20
 HBM_FALLBACK_GBS = 6650.0
 
-# solve parameters of the workload: GaussNewtonSolver::Params defaults
-# (include/solver.h:15-21) with 5 GN x 20 PCG iterations, and the per-node
-# update clamps of config/params.yaml:45-46 (max_update_rot/trans)
-GN_ITERS, PCG_ITERS, PCG_TOL, LAMBDA_SMOOTH, LAMBDA_DAMP = 5, 20, 1e-4, 1.0, 1e-2
+# solve parameters of the workload: 5 GN x 20 PCG iterations, all of them run
+# (pcg_tolerance 0: the same work on every arm); the ARAP weight of the
+# sphere workload (lambda_smooth 10) and the damping the reference's pipeline
+# runs with (config/params.yaml:29, lambda_damping 1.0), at which the solve
+# converges; the per-node update clamps of config/params.yaml:45-46
+# (max_update_rot/trans)
+GN_ITERS, PCG_ITERS, PCG_TOL, LAMBDA_SMOOTH, LAMBDA_DAMP = 5, 20, 0.0, 10.0, 1.0
 MAX_ROT, MAX_TRANS, UPDATE_SCALE = 0.12, 0.04, 1.0
+# the same frame at the GaussNewtonSolver::Params defaults (include/solver.h:
+# 15-21: lambda_smooth 1, lambda_damping 1e-2, tolerance 1e-4), reported beside
+# the headline: that system is indefinite (skin pairs dropped by find_block,
+# kernels/solver_kernels.cu:25-44) and the GN energy rises in both solvers
+DEFAULTS_KW = dict(gn_iterations=5, pcg_iterations=20, pcg_tolerance=1e-4, lambda_smooth=1.0, lambda_damping=1e-2)
+# repetitions of the timing protocol (median, L2 flushed / warm)
+PROTOCOL_REPS = 50
 
 
 def peaks():
@@ -312,20 +322,81 @@ def precision_study():
     }
 
 
+def headline_kw():
+    return dict(gn_iterations=GN_ITERS, pcg_iterations=PCG_ITERS, pcg_tolerance=PCG_TOL,
+                lambda_smooth=LAMBDA_SMOOTH, lambda_damping=LAMBDA_DAMP)
+
+
+def time_solves(solver, dp, T, reps, stream, flush=None):
+    """Per-solve device times (CUDA events on `stream`, the launching stream)
+    of `reps` graphed solves from the initial transforms; with `flush` the L2
+    is overwritten before every solve, without it the solve runs warm."""
+    import torch
+
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    with torch.cuda.stream(stream):
+        for k in range(reps):
+            T.copy_(dp.init_transforms)
+            if flush is not None:
+                flush.fill_(1)
+            evs[k][0].record(stream)
+            solver.gn_solve(dp, T, MAX_ROT, MAX_TRANS, UPDATE_SCALE, stats=False, stream=stream)
+            evs[k][1].record(stream)
+    stream.synchronize()
+    return [a.elapsed_time(b) for a, b in evs]
+
+
+def fp64_energy(problem, transforms, lambda_smooth):
+    """Checker: the FP64 oracle's energy at `transforms` (host), the same
+    function for every arm's output."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    return float(O.energy(problem, transforms, lambda_smooth, nthreads=os.cpu_count() or 1))
+
+
+def reference_parity(problem, ours_T, kw, runs=3):
+    """Checker leg, outside every timed region: the reference's own solver
+    (oracle/_ref/libcfref_cuda.so) on the same inputs and parameters, `runs`
+    times (its float-atomic assembly is not deterministic); the largest
+    per-component distance of this build's transforms from its runs, its own
+    run-to-run spread, and the FP64 oracle's energy at every output."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_solver as R
+
+    from cudafusion_b200.types import dq_as_array
+
+    if not R.available():
+        return {"unavailable": "oracle/_ref/libcfref_cuda.so was not built (make -C oracle ref)"}
+    ref = R.RefSolver(problem, **kw)
+    Ts = [ref.gn_solve(kw["gn_iterations"], MAX_ROT, MAX_TRANS, UPDATE_SCALE) for _ in range(runs)]
+    ref.close()
+    dist = lambda a, b: float(np.abs(dq_as_array(a) - dq_as_array(b)).max())  # noqa: E731
+    lam = kw["lambda_smooth"]
+    e_ours = fp64_energy(problem, ours_T, lam)
+    e_ref = [fp64_energy(problem, t, lam) for t in Ts]
+    return {
+        "reference_runs": runs,
+        "transform_max_abs_diff": max(dist(ours_T, t) for t in Ts),
+        "reference_spread": max(dist(t, Ts[0]) for t in Ts),
+        "energy_initial_fp64": fp64_energy(problem, problem.init_transforms, lam),
+        "energy_final_fp64": e_ours,
+        "reference_energy_final_fp64": e_ref,
+        "energy_rel_diff_max": max(abs(e_ours - e) / abs(e) for e in e_ref),
+    }
+
+
 def run_b200(args, world, rank, local):
     import torch
 
     from cudafusion_b200 import _lib, synth
     from cudafusion_b200.solver import DeviceProblem, GaussNewtonSolver, Params
+    from cudafusion_b200.types import DQ_DTYPE
 
     problem = synth.config2()
     N, M = problem.num_nodes, problem.num_corrs
-    prm = Params(gn_iterations=GN_ITERS, pcg_iterations=PCG_ITERS, pcg_tolerance=PCG_TOL,
-                 lambda_smooth=LAMBDA_SMOOTH, lambda_damping=LAMBDA_DAMP)
-    solver = GaussNewtonSolver(prm, max_nodes=8192, max_corrs=max(M, 1))
+    solver = GaussNewtonSolver(Params(**headline_kw()), max_nodes=8192, max_corrs=max(M, 1))
     if args.pcg_mode:
-        from cudafusion_b200 import _lib
-
         solver.set_option(_lib.CF_OPT_PCG_MODE, args.pcg_mode)
     dp = DeviceProblem(problem)
     T = dp.init_transforms.clone()
@@ -333,49 +404,36 @@ def run_b200(args, world, rank, local):
     # a non-default stream: the solve's launch sequence runs as a CUDA graph
     side = torch.cuda.Stream()
 
-    def step():
-        T.copy_(dp.init_transforms)
-        flush.fill_(1)
-        solver.gn_solve(dp, T, MAX_ROT, MAX_TRANS, UPDATE_SCALE, stats=False, stream=side)
-
     with torch.cuda.stream(side):
         # set-up, outside the timed region: the autotuner picks the PCG
         # configuration on this problem (unless --pcg-mode fixes it)
         tune = None if args.pcg_mode else solver.autotune([dp], [dp.init_transforms], MAX_ROT, MAX_TRANS,
                                                           UPDATE_SCALE, stream=side)
         stats = solver.gn_solve(dp, T, MAX_ROT, MAX_TRANS, UPDATE_SCALE, stats=True, stream=side)
-        for _ in range(args.warmup):
-            step()
     side.synchronize()
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    T_out = T.cpu().numpy().view(DQ_DTYPE).copy()
+    time_solves(solver, dp, T, args.warmup, side, flush)
     sampler = ClockSampler(local) if rank == 0 else None
     barrier(world)
     if sampler:
         sampler.start()
     launches0 = solver.launch_count()
     t_wall = time.perf_counter()
-    with torch.cuda.stream(side):
-        for k in range(args.steps):
-            T.copy_(dp.init_transforms)
-            flush.fill_(1)
-            evs[k][0].record(side)
-            solver.gn_solve(dp, T, MAX_ROT, MAX_TRANS, UPDATE_SCALE, stats=False, stream=side)
-            evs[k][1].record(side)
-    side.synchronize()
+    per_step = time_solves(solver, dp, T, args.steps, side, flush)
     barrier(world)
     t_wall = time.perf_counter() - t_wall
     clocks = sampler.stop() if sampler else None
     launches = solver.launch_count() - launches0
     graphed = solver.get_option(_lib.CF_OPT_GRAPH_ACTIVE)
-    per_step = [a.elapsed_time(b) for a, b in evs]
     value = replica_value(sum(per_step), args.steps, world)
+    # the timing protocol beside the timed steps: medians of PROTOCOL_REPS
+    # solves with the L2 flushed before each and with the L2 warm
+    cold = time_solves(solver, dp, T, PROTOCOL_REPS, side, flush)
+    warm = time_solves(solver, dp, T, PROTOCOL_REPS, side, None)
     # per-kernel event timing (direct launches: the profiler brackets every
     # launch with events, so this pass runs outside the graph)
     solver.profile_enable(True)
-    with torch.cuda.stream(side):
-        for _ in range(max(3, min(args.steps, 10))):
-            step()
-    side.synchronize()
+    time_solves(solver, dp, T, max(3, min(args.steps, 10)), side, flush)
     phases = solver.profile_read()
     solver.profile_enable(False)
 
@@ -409,6 +467,18 @@ def run_b200(args, world, rank, local):
     h2d = h_nodes.numel() + h_canon.numel() * 4 + h_corrs.numel() + h_T0.numel()
     d2h = h_Tout.numel() + 8 * (2 * 32 + 33) + 4 * 34  # transforms + the stats record + error word
 
+    # the same frame at the solver.h defaults (indefinite system, rising
+    # energy): timed the same way, with its own energies
+    sd = GaussNewtonSolver(Params(**DEFAULTS_KW), max_nodes=8192, max_corrs=max(M, 1))
+    Td = dp.init_transforms.clone()
+    with torch.cuda.stream(side):
+        st_d = sd.gn_solve(dp, Td, MAX_ROT, MAX_TRANS, UPDATE_SCALE, stats=True, stream=side)
+    side.synchronize()
+    Td_out = Td.cpu().numpy().view(DQ_DTYPE).copy()
+    time_solves(sd, dp, Td, 3, side, flush)
+    d_times = time_solves(sd, dp, Td, 10, side, flush)
+    sd.close()
+
     if rank != 0:
         return None
     hbm, peak_kind = peaks()
@@ -433,8 +503,11 @@ def run_b200(args, world, rank, local):
                 "ms_per_launch": dur, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
     nthreads = os.cpu_count() or 1
     cpu = cpu_baseline(problem, nthreads) if not args.no_cpu_baseline else None
+    parity = None if args.no_parity else reference_parity(problem, T_out, headline_kw())
+    parity_d = None if args.no_parity else reference_parity(problem, Td_out, DEFAULTS_KW)
     learned = None if args.no_learned else learned_comparison()
     precision = None if args.no_precision else precision_study()
+    c1 = config1_b200()
     line = {
         "metric": METRIC,
         "value": value,
@@ -453,7 +526,8 @@ def run_b200(args, world, rank, local):
                         f"{GN_ITERS} GN x {PCG_ITERS} PCG, plain init",
             "nodes": N, "corrs": M, "gn_iterations": GN_ITERS, "pcg_iterations": PCG_ITERS,
             "pcg_tolerance": PCG_TOL, "lambda_smooth": LAMBDA_SMOOTH, "lambda_damping": LAMBDA_DAMP,
-            "max_rot": MAX_ROT, "max_trans": MAX_TRANS, "l2": "flushed between steps (256 MiB write)",
+            "arap_jacobian": "the reference's sign", "max_rot": MAX_ROT, "max_trans": MAX_TRANS,
+            "l2": "flushed between steps (256 MiB write)",
             "parallelism": f"replicas x{world}", "blocks": stats["num_blocks"],
         },
         "roofline": roof,
@@ -464,12 +538,27 @@ def run_b200(args, world, rank, local):
         "gpu_launches_per_step": launches / args.steps,
         "cuda_graph": bool(graphed),
         "autotune": tune,
+        "protocol": {"reps": PROTOCOL_REPS, "median_ms_l2_flushed": statistics.median(cold),
+                     "median_ms_l2_warm": statistics.median(warm), "min_ms_l2_flushed": min(cold),
+                     "min_ms_l2_warm": min(warm)},
+        "energy_initial": stats["energy_initial"],
+        "energy_final": stats["energy_final"],
+        "energy_per_gn": stats["energy"],
+        "pcg_iterations": stats["pcg_iterations"],
+        "parity": parity,
+        "solver_h_defaults": {
+            "params": DEFAULTS_KW,
+            "ms_per_solve": statistics.mean(d_times),
+            "energy_per_gn": st_d["energy"],
+            "pcg_iterations": st_d["pcg_iterations"],
+            "parity": parity_d,
+            "note": "indefinite system (skin pairs dropped by find_block): the GN energy rises in both solvers "
+                    "and the reference's own runs land far apart",
+        },
+        "config1": c1,
         "learned": learned,
         "precision": precision,
         "clocks": clocks,
-        "energy_initial": stats["energy_initial"],
-        "energy_final": stats["energy_final"],
-        "pcg_iterations": stats["pcg_iterations"],
         "wall_s_timed_region": t_wall,
     }
     return line
@@ -1386,9 +1475,10 @@ def run_linesearch(args, world, rank, local):
             "timing": "wall clock around the call (it synchronises once, at its read-back); L2 flushed before each",
             "best_scale": res["best_scale"], "trial_valid": res["trial_valid"],
         },
-        "reference_data_flow_ms": statistics.median(host_ms),
-        "reference_data_flow": "the same trials driven as the reference's host loop: a synchronous call per step, "
-                               "the 23 MB of records downloaded per trial and the RMSE summed on the host",
+        "host_loop_order_ms": statistics.median(host_ms),
+        "host_loop_order": "this library's own kernels called in the reference's host-loop order and driven from "
+                           "Python (a synchronous call per step, the 23 MB of records downloaded per trial, the RMSE "
+                           "summed on the host by the oracle): a data-flow comparison, not a reference figure",
         "cpu_baseline": None,
         "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 3 * 8 * 10},
         "gpu_launches": None,
@@ -1396,61 +1486,103 @@ def run_linesearch(args, world, rank, local):
     }
 
 
+# config 1: the small sphere (N=256, M=20k), 5 GN x 10 PCG at lambda_smooth
+# 10 and the solver.h damping, all iterations run (fixed-iteration timing)
+CONFIG1_KW = dict(gn_iterations=5, pcg_iterations=10, pcg_tolerance=0.0, lambda_smooth=10.0, lambda_damping=1e-2)
+
+
+def config1_b200(reps=PROTOCOL_REPS):
+    """Config 1 through this library: median ms per solve, L2 flushed."""
+    import torch
+
+    from cudafusion_b200 import synth
+    from cudafusion_b200.solver import DeviceProblem, GaussNewtonSolver, Params
+
+    p = synth.config1()
+    s = GaussNewtonSolver(Params(**CONFIG1_KW), max_nodes=p.num_nodes, max_corrs=p.num_corrs)
+    dp = DeviceProblem(p)
+    T = dp.init_transforms.clone()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    side = torch.cuda.Stream()
+    time_solves(s, dp, T, 5, side, flush)
+    t = time_solves(s, dp, T, reps, side, flush)
+    s.close()
+    return {"workload": f"sphere, N={p.num_nodes}, M={p.num_corrs}, 5 GN x 10 PCG, lambda_smooth 10, "
+                        "lambda_damping 1e-2", "median_ms": statistics.median(t), "reps": reps,
+            "l2": "flushed before each solve"}
+
+
 def run_reference(args, world, rank, local):
+    """`--impl reference`: CUDAFusion's own solver (GaussNewtonSolver::solve +
+    WarpField::apply_twist_increment + warp_point, kernels/solver_kernels.cu
+    and src/warp_field.cu unmodified, rebuilt for sm_100a with the reference's
+    --use_fast_math) on the same frame and parameters; its final transforms
+    are read back and their FP64 energy reported beside the time."""
     import torch
 
     if rank != 0:
         return None
-    so = os.path.join(ROOT, "oracle", "_ref", "libcfref_cuda.so")
-    if not os.path.exists(so):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_solver as R
+
+    if not R.available():
         return {"impl": "reference", "unavailable": "oracle/_ref/libcfref_cuda.so was not built "
                 "(needs the reference sources: make -C oracle ref)"}
     from cudafusion_b200 import synth
 
-    ref = ctypes.CDLL(so)
-    ref.ref_create.restype = ctypes.c_void_p
-    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
     problem = synth.config2()
     N, M = problem.num_nodes, problem.num_corrs
-    ip = (ctypes.c_int * 3)(GN_ITERS, PCG_ITERS, 0)
-    fp = (ctypes.c_float * 4)(PCG_TOL, LAMBDA_SMOOTH, 1.0, LAMBDA_DAMP)
-    h = ctypes.c_void_p(ref.ref_create(ip, fp, 8192))
-    rc = ref.ref_upload(h, P(problem.nodes), N, P(problem.canon), P(problem.corrs), M, P(problem.init_transforms))
-    if rc != 0:
-        return {"impl": "reference", "unavailable": f"reference upload failed with cudaError {rc}"}
+    kw = headline_kw()
+    ref = R.RefSolver(problem, **kw)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
-    ms = ctypes.c_float()
 
-    def one():
-        ref.ref_set_transforms(h, P(problem.init_transforms), N)
-        flush.fill_(1)
-        torch.cuda.synchronize()
-        rc = ref.ref_gn_solve_timed(h, GN_ITERS, ctypes.c_float(MAX_ROT), ctypes.c_float(MAX_TRANS),
-                                    ctypes.c_float(UPDATE_SCALE), ctypes.byref(ms))
-        if rc != 0:
-            raise RuntimeError(f"reference solve failed with cudaError {rc}")
-        return ms.value
+    def one(r, reps, flush_l2=True):
+        out = []
+        for _ in range(reps):
+            r.set_transforms(r.problem.init_transforms)
+            if flush_l2:
+                flush.fill_(1)
+            torch.cuda.synchronize()
+            out.append(r.gn_solve_timed(r.gn_iters, MAX_ROT, MAX_TRANS, UPDATE_SCALE))
+        return out
 
-    for _ in range(args.warmup):
-        one()
+    ref.gn_iters = GN_ITERS
+    one(ref, args.warmup)
     sampler = ClockSampler(local)
     sampler.start()
-    times = [one() for _ in range(args.steps)]
+    times = one(ref, args.steps)
     clocks = sampler.stop()
     value = sum(times) / len(times)
+    T_out = ref.transforms()
+    cold = one(ref, PROTOCOL_REPS)
+    warm = one(ref, PROTOCOL_REPS, flush_l2=False)
     # end to end: host structs uploaded by the reference's own DeviceArray /
     # WarpField uploads, solve, transforms downloaded
-    Tout = np.zeros(N, problem.init_transforms.dtype)
     e2e = []
     for _ in range(max(3, min(args.steps, 5))):
         flush.fill_(1)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        ref.ref_upload(h, P(problem.nodes), N, P(problem.canon), P(problem.corrs), M, P(problem.init_transforms))
-        ref.ref_gn_solve(h, GN_ITERS, ctypes.c_float(MAX_ROT), ctypes.c_float(MAX_TRANS), ctypes.c_float(UPDATE_SCALE))
-        ref.ref_get_transforms(h, P(Tout), N)
+        ref.upload(problem.init_transforms)
+        ref.gn_solve(GN_ITERS, MAX_ROT, MAX_TRANS, UPDATE_SCALE)
         e2e.append((time.perf_counter() - t0) * 1e3)
+    ref.close()
     h2d = problem.nodes.nbytes + problem.canon.nbytes + problem.corrs.nbytes + 2 * problem.init_transforms.nbytes
+    # the same frame at the solver.h defaults
+    refd = R.RefSolver(problem, **DEFAULTS_KW)
+    refd.gn_iters = DEFAULTS_KW["gn_iterations"]
+    one(refd, 3)
+    d_times = one(refd, 10)
+    Td_out = refd.transforms()
+    refd.close()
+    # config 1, the small sphere
+    p1 = synth.config1()
+    r1 = R.RefSolver(p1, **CONFIG1_KW)
+    r1.gn_iters = CONFIG1_KW["gn_iterations"]
+    one(r1, 5)
+    c1 = one(r1, PROTOCOL_REPS)
+    r1.close()
+    lam, lamd = kw["lambda_smooth"], DEFAULTS_KW["lambda_smooth"]
     return {
         "impl": "reference",
         "metric": METRIC,
@@ -1468,6 +1600,9 @@ def run_reference(args, world, rank, local):
         "config": {
             "workload": f"two-cylinder 640x480 frame, N={N} nodes, M={M} correspondences, "
                         f"{GN_ITERS} GN x {PCG_ITERS} PCG, plain init",
+            "nodes": N, "corrs": M, "gn_iterations": GN_ITERS, "pcg_iterations": PCG_ITERS,
+            "pcg_tolerance": PCG_TOL, "lambda_smooth": LAMBDA_SMOOTH, "lambda_damping": LAMBDA_DAMP,
+            "arap_jacobian": "the reference's sign", "max_rot": MAX_ROT, "max_trans": MAX_TRANS,
             "implementation": "CUDAFusion GaussNewtonSolver::solve + WarpField::apply_twist_increment + warp_point, "
                               "rebuilt for sm_100a with --use_fast_math (oracle/_ref/libcfref_cuda.so)",
             "l2": "flushed between steps (256 MiB write)",
@@ -1477,6 +1612,17 @@ def run_reference(args, world, rank, local):
                          "sample": "the reference path is CUDA: the full solve timed on the GPU, one host thread"},
         "e2e": {"value": statistics.median(e2e), "unit": "ms", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(problem.init_transforms.nbytes)},
+        "protocol": {"reps": PROTOCOL_REPS, "median_ms_l2_flushed": statistics.median(cold),
+                     "median_ms_l2_warm": statistics.median(warm), "min_ms_l2_flushed": min(cold),
+                     "min_ms_l2_warm": min(warm)},
+        "energy_initial_fp64": fp64_energy(problem, problem.init_transforms, lam),
+        "energy_final_fp64": fp64_energy(problem, T_out, lam),
+        "solver_h_defaults": {"params": DEFAULTS_KW, "ms_per_solve": statistics.mean(d_times),
+                              "energy_initial_fp64": fp64_energy(problem, problem.init_transforms, lamd),
+                              "energy_final_fp64": fp64_energy(problem, Td_out, lamd)},
+        "config1": {"workload": f"sphere, N={p1.num_nodes}, M={p1.num_corrs}, 5 GN x 10 PCG, lambda_smooth 10, "
+                                "lambda_damping 1e-2", "median_ms": statistics.median(c1), "reps": PROTOCOL_REPS,
+                    "l2": "flushed before each solve"},
         "clocks": clocks,
     }
 
@@ -1490,6 +1636,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-start comparison")
     ap.add_argument("--no-precision", action="store_true", help="skip the 8192-node precision study")
+    ap.add_argument("--no-parity", action="store_true", help="skip the check against the reference's solver")
     ap.add_argument("--pcg-mode", type=int, default=0, help="0 auto, 1 grid-wide, 2 single cluster, 3 streaming")
     ap.add_argument("--workload", default="frame",
                     choices=["frame", "batch", "learned", "corr", "raster", "linesearch", "tsdf"],
@@ -1511,7 +1658,8 @@ def main():
             line = {"impl": "reference", "unavailable": "the reference's line search is host code inside "
                     "DynamicFusionPipeline (include/fusion_app.h:493-641), which needs OpenCV, Open3D and yaml-cpp "
                     "to build; bench.py --workload linesearch reports the same trials driven the reference's way "
-                    "as reference_data_flow_ms"}
+                    "as host_loop_order_ms (this library's kernels in the reference's host-loop order, not a "
+                    "reference figure)"}
         elif args.impl == "reference" and args.workload == "tsdf":
             line = run_reference_tsdf(args, world, rank, local)
         elif args.workload == "tsdf":

@@ -97,6 +97,7 @@ EXPORTS = [
     "cf_tsdf_integrate",
     "cf_tsdf_warp_voxel_centres",
     "cf_mark_optimized_voxels",
+    "cf_compute_voxel_knn",
     "cf_get_version",
     "cf_last_cuda_error",
 ]
@@ -320,6 +321,7 @@ def lib():
                                         ctypes.POINTER(Mat4), vp, vp, i, vp, vp, vp, i, vp, vp]
         L.cf_tsdf_warp_voxel_centres.argtypes = [vp, ctypes.POINTER(TsdfParams), vp, vp, i, vp, vp, vp, vp]
         L.cf_mark_optimized_voxels.argtypes = [vp, vp, i, ctypes.POINTER(ctypes.c_int * 3), i, vp, vp, vp]
+        L.cf_compute_voxel_knn.argtypes = [vp, ctypes.POINTER(TsdfParams), vp, i, vp, vp, vp]
         L.cf_get_version.argtypes = [ctypes.POINTER(i)] * 3
         L.cf_last_cuda_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
         for name in EXPORTS:

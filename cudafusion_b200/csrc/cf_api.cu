@@ -2145,6 +2145,24 @@ cf_status cf_tsdf_warp_voxel_centres(float* d_points, const cf_tsdf_params* para
   return CF_OK;
 }
 
+cf_status cf_compute_voxel_knn(const cf_tsdf_voxel* d_voxels, const cf_tsdf_params* params,
+                               const cf_deform_node* d_nodes, int num_nodes, int* d_voxel_knn, float* d_voxel_knn_w,
+                               void* stream) {
+  unsigned V = 0;
+  if (!tsdf_voxels(params, &V) || num_nodes < 0) return CF_ERR_INVALID_ARG;
+  // src/warp_field.cu:962-963: no nodes, no launch and the outputs untouched
+  if (V == 0 || num_nodes == 0) return CF_OK;
+  if (num_nodes > voxel_knn_max_nodes()) return CF_ERR_CAPACITY;
+  if (!d_voxels || !d_nodes || !d_voxel_knn || !d_voxel_knn_w) return CF_ERR_INVALID_ARG;
+  if (reinterpret_cast<uintptr_t>(d_voxels) & 3u) return CF_ERR_INVALID_ARG;
+  if ((reinterpret_cast<uintptr_t>(d_voxel_knn) | reinterpret_cast<uintptr_t>(d_voxel_knn_w) |
+       reinterpret_cast<uintptr_t>(d_nodes)) & 15u)
+    return CF_ERR_INVALID_ARG;
+  CF_TRY(launch_voxel_knn(reinterpret_cast<const float*>(d_voxels), params, d_nodes, num_nodes, d_voxel_knn,
+                          d_voxel_knn_w, 0, (cudaStream_t)stream));
+  return CF_OK;
+}
+
 cf_status cf_mark_optimized_voxels(const cf_correspondence* d_corrs, const int* d_canonical_vidx, int num_pixels,
                                    const int dims[3], int frame_id, int* d_voxel_opt_counts, int* d_voxel_opt_frame,
                                    void* stream) {

@@ -266,6 +266,11 @@ cudaError_t launch_tsdf_centres(float* out, const cf_tsdf_params* p, const int* 
 cudaError_t launch_mark_optimized(const cf_correspondence* corrs, const int* vidx, int P, const int dims[3],
                                   int frame, int* counts, int* frames, cudaStream_t s);
 cudaError_t launch_tsdf_init(cf_tsdf_voxel* vox, unsigned V, cudaStream_t s);
+// cf_voxelknn.cu: the voxel kNN field (variant 0: default pruning, 1: tile
+// pruning only, 2: tile and warp pruning)
+int voxel_knn_max_nodes();
+cudaError_t launch_voxel_knn(const float* vox, const cf_tsdf_params* p, const cf_deform_node* nodes, int N,
+                             int* ids, float* ws, int variant, cudaStream_t s);
 // cf_raster.cu: live-surface prediction
 cudaError_t launch_mesh_skin(const float* canon, float* warped, int V, const cf_voxel_grid* grid,
                              const cf_deform_node* nodes, const cf_dual_quat* T, int N, const int* vk, const float* vw,

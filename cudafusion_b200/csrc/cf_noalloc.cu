@@ -97,14 +97,21 @@ __global__ void na_reduce_kernel(const double* __restrict__ part, double* __rest
 
 }  // namespace
 
-// Device address of the static scratch on the current device (looked up once).
-cudaError_t noalloc_scratch(void** out) {
+// Device address of the static scratch on the current device.  Looked up
+// again on every call made outside a stream capture (cheap), so a context
+// torn down and re-created (cudaDeviceReset) never leaves a stale address;
+// inside a capture the address of the last uncaptured call is used.
+cudaError_t noalloc_scratch(cudaStream_t s, void** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(s, &cap);
+  if (e != cudaSuccess) return e;
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_scratch_ptr[dev]) {
+  if (cap == cudaStreamCaptureStatusNone || !g_scratch_ptr[dev]) {
+    if (cap != cudaStreamCaptureStatusNone) return cudaErrorStreamCaptureUnsupported;
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
@@ -117,7 +124,7 @@ cudaError_t noalloc_scratch(void** out) {
 cudaError_t launch_energy_noalloc(const cf_problem* pr, const cf_dual_quat* T, float lambda, double* d_energy,
                                   cudaStream_t s) {
   void* base = nullptr;
-  cudaError_t e = noalloc_scratch(&base);
+  cudaError_t e = noalloc_scratch(s, &base);
   if (e != cudaSuccess) return e;
   cf_dual_quat* plain = reinterpret_cast<cf_dual_quat*>(base);
   double* part = reinterpret_cast<double*>(static_cast<unsigned char*>(base) + kNaPlainBytes);

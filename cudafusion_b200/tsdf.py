@@ -119,6 +119,23 @@ class TSDFVolume:
         return out
 
 
+    def compute_voxel_knn(self, nodes, num_nodes, voxel_knn=None, voxel_knn_w=None, stream=None):
+        """WarpField::compute_voxel_knn (src/warp_field.cu:957-981) over this
+        volume: nodes is the device DeformNode array (uint8, 96 bytes each).
+        Returns (voxel_knn int32 [n*4], voxel_knn_w float32 [n*4]) on the
+        device, allocated here unless given; with no nodes they are returned
+        untouched, as the reference leaves them."""
+        dev = self.voxels.device
+        if voxel_knn is None:
+            voxel_knn = torch.empty(4 * self.n, dtype=torch.int32, device=dev)
+        if voxel_knn_w is None:
+            voxel_knn_w = torch.empty(4 * self.n, dtype=torch.float32, device=dev)
+        check(_lib.lib().cf_compute_voxel_knn(_ptr(self.voxels), ctypes.byref(self._c), _ptr(nodes), int(num_nodes),
+                                              _ptr(voxel_knn), _ptr(voxel_knn_w), _stream_ptr(stream)),
+              "cf_compute_voxel_knn")
+        return voxel_knn, voxel_knn_w
+
+
 def mark_optimized_voxels(corrs, canonical_vidx, num_pixels, dims, frame_id, counts, frames, stream=None):
     """mark_optimized_voxels_kernel: corrs is the device correspondence
     records (uint8, 76 bytes each), canonical_vidx / counts / frames device

@@ -378,10 +378,12 @@ CF_API cf_status cf_gn_solve_learned(cf_gn* h, cf_mpnn* net, const cf_problem* p
  * writes it to *d_energy (device).  Allocates nothing: its scratch is a static
  * device array of this library sized for CF_NOALLOC_MAX_NODES nodes (about
  * 260 KB, held on every GPU that loads the library until exit); larger
- * problems return CF_ERR_CAPACITY.  The first call on a device looks the
- * scratch address up (cudaGetSymbolAddress) and must happen before any stream
- * capture.  Calls share the scratch: calls that overlap on the GPU race and
- * must be serialised by the caller.  Asynchronous on `stream`. */
+ * problems return CF_ERR_CAPACITY.  Every call made outside a stream capture
+ * looks the scratch address up on the current device (cudaGetSymbolAddress),
+ * so a device reset between calls is harmless; the first call on a device
+ * must therefore come before any stream capture (a capturing first call
+ * returns CF_ERR_CUDA).  Calls share the scratch: calls that overlap on the
+ * GPU race and must be serialised by the caller.  Asynchronous on `stream`. */
 #define CF_NOALLOC_MAX_NODES 8192
 CF_API cf_status cf_energy_noalloc(const cf_problem* problem, const cf_dual_quat* d_transforms,
                                    float lambda_smooth, double* d_energy, void* stream);
@@ -732,6 +734,25 @@ CF_API cf_status cf_tsdf_warp_voxel_centres(float* d_points, const cf_tsdf_param
 CF_API cf_status cf_mark_optimized_voxels(const cf_correspondence* d_corrs, const int* d_canonical_vidx,
                                           int num_pixels, const int dims[3], int frame_id,
                                           int* d_voxel_opt_counts, int* d_voxel_opt_frame, void* stream);
+
+/* WarpField::compute_voxel_knn, include/warp_field.h:72-74 and
+ * src/warp_field.cu:957-981, with compute_voxel_knn_kernel (:299-405): the
+ * voxel kNN field of the volume d_voxels (params: dims, origin, voxel_size)
+ * over the num_nodes nodes d_nodes.  For every voxel v (index
+ * (z * dims[1] + y) * dims[0] + x) it writes d_voxel_knn[4v..4v+3] and
+ * d_voxel_knn_w[4v..4v+3]: ids -1 and weights 0 when the voxel's weight is
+ * <= 0; otherwise the 4 nodes with the smallest squared distance to the
+ * centre origin + (v + 0.5) voxel_size, ties to the lower index, nearest
+ * first (-1 / 0 past the number of nodes), each weighted exp(-d / (2 r^2)),
+ * r = max(radius, 1e-6), normalised by their sum when it exceeds 1e-8.  The
+ * ids are the reference's bit for bit; the weights agree to float rounding.
+ * The caller owns both outputs (4 entries per voxel, 16-byte aligned; the
+ * reference reallocates its DeviceArrays here).  num_nodes == 0 writes
+ * nothing, like the reference.  At most 49152 nodes (CF_ERR_CAPACITY).
+ * Asynchronous on `stream`. */
+CF_API cf_status cf_compute_voxel_knn(const cf_tsdf_voxel* d_voxels, const cf_tsdf_params* params,
+                                      const cf_deform_node* d_nodes, int num_nodes, int* d_voxel_knn,
+                                      float* d_voxel_knn_w, void* stream);
 
 /* Library / device information. */
 CF_API cf_status cf_get_version(int* major, int* minor, int* patch);

@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -52,10 +53,73 @@ inline void check(cf_status s, const char* where) {
 #endif
 }
 
+// The caller's DualQuat / DeformNode / Correspondence (include/types.h:86-94,
+// 185-192, 198-206) against the ABI structs: sizes, the DualQuat alignment,
+// and the byte offset of every field, so a reordered or retyped member fails
+// to compile instead of being read at the wrong place.
+template <class Node>
+constexpr bool node_layout_matches() {
+  return sizeof(Node) == sizeof(cf_deform_node) && offsetof(Node, pos) == offsetof(cf_deform_node, pos) &&
+         offsetof(Node, normal) == offsetof(cf_deform_node, normal) &&
+         offsetof(Node, radius) == offsetof(cf_deform_node, radius) &&
+         offsetof(Node, neighbors) == offsetof(cf_deform_node, neighbors) &&
+         offsetof(Node, neighbor_w) == offsetof(cf_deform_node, neighbor_w) &&
+         offsetof(Node, num_neighbors) == offsetof(cf_deform_node, num_neighbors);
+}
+
+template <class DQ>
+constexpr bool dq_layout_matches() {
+  return sizeof(DQ) == sizeof(cf_dual_quat) && alignof(DQ) == alignof(cf_dual_quat) &&
+         offsetof(DQ, real) == offsetof(cf_dual_quat, real) && offsetof(DQ, dual) == offsetof(cf_dual_quat, dual);
+}
+
+template <class Corr>
+constexpr bool corr_layout_matches() {
+  return sizeof(Corr) == sizeof(cf_correspondence) && offsetof(Corr, src) == offsetof(cf_correspondence, src) &&
+         offsetof(Corr, dst) == offsetof(cf_correspondence, dst) &&
+         offsetof(Corr, normal) == offsetof(cf_correspondence, normal) &&
+         offsetof(Corr, node_ids) == offsetof(cf_correspondence, node_ids) &&
+         offsetof(Corr, node_ws) == offsetof(cf_correspondence, node_ws) &&
+         offsetof(Corr, weight) == offsetof(cf_correspondence, weight) &&
+         offsetof(Corr, valid) == offsetof(cf_correspondence, valid);
+}
+
 template <class Node, class DQ, class Corr>
 constexpr bool layouts_match() {
-  return sizeof(Node) == sizeof(cf_deform_node) && sizeof(DQ) == sizeof(cf_dual_quat) &&
-         sizeof(Corr) == sizeof(cf_correspondence) && alignof(DQ) == alignof(cf_dual_quat);
+  return node_layout_matches<Node>() && dq_layout_matches<DQ>() && corr_layout_matches<Corr>();
+}
+
+// CameraIntrinsics (include/types.h:148-162) and Mat4 (:26-60).
+template <class Cam>
+constexpr bool camera_layout_matches() {
+  return sizeof(Cam) == sizeof(cf_camera) && offsetof(Cam, fx) == offsetof(cf_camera, fx) &&
+         offsetof(Cam, fy) == offsetof(cf_camera, fy) && offsetof(Cam, cx) == offsetof(cf_camera, cx) &&
+         offsetof(Cam, cy) == offsetof(cf_camera, cy) && offsetof(Cam, width) == offsetof(cf_camera, width) &&
+         offsetof(Cam, height) == offsetof(cf_camera, height);
+}
+
+template <class M4>
+constexpr bool mat4_layout_matches() {
+  return sizeof(M4) == sizeof(cf_mat4) && offsetof(M4, m) == 0;
+}
+
+// TSDFVoxel (include/types.h:168-176) and TSDFVolume::Params
+// (include/tsdf_volume.h:10-19).
+template <class Voxel>
+constexpr bool voxel_layout_matches() {
+  return sizeof(Voxel) == sizeof(cf_tsdf_voxel) && offsetof(Voxel, tsdf) == offsetof(cf_tsdf_voxel, tsdf) &&
+         offsetof(Voxel, weight) == offsetof(cf_tsdf_voxel, weight) &&
+         offsetof(Voxel, color) == offsetof(cf_tsdf_voxel, color);
+}
+
+template <class Params>
+constexpr bool tsdf_params_layout_matches() {
+  return sizeof(Params) == sizeof(cf_tsdf_params) && offsetof(Params, dims) == offsetof(cf_tsdf_params, dims) &&
+         offsetof(Params, voxel_size) == offsetof(cf_tsdf_params, voxel_size) &&
+         offsetof(Params, truncation) == offsetof(cf_tsdf_params, truncation) &&
+         offsetof(Params, origin) == offsetof(cf_tsdf_params, origin) &&
+         offsetof(Params, decay_alpha) == offsetof(cf_tsdf_params, decay_alpha) &&
+         offsetof(Params, max_weight) == offsetof(cf_tsdf_params, max_weight);
 }
 
 class GaussNewtonSolver {
@@ -166,7 +230,7 @@ class WarpField {
   static constexpr int MAX_NODES = CF_MAX_NODES_DEFAULT;  // include/warp_field.h:14
 
   explicit WarpField(float node_radius, int max_nodes = MAX_NODES) : node_radius_(node_radius), max_nodes_(max_nodes) {
-    static_assert(sizeof(Node) == sizeof(cf_deform_node) && sizeof(DQ) == sizeof(cf_dual_quat), "layouts");
+    static_assert(node_layout_matches<Node>() && dq_layout_matches<DQ>(), "DeformNode / DualQuat layouts");
     check_cuda(cudaMalloc(&d_nodes_, sizeof(Node) * max_nodes), "WarpField");
     check_cuda(cudaMalloc(&d_T_, sizeof(DQ) * max_nodes), "WarpField");
     check_cuda(cudaMalloc(&d_Tprev_, sizeof(DQ) * max_nodes), "WarpField");
@@ -275,8 +339,7 @@ class CorrespondenceSearch {
   template <class Cam, class M4, class Corr>
   int find_correspondences(const cf_corr_frame& frame, const Cam& cam, const M4& T_cam_world, const M4& T_world_cam,
                            const cf_corr_params& params, Corr* d_corrs, int* d_num_valid, int* d_stats = nullptr) {
-    static_assert(sizeof(Cam) == sizeof(cf_camera) && sizeof(M4) == sizeof(cf_mat4) &&
-                      sizeof(Corr) == sizeof(cf_correspondence),
+    static_assert(camera_layout_matches<Cam>() && mat4_layout_matches<M4>() && corr_layout_matches<Corr>(),
                   "CameraIntrinsics / Mat4 / Correspondence layouts");
     check(cf_find_correspondences(h_, &frame, reinterpret_cast<const cf_camera*>(&cam),
                                   reinterpret_cast<const cf_mat4*>(&T_cam_world),
@@ -316,8 +379,8 @@ class LiveSurfaceRaster {
                const float* d_voxel_knn_w, const Cam& cam, const M4& T_cam_world, const cf_voxel_grid& grid,
                V3* d_live_vertices, V3* d_live_normals, int* d_hit_voxel_idx) {
     static_assert(sizeof(V3) == 3 * sizeof(float) && sizeof(I3) == 3 * sizeof(int), "float3 / int3");
-    static_assert(sizeof(Node) == sizeof(cf_deform_node) && sizeof(DQ) == sizeof(cf_dual_quat) &&
-                      sizeof(Cam) == sizeof(cf_camera) && sizeof(M4) == sizeof(cf_mat4),
+    static_assert(node_layout_matches<Node>() && dq_layout_matches<DQ>() && camera_layout_matches<Cam>() &&
+                      mat4_layout_matches<M4>(),
                   "DeformNode / DualQuat / CameraIntrinsics / Mat4 layouts");
     check(cf_predict_live_surface(h_, reinterpret_cast<const float*>(d_canonical), reinterpret_cast<float*>(d_warped),
                                   reinterpret_cast<const int*>(d_triangles), num_vertices, num_triangles,
@@ -366,10 +429,10 @@ class TSDFIntegrator {
                  const Node* d_nodes = nullptr, const DQ* d_transforms = nullptr, int num_nodes = 0,
                  const int* d_voxel_knn = nullptr, const float* d_voxel_knn_w = nullptr,
                  const int* d_voxel_opt_counts = nullptr, int min_opt_count = 0) {
-    static_assert(sizeof(Voxel) == sizeof(cf_tsdf_voxel) && sizeof(Params) == sizeof(cf_tsdf_params),
+    static_assert(voxel_layout_matches<Voxel>() && tsdf_params_layout_matches<Params>(),
                   "TSDFVoxel / TSDFVolume::Params layouts");
-    static_assert(sizeof(Node) == sizeof(cf_deform_node) && sizeof(DQ) == sizeof(cf_dual_quat) &&
-                      sizeof(Cam) == sizeof(cf_camera) && sizeof(M4) == sizeof(cf_mat4),
+    static_assert(node_layout_matches<Node>() && dq_layout_matches<DQ>() && camera_layout_matches<Cam>() &&
+                      mat4_layout_matches<M4>(),
                   "DeformNode / DualQuat / CameraIntrinsics / Mat4 layouts");
     if (d_nodes && num_nodes > cap_) check(CF_ERR_CAPACITY, "TSDFVolume::integrate");
     check(cf_tsdf_integrate(reinterpret_cast<cf_tsdf_voxel*>(d_voxels),
@@ -387,7 +450,7 @@ class TSDFIntegrator {
   static void mark_optimized_voxels(const Corr* d_corrs, const int* d_canonical_vidx, int num_pixels,
                                     const Dims& dims, int frame_id, int* d_voxel_opt_counts,
                                     int* d_voxel_opt_frame) {
-    static_assert(sizeof(Corr) == sizeof(cf_correspondence) && sizeof(Dims) == 3 * sizeof(int),
+    static_assert(corr_layout_matches<Corr>() && sizeof(Dims) == 3 * sizeof(int),
                   "Correspondence / int3 layouts");
     check(cf_mark_optimized_voxels(reinterpret_cast<const cf_correspondence*>(d_corrs), d_canonical_vidx, num_pixels,
                                    reinterpret_cast<const int*>(&dims), frame_id, d_voxel_opt_counts,

@@ -413,3 +413,41 @@ def mark_optimized_voxels(recs, vidx_map, dims, frame, counts, frames):
              [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
               ctypes.c_void_p, ctypes.c_void_p])(_p(valid), _p(weight), _p(vm), vm.size, _p(dims), frame, _p(counts),
                                                  _p(frames))
+
+
+# ---- voxel kNN field (oracle/cf_oracle_voxelknn.c) ----
+
+
+def voxel_knn(vox, params, nodes, lo=0, hi=None, nthreads=1):
+    """compute_voxel_knn_kernel (src/warp_field.cu:299-405) over voxels [lo, hi) of `vox`
+    (float32 (V, 3) voxel records); params = dict(dims, origin, voxel_size).  Returns
+    (ids int32 (n, 4), ws float32 (n, 4)); with no nodes the arrays stay -2 / NaN (untouched)."""
+    dims = np.ascontiguousarray(params["dims"], np.int32)
+    hi = vox.shape[0] if hi is None else hi
+    org = np.ascontiguousarray(params["origin"], np.float32)
+    nd = np.ascontiguousarray(nodes, NODE_DTYPE)
+    v = np.ascontiguousarray(vox, np.float32)
+    ids = np.full((hi - lo, 4), -2, np.int32)
+    ws = np.full((hi - lo, 4), np.nan, np.float32)
+    _tsdf_fn("cfo_voxel_knn", None,
+             [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p, ctypes.c_int,
+              ctypes.c_longlong, ctypes.c_longlong, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int])(
+        _p(v), _p(dims), _p(org), params["voxel_size"], _p(nd), nd.shape[0], lo, hi, _p(ids), _p(ws), nthreads)
+    return ids, ws
+
+
+def voxel_knn_list(vox, params, nodes, vidx, nthreads=1):
+    """The same for the voxels listed in `vidx` (int64): (ids (n, 4), ws (n, 4))."""
+    dims = np.ascontiguousarray(params["dims"], np.int32)
+    org = np.ascontiguousarray(params["origin"], np.float32)
+    nd = np.ascontiguousarray(nodes, NODE_DTYPE)
+    v = np.ascontiguousarray(vox, np.float32)
+    vi = np.ascontiguousarray(vidx, np.int64)
+    ids = np.full((vi.size, 4), -2, np.int32)
+    ws = np.full((vi.size, 4), np.nan, np.float32)
+    _tsdf_fn("cfo_voxel_knn_list", None,
+             [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p, ctypes.c_int,
+              ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int])(
+        _p(v), _p(dims), _p(org), params["voxel_size"], _p(nd), nd.shape[0], _p(vi), vi.size, _p(ids), _p(ws),
+        nthreads)
+    return ids, ws

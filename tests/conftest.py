@@ -37,3 +37,11 @@ def cflib():
     from cudafusion_b200 import _lib
 
     return _lib.lib()
+
+
+def reference_dir():
+    """The CUDAFusion checkout, where one is on this machine: CF_REFERENCE_DIR,
+    else a `reference` directory beside this repository.  None when absent
+    (tests that compile or run the reference's sources then skip)."""
+    d = os.environ.get("CF_REFERENCE_DIR") or os.path.join(os.path.dirname(ROOT), "reference")
+    return d if os.path.isdir(os.path.join(d, "include")) else None

@@ -1,8 +1,9 @@
 """Generates tests/golden/se3_kat.npz: known-answer vectors of the reference's
 own se3 functions (CUDAFusion include/se3_math.cuh, include/fusion_math.h),
 compiled for the host from the reference sources by oracle/Makefile (target
-`ref`) and run here.  Needs the reference checkout (REF, default
-/root/reference); the committed .npz is what the tests read.
+`ref`) and run here.  Needs the reference checkout (REF, by default a
+`reference` directory beside this repository); the committed .npz is what the
+tests read.
 
     python tests/golden/make_golden.py
 """

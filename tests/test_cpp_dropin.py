@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 import torch
 
-from conftest import ROOT, has_gpu
+from conftest import ROOT, has_gpu, reference_dir
 
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 SRC = os.path.join(ROOT, "tests", "cpp", "dropin_loop.cpp")
@@ -102,3 +102,41 @@ def test_frontend_classes_compile_and_fail_loudly_without_gpu(cflib, tmp_path):
     r = subprocess.run([out, "nodev"], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0, r.stdout + r.stderr
 
+
+
+def _compile_only(src, extra_includes=()):
+    cmd = ["g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", "-I", os.path.join(ROOT, "include"),
+           "-I", os.path.join(CUDA, "include")]
+    for d in extra_includes:
+        cmd += ["-I", d]
+    return subprocess.run(cmd + [src], capture_output=True, text=True)
+
+
+@pytest.mark.skipif(reference_dir() is None, reason="the CUDAFusion sources are not on this machine "
+                    "(set CF_REFERENCE_DIR)")
+def test_layouts_checked_against_reference_headers():
+    """Every templated method of the drop-in classes instantiated with the
+    reference's own types from its include/types.h and include/tsdf_volume.h:
+    the size and per-field offset checks hold for the real definitions."""
+    src = os.path.join(ROOT, "tests", "cpp", "dropin_reftypes.cpp")
+    r = _compile_only(src, [os.path.join(reference_dir(), "include")])
+    assert r.returncode == 0, r.stderr
+
+
+def test_layout_check_catches_field_order_drift(tmp_path):
+    """A Correspondence of the right size with dst and normal swapped must not
+    compile: the checks compare field offsets, not only sizes."""
+    src = tmp_path / "drift.cpp"
+    src.write_text("""
+#include "cudafusion_b200.hpp"
+struct DualQuat { float4 real; float4 dual; };
+struct DeformNode { float3 pos; float3 normal; float radius; int neighbors[8]; float neighbor_w[8];
+                    int num_neighbors; };
+struct Correspondence { float3 src, normal, dst; int node_ids[4]; float node_ws[4]; float weight; bool valid; };
+static_assert(sizeof(Correspondence) == sizeof(cf_correspondence), "same size");
+static_assert(cudafusion_b200::layouts_match<DeformNode, DualQuat, Correspondence>(), "drift detected");
+""")
+    r = _compile_only(str(src))
+    assert r.returncode != 0
+    assert "drift detected" in r.stderr
+    assert "same size" not in r.stderr
