@@ -1486,6 +1486,223 @@ def run_linesearch(args, world, rank, local):
     }
 
 
+VOXELKNN_METRIC = "ms per voxel kNN field (WarpField::compute_voxel_knn) of the 256^3 volume"
+
+
+def voxelknn_algorithmic_bytes(V, N):
+    """Per launch: every 12-byte voxel record read once (its weight decides
+    the voxel), the 16-byte id list and 16-byte weight list written for every
+    voxel, the nodes' positions and radii read once (16 B each)."""
+    return 44 * V + 16 * N
+
+
+def run_voxelknn(args, world, rank, local):
+    """`--workload voxelknn`: the voxel kNN field of the reference's 256^3 x
+    6 mm volume after a frame was integrated (2.1 M voxels hold data, the
+    free space in front of the surface included) over the 1728-node surface
+    graph, as DynamicFusionPipeline recomputes it after a graph update
+    (include/fusion_app.h:1002,1039)."""
+    import torch
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from cudafusion_b200 import synth
+    from cudafusion_b200.tsdf import TSDFVolume, TsdfParams
+
+    f = synth.voxelknn_frame()
+    p = f.params
+    vol = TSDFVolume(TsdfParams(dims=tuple(int(v) for v in p["dims"]), voxel_size=p["voxel_size"],
+                                origin=tuple(float(v) for v in p["origin"])))
+    vol.voxels.copy_(torch.from_numpy(f.voxels.view(np.uint8).reshape(-1).copy()))
+    V, N = vol.n, len(f.nodes)
+    nodes = torch.from_numpy(f.nodes.view(np.uint8).reshape(-1).copy()).cuda()
+    ids = torch.empty(4 * V, dtype=torch.int32, device="cuda")
+    ws = torch.empty(4 * V, dtype=torch.float32, device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    side = torch.cuda.Stream()
+
+    def one():
+        vol.compute_voxel_knn(nodes, N, ids, ws, stream=side)
+
+    with torch.cuda.stream(side):
+        for _ in range(args.warmup):
+            flush.fill_(1)
+            one()
+    side.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    sampler = ClockSampler(local) if rank == 0 else None
+    barrier(world)
+    if sampler:
+        sampler.start()
+    t_wall = time.perf_counter()
+    with torch.cuda.stream(side):
+        for k in range(args.steps):
+            flush.fill_(1)
+            evs[k][0].record(side)
+            one()
+            evs[k][1].record(side)
+    side.synchronize()
+    barrier(world)
+    t_wall = time.perf_counter() - t_wall
+    clocks = sampler.stop() if sampler else None
+    value = replica_value(sum(a.elapsed_time(b) for a, b in evs), args.steps, world)
+    # end to end through the public API: the nodes from pinned host memory
+    # (the volume stays on the device, as the pipeline keeps it), the field,
+    # and the list of the volume's centre voxel read back
+    h_nodes = torch.from_numpy(f.nodes.view(np.uint8).reshape(-1).copy()).pin_memory()
+    h_out = torch.empty(4, dtype=torch.int32).pin_memory()
+    mid = V // 2 + int(p["dims"][0]) // 2
+    e2e_times = []
+    barrier(world)
+    with torch.cuda.stream(side):
+        for _ in range(max(3, min(args.steps, 10))):
+            flush.fill_(1)
+            side.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(side)
+            nodes.copy_(h_nodes, non_blocking=True)
+            one()
+            h_out.copy_(ids[4 * mid: 4 * mid + 4], non_blocking=True)
+            b.record(side)
+            side.synchronize()
+            e2e_times.append(a.elapsed_time(b))
+    e2e_ms = replica_value(sum(e2e_times), len(e2e_times), world)
+    if rank != 0:
+        return None
+    hbm, peak_kind = peaks()
+    alg = voxelknn_algorithmic_bytes(V, N)
+    achieved = alg / (value * 1e-3) / 1e9
+    active = int(f.meta["active"])
+    cpu = None
+    if not args.no_cpu_baseline:
+        import oracle as O
+
+        rng = np.random.default_rng(3)
+        act = np.where(~(f.voxels[:, 1] <= 0))[0]
+        sample = np.sort(rng.choice(act, 20000, replace=False)).astype(np.int64)
+        nthreads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        O.voxel_knn_list(f.voxels, p, f.nodes, sample, nthreads=nthreads)
+        dt = (time.perf_counter() - t0) * 1e3
+        cpu = {"value": dt * active / sample.size, "unit": "ms", "cores": nthreads, "kind": "port",
+               "sample": f"{sample.size} of the {active} voxels with data (the C oracle, OpenMP), scaled to all of "
+                         "them; the empty voxels' constant lists are not counted"}
+    return {
+        "metric": VOXELKNN_METRIC,
+        "value": value,
+        "unit": "ms",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": value * world,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": f"voxel kNN field of a {'x'.join(str(int(v)) for v in p['dims'])} volume ({V} voxels, "
+                        f"{active} with data) over {N} surface nodes",
+            "l2": "flushed between steps (256 MiB write); the 0.54 GB field exceeds L2",
+            "parallelism": f"replicas x{world}",
+        },
+        "roofline": {"kernel": "voxel_knn_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm, "traffic": load_traffic("voxel_knn_kernel"),
+                     "algorithmic_bytes_per_launch": alg, "ms_per_launch": value,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(h_nodes.numel()),
+                "d2h_bytes_per_step": 16},
+        "gpu_launches": args.steps,
+        "gpu_launches_per_step": 1,
+        "clocks": clocks,
+        "wall_s_timed_region": t_wall,
+    }
+
+
+def run_reference_voxelknn(args, world, rank, local):
+    """`--impl reference --workload voxelknn`: the reference's own
+    compute_voxel_knn_kernel (src/warp_field.cu:299-405) in its launch shape
+    on the same volume and nodes; its public call WarpField::compute_voxel_knn
+    (which also reallocates the field and synchronises) is reported beside."""
+    import torch
+
+    if rank != 0:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_voxelknn
+
+    if not ref_voxelknn.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libcfref_voxelknn.so was not built "
+                "(needs the reference sources: make -C oracle ref)"}
+    from cudafusion_b200 import synth
+
+    f = synth.voxelknn_frame()
+    ref = ref_voxelknn.RefVoxelKnn(f.params, f.voxels, f.nodes)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    _, _, public_ms = ref.compute(read=False)
+
+    def one():
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        return ref.kernel_ms()
+
+    for _ in range(args.warmup):
+        one()
+    sampler = ClockSampler(local)
+    sampler.start()
+    times = [one() for _ in range(args.steps)]
+    clocks = sampler.stop()
+    value = sum(times) / len(times)
+    public = []
+    for _ in range(3):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        public.append(ref.compute(read=False)[2])
+    e2e = []
+    for _ in range(3):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        lib_nodes = np.ascontiguousarray(f.nodes)
+        ref_voxelknn.lib().refk_set_nodes(ref.h, lib_nodes.ctypes.data_as(ctypes.c_void_p), len(lib_nodes))
+        ref.compute(read=False)
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    ref.close()
+    V = int(np.prod(np.asarray(f.params["dims"], np.int64)))
+    return {
+        "impl": "reference",
+        "metric": VOXELKNN_METRIC,
+        "value": value,
+        "unit": "ms",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": value,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": f"voxel kNN field of a 256x256x256 volume ({V} voxels, {f.meta['active']} with data) "
+                        f"over {len(f.nodes)} surface nodes",
+            "implementation": "CUDAFusion compute_voxel_knn_kernel (8x8 blocks, one z slice per grid layer), rebuilt "
+                              "for sm_100a with --use_fast_math (oracle/_ref/libcfref_voxelknn.so)",
+            "l2": "flushed between steps (256 MiB write)",
+            "parallelism": "single GPU (rank 0 of the launch)",
+        },
+        "public_call_ms": statistics.median(public),
+        "public_call": "WarpField::compute_voxel_knn: cudaFree + cudaMalloc of the two field arrays, the kernel, "
+                       "cudaDeviceSynchronize",
+        "cpu_baseline": {"value": value, "unit": "ms", "cores": 1, "kind": "reference",
+                         "sample": "the reference path is CUDA: the kernel timed on the GPU, one host thread"},
+        "e2e": {"value": statistics.median(e2e), "unit": "ms", "h2d_bytes_per_step": int(f.nodes.nbytes),
+                "d2h_bytes_per_step": 0},
+        "clocks": clocks,
+    }
+
+
 # config 1: the small sphere (N=256, M=20k), 5 GN x 10 PCG at lambda_smooth
 # 10 and the solver.h damping, all iterations run (fixed-iteration timing)
 CONFIG1_KW = dict(gn_iterations=5, pcg_iterations=10, pcg_tolerance=0.0, lambda_smooth=10.0, lambda_damping=1e-2)
@@ -1639,11 +1856,12 @@ def main():
     ap.add_argument("--no-parity", action="store_true", help="skip the check against the reference's solver")
     ap.add_argument("--pcg-mode", type=int, default=0, help="0 auto, 1 grid-wide, 2 single cluster, 3 streaming")
     ap.add_argument("--workload", default="frame",
-                    choices=["frame", "batch", "learned", "corr", "raster", "linesearch", "tsdf"],
+                    choices=["frame", "batch", "learned", "corr", "raster", "linesearch", "tsdf", "voxelknn"],
                     help="frame: the headline line; batch / learned: the batched-solve and learned-start "
                          "measurements alone; corr: the projective correspondence search; raster: the "
                          "live-surface prediction (mesh skinning + rasterisation); linesearch: the GN step's "
-                         "ten-trial line search; tsdf: the warped TSDF integration")
+                         "ten-trial line search; tsdf: the warped TSDF integration; voxelknn: the voxel kNN "
+                         "field of the volume")
     ap.add_argument("--problems", type=int, default=64, help="problems of --workload batch")
     ap.add_argument("--frames", type=int, default=300, help="frames of --workload learned")
     args = ap.parse_args()
@@ -1662,6 +1880,10 @@ def main():
                     "reference figure)"}
         elif args.impl == "reference" and args.workload == "tsdf":
             line = run_reference_tsdf(args, world, rank, local)
+        elif args.impl == "reference" and args.workload == "voxelknn":
+            line = run_reference_voxelknn(args, world, rank, local)
+        elif args.workload == "voxelknn":
+            line = run_voxelknn(args, world, rank, local)
         elif args.workload == "tsdf":
             line = run_tsdf(args, world, rank, local)
         elif args.workload == "linesearch":

@@ -196,31 +196,44 @@ struct AsmArgs {
 // index of (p, q), p <= q, in the packed upper triangle of a 6x6 block
 __host__ __device__ constexpr int tri(int p, int q) { return p * 6 - p * (p - 1) / 2 + (q - p); }
 
-// The row's incidence records (skinned src + fw, normal + residual, skin
-// weights) and entries: the first `ns` / `nt` staged in shared memory, the
-// rest (rows beyond the staging capacity) read from global memory.
+// The row's incidence records, staged as the factors the windows need:
+// U = ((src - x_r) x n, fw w_a) and N = (n, fw w_a r), with the skin weights
+// of the correspondence (for w_b) and the slot a; the first `ns` / `nt` staged
+// in shared memory, the rest (rows beyond the staging capacity) formed from
+// global memory.
 struct RowRecords {
-  const float4* s_sf;
-  const float4* s_nr;
+  const float4* s_u;
+  const float4* s_n;
   const float4* s_ws;
   const int* s_a;     // slot a of each staged incidence
   const int* s_trip;  // the row's entries (ii << 2) | b
   const int* inc;     // the row's incidences (c << 2) | a
   const int* trip;    // the row's entries in global memory
+  float3 xr;          // the row's node
   int ns, nt;
-  __device__ __forceinline__ void get(const Work& w, int ii, float4& sf, float4& nr, float4& ws) const {
+  __device__ __forceinline__ void get(const Work& w, int ii, float4& u, float4& n, float4& ws, int& a) const {
     if (ii < ns) {
-      sf = s_sf[ii];
-      nr = s_nr[ii];
+      u = s_u[ii];
+      n = s_n[ii];
       ws = s_ws[ii];
+      a = s_a[ii];
     } else {
-      const int c = __ldg(inc + ii) >> 2;
-      sf = __ldcg(w.c_srcfw + c);
-      nr = __ldcg(w.c_nres + c);
+      const int e = __ldg(inc + ii);
+      const int c = e >> 2;
+      a = e & 3;
+      const float4 sf = __ldcg(w.c_srcfw + c), nr = __ldcg(w.c_nres + c);
       ws = __ldg(w.pk_ws + c);
+      factor(sf, nr, sel4(ws, a), xr, u, n);
     }
   }
-  __device__ __forceinline__ int slot(int ii) const { return ii < ns ? s_a[ii] : (__ldg(inc + ii) & 3); }
+  // (src, fw), (n, r) and w_a -> U, N
+  __device__ __forceinline__ static void factor(float4 sf, float4 nr, float wa, float3 xr, float4& u, float4& n) {
+    const float3 l = sub3(f3(sf.x, sf.y, sf.z), xr);
+    const float3 cp = cross3(l, f3(nr.x, nr.y, nr.z));
+    const float fwa = sf.w * wa;
+    u = make_float4(cp.x, cp.y, cp.z, fwa);
+    n = make_float4(nr.x, nr.y, nr.z, fwa * nr.w);
+  }
   __device__ __forceinline__ int entry(int t) const { return t < nt ? s_trip[t] : __ldg(trip + t); }
 };
 
@@ -241,22 +254,35 @@ __device__ __forceinline__ void reduce_scatter32(float* a) {
   }
 }
 
-constexpr int kPartVals = 42;  // 36 block values + 6 rhs (diagonal block only)
+// Per block, the sums the windows accumulate (g = fw w_a w_b, u = (src - x_r)
+// x n of the row's node, n the normal):
+//   [0, 6)   S_uu = sum g u u^T (upper triangle: 00 01 02 11 12 22)
+//   [6, 15)  S_un = sum g u n^T (row-major)
+//   [15, 21) S_nn = sum g n n^T (upper triangle)
+//   [21, 27) the rhs, diagonal block only: -sum fw w_a r (u, n)
+// With d = x_c - x_r and D = [d]_x (D v = d x v), the column node's
+// u_c = u - D n, so the block J_a^T ... sum is
+//   [[S_uu + S_un D, S_un], [S_un^T + S_nn D, S_nn]],
+// the off-diagonal block of kernels/solver_kernels.cu:113-137 regrouped (the
+// diagonal block is the same with D = 0).
+constexpr int kSums = 21;
+constexpr int kPartVals = 27;
+__host__ __device__ constexpr int sym3(int p, int q) {
+  return p <= q ? p * 3 - p * (p - 1) / 2 + (q - p) : q * 3 - q * (q - 1) / 2 + (p - q);
+}
 
 // One CTA per block row r.
 //  1. stage: the row's entry list, its incidences' slots and records
-//     (cp.async, one wait)
+//     (cp.async, one wait), then each staged incidence's factors U and N
 //  2. windows: the row's blocks (diagonal first, then the upper off-diagonal
 //     blocks) are cut into windows of 32 entries; warp w takes a contiguous
-//     run of W/8 windows, accumulates lane-private sums of
-//     fw J_a J_b^T (and -fw J_a r for the diagonal) and, whenever it leaves a
-//     block, reduce-scatters them into a partial slot of that block
-//  3. combine: per block value, the warps' partials in warp order (Kahan on
-//     the diagonal block), the ARAP terms of the block's edges (precomputed
-//     by the residual launch), the damping; blocks written with their
-//     transposes, the rhs and the row's ARAP energy.
-// 3 CTAs per SM (80 registers, 74 KB of shared memory each): the per-row
-// phases are latency chains, so rows in flight matter more than registers
+//     run of W/8 windows, accumulates lane-private sums of the 21 products of
+//     g (u, n) (u, n)^T (and the rhs for the diagonal) and, whenever it
+//     leaves a block, reduce-scatters them into a partial slot of that block
+//  3. combine: per block, the warps' partials in warp order (Kahan on the
+//     diagonal block); then per block value its expansion, the ARAP terms of
+//     the block's edges (precomputed by the residual launch) and the damping;
+//     blocks written with their transposes, the rhs and the row's ARAP energy.
 __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern pt, AsmArgs aa) {
   extern __shared__ float4 stage_buf[];
   const int r = w.row_order[blockIdx.x], lane = lane_id(), wid = threadIdx.x >> 5;  // longest rows first
@@ -274,17 +300,19 @@ __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern p
   int4* s_blk = reinterpret_cast<int4*>(s_wpre + Up);  // [Up] (segment start, count, column, transpose position)
   int* s_boff = reinterpret_cast<int*>(s_blk + Up);    // [Up] first block edge of each upper block
   int* s_erole = s_boff + Up;                          // [kRowEdges] role of each row edge
-  float* s_part = reinterpret_cast<float*>(s_erole + kRowEdges);  // [U+8][42]
+  float* s_part = reinterpret_cast<float*>(s_erole + kRowEdges);  // [U+8][27]
+  float* s_sum = s_part + (size_t)(U + kWarps) * kPartVals;       // [U][27] the blocks' sums
   RowRecords R;
   R.ns = min(n_inc, cap);
   R.nt = min(pt.seg_off[dpos + nb - 1] + pt.seg_cnt[dpos + nb - 1] - 4 * i0, 4 * cap);
-  R.s_sf = stage_buf;
-  R.s_nr = stage_buf + cap;
+  R.s_u = stage_buf;
+  R.s_n = stage_buf + cap;
   R.s_ws = stage_buf + 2 * cap;
   R.s_a = s_a;
   R.s_trip = s_trip;
   R.inc = w.inc + i0;
   R.trip = w.trip + 4 * (size_t)i0;
+  R.xr = node_pos(aa.nodes, r);
   // block info, ARAP terms of the row's edges and of its blocks' edges
   const int u0 = pt.ustart[r];
   const int a0 = pt.arap_row_ptr[r], a1 = pt.arap_row_ptr[r + 1] - a0, na = min(a1, kRowEdges);
@@ -312,15 +340,25 @@ __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern p
     for (int k = 0; k < 9; k++) cp_async16(s_bterm + 9 * e + k, src + k);
   }
   for (int t = threadIdx.x; t < R.nt; t += kThreads) s_trip[t] = __ldg(R.trip + t);
+  float4* su = stage_buf;
+  float4* sn = stage_buf + cap;
   for (int ii = threadIdx.x; ii < R.ns; ii += kThreads) {
     const int e = __ldg(R.inc + ii);
     const int c = e >> 2;
     s_a[ii] = e & 3;
-    cp_async16(stage_buf + ii, w.c_srcfw + c);
-    cp_async16(stage_buf + cap + ii, w.c_nres + c);
+    cp_async16(su + ii, w.c_srcfw + c);
+    cp_async16(sn + ii, w.c_nres + c);
     cp_async16(stage_buf + 2 * cap + ii, w.pk_ws + c);
   }
   cp_async_commit_wait_all();
+  // each thread turns the records it staged into the factors (its own
+  // copies: no barrier needed between the wait and the rewrite)
+  for (int ii = threadIdx.x; ii < R.ns; ii += kThreads) {
+    float4 u, n;
+    RowRecords::factor(su[ii], sn[ii], sel4(R.s_ws[ii], s_a[ii]), R.xr, u, n);
+    su[ii] = u;
+    sn[ii] = n;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     int run = 0;
@@ -335,85 +373,56 @@ __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern p
   // ---- 2. windows ----
   const int W = s_wpre[nb];
   const int wa = (int)((long long)W * wid / kWarps), wb = (int)((long long)W * (wid + 1) / kWarps);
-  const float3 xr = node_pos(aa.nodes, r);
   int k = 0;
   while (k < nb && s_wpre[k + 1] <= wa) k++;
-  // lane-private sums: an off-diagonal block's 36 values (p * 6 + q); the
-  // diagonal block's upper triangle (tri(p, q)) and its rhs (21 + p)
-  float acc[36];
+  // lane-private sums (the layout above); the 5 slots past the diagonal
+  // block's 27 stay zero for the reduce-scatter
+  float acc[32];
 #pragma unroll
-  for (int q = 0; q < 36; q++) acc[q] = 0.f;
-  float3 xc = node_pos(aa.nodes, k < nb ? s_blk[k].z : r);
+  for (int q = 0; q < 32; q++) acc[q] = 0.f;
   int seg0 = k < nb ? s_blk[k].x : 0, segn = k < nb ? s_blk[k].y : 0;
   for (int win = wa; win < wb; win++) {
     const int t = seg0 + (win - s_wpre[k]) * 32 + lane;
     if (t < seg0 + segn) {
       const int e = R.entry(t);
       const int ii = e >> 2, b = e & 3;
-      float4 sf, nr, w4;
-      R.get(w, ii, sf, nr, w4);
-      if (sf.w != 0.f) {
-        const int a = R.slot(ii);
-        const float3 src = f3(sf.x, sf.y, sf.z), n = f3(nr.x, nr.y, nr.z);
-        float Ja[6], Jb[6];
-        jac_row(src, xr, n, sel4(w4, a), Ja);
-        jac_row(src, xc, n, sel4(w4, b), Jb);
-        if (k == 0) {  // (the block index is uniform in the warp)
+      float4 u, n, w4;
+      int a;
+      R.get(w, ii, u, n, w4, a);
+      const float g = u.w * sel4(w4, b);
+      if (g != 0.f) {
+        const float gu[3] = {g * u.x, g * u.y, g * u.z};
+        const float gn[3] = {g * n.x, g * n.y, g * n.z};
+        const float uu[3] = {u.x, u.y, u.z};
+        const float nn[3] = {n.x, n.y, n.z};
 #pragma unroll
-          for (int p = 0; p < 6; p++) {
-            const float f = sf.w * Ja[p];
+        for (int p = 0; p < 3; p++) {
 #pragma unroll
-            for (int q = p; q < 6; q++) acc[tri(p, q)] += f * Jb[q];
+          for (int q = p; q < 3; q++) {
+            acc[sym3(p, q)] += gu[p] * uu[q];
+            acc[15 + sym3(p, q)] += gn[p] * nn[q];
           }
-          if (a == b) {
 #pragma unroll
-            for (int p = 0; p < 6; p++) acc[21 + p] += -sf.w * Ja[p] * nr.w;
-          }
-        } else {
+          for (int q = 0; q < 3; q++) acc[6 + 3 * p + q] += gu[p] * nn[q];
+        }
+        if (k == 0 && a == b) {  // (the block index is uniform in the warp)
 #pragma unroll
-          for (int p = 0; p < 6; p++) {
-            const float f = sf.w * Ja[p];
-#pragma unroll
-            for (int q = 0; q < 6; q++) acc[p * 6 + q] += f * Jb[q];
+          for (int p = 0; p < 3; p++) {
+            acc[21 + p] += -n.w * uu[p];
+            acc[24 + p] += -n.w * nn[p];
           }
         }
       }
     }
     // leaving block k (next window belongs to another block, or the run ends)
     if (win + 1 == wb || win + 1 == s_wpre[k + 1]) {
-      float* dst = s_part + (size_t)(k + wid) * kPartVals;
-      if (k == 0) {  // 27 values (acc[27..31] stay zero): one reduce-scatter
-        reduce_scatter32(acc);
-        if (lane < 27) dst[lane] = acc[0];
-      } else {
-        float extra[4] = {acc[32], acc[33], acc[34], acc[35]};
-        reduce_scatter32(acc);
-        dst[lane] = acc[0];
-        // the last 4 values: halved over lane bits 4 and 3 (3 exchanges),
-        // then summed over bits 2..0; lane 8g holds value 2 (g >> 1) + (g & 1)
+      reduce_scatter32(acc);
+      if (lane < kPartVals) s_part[(size_t)(k + wid) * kPartVals + lane] = acc[0];
 #pragma unroll
-        for (int q = 0; q < 2; q++) {
-          const bool up = (lane & 16) != 0;
-          const float send = up ? extra[q] : extra[q + 2];
-          const float keep = up ? extra[q + 2] : extra[q];
-          extra[q] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-        }
-        {
-          const bool up = (lane & 8) != 0;
-          const float send = up ? extra[0] : extra[1];
-          const float keep = up ? extra[1] : extra[0];
-          extra[0] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-        }
-#pragma unroll
-        for (int o = 4; o > 0; o >>= 1) extra[0] += __shfl_xor_sync(0xffffffffu, extra[0], o);
-        if ((lane & 7) == 0) dst[32 + 2 * ((lane >> 4) & 1) + ((lane >> 3) & 1)] = extra[0];
-      }
-#pragma unroll
-      for (int q = 0; q < 36; q++) acc[q] = 0.f;
+      for (int q = 0; q < 32; q++) acc[q] = 0.f;
       if (win + 1 < wb) {
         k++;
         while (k < nb && s_wpre[k + 1] <= win + 1) k++;
-        xc = node_pos(aa.nodes, s_blk[k].z);
         seg0 = s_blk[k].x;
         segn = s_blk[k].y;
       }
@@ -421,9 +430,25 @@ __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern p
   }
   __syncthreads();
 
-  // ---- 3. combine ----
-  const int nwork = 27 + 36 * (nb - 1);
-  for (int item = threadIdx.x; item < nwork; item += kThreads) {
+  // ---- 3a. the blocks' sums: the warps' partials in warp order ----
+  for (int item = threadIdx.x; item < kPartVals + kSums * (nb - 1); item += kThreads) {
+    const int kb = item < kPartVals ? 0 : 1 + (item - kPartVals) / kSums;
+    const int v = item < kPartVals ? item : (item - kPartVals) % kSums;
+    const int w0 = s_wpre[kb], w1 = s_wpre[kb + 1];
+    float tot = 0.f, comp = 0.f;
+    for (int ww = 0; ww < kWarps && w1 > w0; ww++) {  // the warps whose window runs met block kb
+      const int a_w = (int)((long long)W * ww / kWarps), b_w = (int)((long long)W * (ww + 1) / kWarps);
+      if (a_w >= b_w || a_w >= w1 || b_w <= w0) continue;
+      const float x = s_part[(size_t)(kb + ww) * kPartVals + v];
+      if (kb == 0) kahan_add(tot, comp, x); else tot += x;
+    }
+    s_sum[(size_t)kb * kPartVals + v] = tot - comp;
+  }
+  __syncthreads();
+
+  // ---- 3b. per block value: expansion, ARAP terms, damping ----
+  const int pos0 = dpos;
+  for (int item = threadIdx.x; item < 27 + 36 * (nb - 1); item += kThreads) {
     int kb, v;
     if (item < 27) {
       kb = 0;
@@ -432,22 +457,19 @@ __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern p
       kb = 1 + (item - 27) / 36;
       v = (item - 27) % 36;
     }
-    // warps that touched block kb, in warp order
-    const int w0 = s_wpre[kb], w1 = s_wpre[kb + 1];
-    float tot = 0.f, comp = 0.f;
-    if (w1 > w0) {
-      const int idx = v;  // diagonal block: tri(p, q), then the rhs at 21 + p; off-diagonal: p * 6 + q
-      for (int ww = 0; ww < kWarps; ww++) {  // the warps whose window runs met block kb
-        const int a_w = (int)((long long)W * ww / kWarps), b_w = (int)((long long)W * (ww + 1) / kWarps);
-        if (a_w >= b_w || a_w >= w1 || b_w <= w0) continue;
-        const float x = s_part[(size_t)(kb + ww) * kPartVals + idx];
-        if (kb == 0) kahan_add(tot, comp, x); else tot += x;
-      }
-      tot -= comp;
-      comp = 0.f;
-    }
-    const int pos = dpos + kb;
+    const float* S = s_sum + (size_t)kb * kPartVals;
+    const int pos = pos0 + kb;
     if (kb == 0) {
+      // diagonal block: upper triangle tri(p, q) (21) and the rhs (6)
+      float tot, comp = 0.f;
+      int p = 0, q = 0;
+      if (v < 21) {
+        while (tri(p, 5) < v) p++;
+        q = v - tri(p, p) + p;
+        tot = p < 3 ? (q < 3 ? S[sym3(p, q)] : S[6 + 3 * p + (q - 3)]) : S[15 + sym3(p - 3, q - 3)];
+      } else {
+        tot = S[v];
+      }
       // ARAP edges incident to r (kernels/solver_kernels.cu:293-313, 337-350)
       for (int e = 0; e < a1; e++) {
         float x;
@@ -461,9 +483,6 @@ __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern p
       }
       tot -= comp;
       if (v < 21) {
-        int p = 0;
-        while (tri(p, 5) < v) p++;
-        const int q = v - tri(p, p) + p;
         // damping on the diagonal entries (solver_kernels.cu:183-193)
         if (p == q) tot = tot + aa.lambda_damping * fmaxf(fabsf(tot), p < 3 ? 1e-3f : 1e-2f);
         float* out = pt.values + (size_t)pos * 36;
@@ -473,6 +492,28 @@ __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern p
         w.rhs[r * 6 + (v - 21)] = tot;
       }
     } else {
+      const int p = v / 6, q = v % 6;
+      float tot;
+      if (p < 3 && q >= 3) {
+        tot = S[6 + 3 * p + (q - 3)];  // S_un
+      } else if (p >= 3 && q >= 3) {
+        tot = S[15 + sym3(p - 3, q - 3)];  // S_nn
+      } else {
+        // (S_uu + S_un D)[p][q] or (S_un^T + S_nn D)[p - 3][q]:
+        // D[k][q] = e_k . (d x e_q), d = x_c - x_r
+        const float3 xc = node_pos(aa.nodes, s_blk[kb].z);
+        const float d[3] = {xc.x - R.xr.x, xc.y - R.xr.y, xc.z - R.xr.z};
+        // column q of D: d x e_q
+        const float dq[3] = {q == 0 ? 0.f : q == 1 ? -d[2] : d[1], q == 0 ? d[2] : q == 1 ? 0.f : -d[0],
+                             q == 0 ? -d[1] : q == 1 ? d[0] : 0.f};
+        if (p < 3) {
+          tot = S[sym3(p, q)] + S[6 + 3 * p] * dq[0] + S[6 + 3 * p + 1] * dq[1] + S[6 + 3 * p + 2] * dq[2];
+        } else {
+          const int pp = p - 3;
+          tot = S[6 + 3 * q + pp] + S[15 + sym3(pp, 0)] * dq[0] + S[15 + sym3(pp, 1)] * dq[1] +
+                S[15 + sym3(pp, 2)] * dq[2];
+        }
+      }
       // ARAP edges (r, j) visited from r (solver_kernels.cu:315-324)
       const int e0 = s_boff[kb], e1 = kb + 1 < nb ? s_boff[kb + 1] : be1;
       for (int e = e0; e < e1; e++) {
@@ -518,7 +559,7 @@ cudaError_t launch_expand(const Work& w, const Pattern& p, int N, cudaStream_t s
 int assemble_smem_bytes(int max_upper_row) {
   const int Up = (max_upper_row + 4) & ~3;
   return kStageCap * (3 * (int)sizeof(float4) + 5 * (int)sizeof(int)) + kRowEdges * 16 * (int)sizeof(float4) +
-         kRowEdges * 8 + Up * (4 + 16 + 4) + kRowEdges * 4 + (max_upper_row + kWarps) * kPartVals * 4;
+         kRowEdges * 8 + Up * (4 + 16 + 4) + kRowEdges * 4 + (2 * max_upper_row + kWarps) * kPartVals * 4;
 }
 
 cudaError_t launch_assemble(const Work& w, const Pattern& p, const SolveArgs& a, const cf_dual_quat* T,

@@ -169,14 +169,33 @@ __global__ void __launch_bounds__(kVkThreads)
   const int oz = ((warp >> 2) << 1) | (lane >> 4);
   const unsigned tiles_xy = (unsigned)k.tx * (unsigned)k.ty;
 
-  for (unsigned t = blockIdx.x; t < k.tiles; t += gridDim.x) {
+  // this thread's voxel of tile t, and its weight (0 outside the volume);
+  // the weights of the next two tiles are loaded ahead, so that a tile's
+  // DRAM round trip overlaps the work on the tiles before it
+  auto voxel_of = [&](unsigned t, int& x, int& y, int& z) -> bool {
     const unsigned tz = t / tiles_xy, rem = t - tz * tiles_xy;
     const unsigned ty = rem / (unsigned)k.tx, tx = rem - ty * (unsigned)k.tx;
-    const int x = (int)tx * 8 + ox, y = (int)ty * 8 + oy, z = (int)tz * 8 + oz;
-    const bool in = x < k.dx && y < k.dy && z < k.dz;
+    x = (int)tx * 8 + ox;
+    y = (int)ty * 8 + oy;
+    z = (int)tz * 8 + oz;
+    return t < k.tiles && x < k.dx && y < k.dy && z < k.dz;
+  };
+  auto weight_of = [&](unsigned t) -> float {
+    int x, y, z;
+    if (!voxel_of(t, x, y, z)) return 0.f;
+    return __ldcs(vox + 3 * (((size_t)z * (size_t)k.dy + (size_t)y) * (size_t)k.dx + (size_t)x) + 1);
+  };
+  float w_next = weight_of(blockIdx.x), w_after = weight_of(blockIdx.x + gridDim.x);
+  for (unsigned t = blockIdx.x; t < k.tiles; t += gridDim.x) {
+    int x, y, z;
+    const bool in = voxel_of(t, x, y, z);
+    const unsigned tx = (unsigned)(x - ox) >> 3, ty = (unsigned)(y - oy) >> 3, tz = (unsigned)(z - oz) >> 3;
     const size_t vidx = ((size_t)z * (size_t)k.dy + (size_t)y) * (size_t)k.dx + (size_t)x;
+    const float wv = w_next;
+    w_next = w_after;
+    w_after = weight_of(t + 2 * gridDim.x);
     // src/warp_field.cu:319: only voxels with weight > 0 (a NaN weight is not <= 0)
-    const bool active = in && !(__ldcs(vox + 3 * vidx + 1) <= 0.f);
+    const bool active = in && !(wv <= 0.f);
     if (!__syncthreads_or(active)) {
       if (in) {
         __stcs(out_ids + vidx, make_int4(-1, -1, -1, -1));

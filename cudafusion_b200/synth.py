@@ -1025,3 +1025,84 @@ def tsdf_frame(width=640, height=480, dims=(256, 256, 256), extent=1.536, origin
                      camera_pose=pose.astype(np.float32), depth=depth.astype(np.float32), voxels=vox, nodes=nodes,
                      transforms=transforms, voxel_knn=knn, voxel_knn_w=knn_w, counts=counts,
                      meta=dict(node_radius=h, band_voxels=int((counts > 0).sum())))
+
+
+@dataclass
+class VoxelKnnFrame:
+    """The inputs of WarpField::compute_voxel_knn: a canonical volume (12-byte
+    voxel records as float32 (V, 3)), its TSDFVolume::Params fields, and the
+    deformation nodes."""
+
+    params: dict
+    voxels: np.ndarray
+    nodes: np.ndarray
+    meta: dict = field(default_factory=dict)
+
+
+def voxelknn_frame(width=640, height=480, dims=(256, 256, 256), extent=1.536, origin=(-0.768, -0.768, 0.5),
+                   truncation_voxels=5.0, nodes_xy=(48, 36), cam_rot_deg=0.8, cam_trans=(0.004, -0.003, 0.002),
+                   duplicate_nodes=0, seed=23):
+    """The canonical volume as compute_voxel_knn sees it once a frame of the
+    smooth bumpy surface of tsdf_frame (about 1.1 m in front of the camera)
+    has been integrated: a voxel holds weight > 0 where the integration
+    updates it (kernels/tsdf_kernels.cu:85-174: its centre projects to a
+    pixel with depth d > 0 and d - z >= -truncation), so the free space in
+    front of the surface holds data as well as the band around it; weights
+    are random in (0, 50], elsewhere 0.  Nodes sit on the surface on a
+    nodes_xy lattice of pixels (radius 1.5 x the lattice spacing);
+    `duplicate_nodes` more nodes repeat the positions of random ones (exact
+    distance ties, which the reference resolves to the lower index)."""
+    rng = np.random.default_rng(seed)
+    dims = np.asarray(dims, np.int32)
+    vs = float(np.float32(extent / float(dims[0])))
+    trunc = float(np.float32(truncation_voxels * vs))
+    s = width / 640.0
+    fx = fy = 570.342 * s
+    cx, cy = width / 2.0, height / 2.0
+    u, v = np.meshgrid(np.arange(width, dtype=np.float64), np.arange(height, dtype=np.float64))
+    z = 1.1 + 0.12 * np.sin(2 * np.pi * 1.5 * u / width) * np.cos(2 * np.pi * v / height) + 0.06 * (u / width)
+    axis = rng.normal(size=3)
+    axis /= np.linalg.norm(axis)
+    pose = np.eye(4)
+    pose[:3, :3] = _rotmat(quat_from_rotvec(axis * np.deg2rad(cam_rot_deg)))
+    pose[:3, 3] = cam_trans
+    pc = np.stack([z * (u - cx) / fx, z * (v - cy) / fy, z], -1)
+    nu, nv = nodes_xy
+    iu = np.linspace(0.04 * width, 0.96 * width, nu).astype(int)
+    iv = np.linspace(0.04 * height, 0.96 * height, nv).astype(int)
+    node_pos = pc[iv[:, None], iu[None, :]].reshape(-1, 3) @ pose[:3, :3].T + pose[:3, 3]
+    spacing = np.median(np.linalg.norm(np.diff(pc[iv[nv // 2], iu], axis=0), axis=-1))
+    h = 1.5 * spacing
+    if duplicate_nodes:
+        node_pos = np.concatenate([node_pos, node_pos[rng.integers(0, len(node_pos), duplicate_nodes)]])
+    nb, nw, kc = _graph(node_pos, h)
+    nodes = _make_nodes(node_pos, np.zeros_like(node_pos), h, nb, nw, kc)
+    V = int(np.prod(dims.astype(np.int64)))
+    vox = np.zeros((V, 3), np.float32)
+    vox[:, 0] = 1.0
+    vox.view(np.uint32)[:, 2] = 0x00808080
+    org = np.asarray(origin, np.float64)
+    Rcw = pose[:3, :3].T
+    tcw = -Rcw @ pose[:3, 3]
+    plane = int(dims[0]) * int(dims[1])
+    gx, gy = np.meshgrid(np.arange(dims[0]), np.arange(dims[1]))
+    gx, gy = gx.reshape(-1), gy.reshape(-1)
+    zf = z.reshape(-1)
+    for zi in range(int(dims[2])):
+        c = np.stack([org[0] + (gx + 0.5) * vs, org[1] + (gy + 0.5) * vs,
+                      np.full(gx.shape, org[2] + (zi + 0.5) * vs)], -1)
+        p = c @ Rcw.T + tcw
+        with np.errstate(divide="ignore", invalid="ignore"):
+            pu = np.rint(fx * p[:, 0] / p[:, 2] + cx)
+            pv = np.rint(fy * p[:, 1] / p[:, 2] + cy)
+        ok = (p[:, 2] > 0) & (pu >= 0) & (pu < width) & (pv >= 0) & (pv < height)
+        idx = (np.where(ok, pv, 0) * width + np.where(ok, pu, 0)).astype(np.int64)
+        sdf = np.where(ok, zf[idx] - p[:, 2], -np.inf)
+        upd = ok & (sdf >= -trunc)
+        if upd.any():
+            sl = vox[zi * plane:(zi + 1) * plane]
+            sl[upd, 0] = np.minimum(1.0, sdf[upd] / trunc)
+            sl[upd, 1] = rng.uniform(0.0, 50.0, int(upd.sum())) + np.float32(1e-3)
+    params = dict(dims=dims, origin=np.asarray(origin, np.float32), voxel_size=vs)
+    return VoxelKnnFrame(params=params, voxels=vox, nodes=nodes,
+                         meta=dict(active=int((vox[:, 1] > 0).sum()), node_radius=h, nodes=len(nodes)))

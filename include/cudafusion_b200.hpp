@@ -221,9 +221,9 @@ class GaussNewtonSolver {
 };
 
 // The solve-path part of WarpField: node storage, transforms with
-// save/restore, the twist update.  Graph construction (add_nodes_*,
-// prune_nodes, compute_voxel_knn) stays with the reference.  Node and DQ
-// are the caller's DeformNode / DualQuat types.
+// save/restore, the twist update, and the voxel kNN field.  Graph
+// construction (add_nodes_*, prune_nodes) stays with the reference.  Node
+// and DQ are the caller's DeformNode / DualQuat types.
 template <class Node, class DQ>
 class WarpField {
  public:
@@ -298,6 +298,37 @@ class WarpField {
     check_cuda(cudaDeviceSynchronize(), "apply_twist_increment");
     h_T_.resize(n_);
     check_cuda(cudaMemcpy(h_T_.data(), d_T_, sizeof(DQ) * n_, cudaMemcpyDeviceToHost), "apply_twist_increment");
+  }
+
+  // include/warp_field.h:72-74, src/warp_field.cu:957-981: the voxel kNN
+  // field of `volume` (the reference's TSDFVolume: params() with dims,
+  // origin and voxel_size, device_data() of 12-byte voxels) over this
+  // field's nodes.  Like the reference: nothing happens without nodes, the
+  // two arrays are (re)allocated to 4 entries per voxel, and the call
+  // synchronises.
+  template <class Volume, class IntArray, class FloatArray>
+  void compute_voxel_knn(const Volume& volume, IntArray& d_voxel_knn, FloatArray& d_voxel_knn_w) {
+    using Voxel = typename std::remove_cv<typename std::remove_pointer<decltype(volume.device_data())>::type>::type;
+    static_assert(voxel_layout_matches<Voxel>(), "TSDFVoxel layout");
+    if (n_ == 0) return;
+    const auto& p = volume.params();
+    const size_t total = (size_t)p.dims.x * (size_t)p.dims.y * (size_t)p.dims.z;
+    d_voxel_knn.allocate(total * CF_K_NEIGHBORS);
+    d_voxel_knn_w.allocate(total * CF_K_NEIGHBORS);
+    cf_tsdf_params cp{};
+    cp.dims[0] = p.dims.x;
+    cp.dims[1] = p.dims.y;
+    cp.dims[2] = p.dims.z;
+    cp.voxel_size = p.voxel_size;
+    cp.origin[0] = p.origin.x;
+    cp.origin[1] = p.origin.y;
+    cp.origin[2] = p.origin.z;
+    check(cf_compute_voxel_knn(reinterpret_cast<const cf_tsdf_voxel*>(volume.device_data()), &cp,
+                               reinterpret_cast<const cf_deform_node*>(d_nodes_), n_,
+                               reinterpret_cast<int*>(d_voxel_knn.data), reinterpret_cast<float*>(d_voxel_knn_w.data),
+                               nullptr),
+          "WarpField::compute_voxel_knn");
+    check_cuda(cudaDeviceSynchronize(), "WarpField::compute_voxel_knn");
   }
 
   float node_radius() const { return node_radius_; }

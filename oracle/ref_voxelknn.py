@@ -37,6 +37,8 @@ def lib():
         L.refk_set_nodes.argtypes = [vp, vp, i]
         L.refk_compute.restype = i
         L.refk_compute.argtypes = [vp, vp, vp, ctypes.POINTER(f)]
+        L.refk_kernel.restype = i
+        L.refk_kernel.argtypes = [vp, ctypes.POINTER(f)]
         _lib = L
     return _lib
 
@@ -74,6 +76,15 @@ class RefVoxelKnn:
         if rc != 0:
             raise RuntimeError(f"reference compute_voxel_knn failed: {rc}")
         return ids, ws, ms.value
+
+    def kernel_ms(self):
+        """compute_voxel_knn_kernel alone (the reference's launch shape) into
+        the outputs of the last compute(); its CUDA-event time in ms."""
+        ms = ctypes.c_float()
+        rc = lib().refk_kernel(self.h, ctypes.byref(ms))
+        if rc != 0:
+            raise RuntimeError(f"reference compute_voxel_knn_kernel failed: {rc}")
+        return ms.value
 
     def close(self):
         if self.h:

@@ -19,6 +19,10 @@
 
 #define REF_EXPORT extern "C" __attribute__((visibility("default")))
 
+// src/warp_field.cu:299 (external linkage there; launched here by its host stub)
+__global__ void compute_voxel_knn_kernel(const TSDFVoxel* voxels, int3 dims, float3 origin, float voxel_size,
+                                         const DeformNode* nodes, int num_nodes, int* knn_ids, float* knn_ws);
+
 namespace {
 struct RefKnn {
   TSDFVolume* vol = nullptr;
@@ -83,5 +87,24 @@ REF_EXPORT int refk_compute(void* hp, int* ids, float* ws, float* ms) {
     return -1;
   if (ws && cudaMemcpy(ws, h->knn_w.data, sizeof(float) * 4 * (size_t)h->V, cudaMemcpyDeviceToHost) != cudaSuccess)
     return -1;
+  return (int)cudaGetLastError();
+}
+
+// The kernel alone, as WarpField::compute_voxel_knn launches it (8x8 blocks,
+// one z slice per grid layer), into the outputs of the last refk_compute:
+// *ms by CUDA events around the launch on the legacy stream.
+REF_EXPORT int refk_kernel(void* hp, float* ms) {
+  RefKnn* h = (RefKnn*)hp;
+  if (!h->knn.data || !h->knn_w.data) return -1;
+  const TSDFVolume::Params& p = h->vol->params();
+  dim3 block(8, 8, 1);
+  dim3 grid((p.dims.x + block.x - 1) / block.x, (p.dims.y + block.y - 1) / block.y, p.dims.z);
+  cudaEventRecord(h->e0, 0);
+  compute_voxel_knn_kernel<<<grid, block>>>(h->vol->device_data(), p.dims, p.origin, p.voxel_size,
+                                            h->warp->device_nodes(), h->warp->num_nodes(), h->knn.data,
+                                            h->knn_w.data);
+  cudaEventRecord(h->e1, 0);
+  cudaEventSynchronize(h->e1);
+  if (ms) cudaEventElapsedTime(ms, h->e0, h->e1);
   return (int)cudaGetLastError();
 }

@@ -40,3 +40,9 @@ void instantiate_with_reference_types(cf::GaussNewtonSolver& solver, cf::WarpFie
                  0);
   cf::TSDFIntegrator::mark_optimized_voxels(corrs.data, ints, 0, tp.dims, 0, ints, ints);
 }
+
+// WarpField::compute_voxel_knn over the reference's TSDFVolume and DeviceArrays.
+void instantiate_voxel_knn(cf::WarpField<DeformNode, DualQuat>& warp, const TSDFVolume& volume,
+                           DeviceArray<int>& knn, DeviceArray<float>& knn_w) {
+  warp.compute_voxel_knn(volume, knn, knn_w);
+}

@@ -226,20 +226,22 @@ def test_full_frame_solve_at_solver_h_defaults_within_reference_cloud(p2):
     """The headline frame at the solver.h defaults (lambda_smooth 1, damping
     1e-2), 5 GN x 20 PCG.  The system is indefinite (dropped skin pairs), so
     both solvers' energies rise over the GN iterations and the reference's
-    own runs land far apart.  Ours must land inside that cloud: nearer to one
-    reference run than the reference's runs are to each other, in transforms
-    and in energy, with the energy rising in both."""
+    own runs land far apart (its float atomics change the rounding of every
+    run).  Ours must look like one more reference run: its median distance
+    to the reference's runs within 1.5x their median distance to each other,
+    its energy within the reference's range widened by half that range, and
+    the energy rising in both."""
     kw = dict(gn_iterations=5, pcg_iterations=20, pcg_tolerance=1e-4, lambda_smooth=1.0, lambda_damping=1e-2)
     T, st = ours_gn(p2, kw)
-    Trefs = ref_gn_runs(p2, kw, runs=6)
+    Trefs = ref_gn_runs(p2, kw, runs=10)
     e0 = O.energy(p2, p2.init_transforms, 1.0, nthreads=THREADS)
     e_ours = O.energy(p2, T, 1.0, nthreads=THREADS)
     e_refs = [O.energy(p2, t, 1.0, nthreads=THREADS) for t in Trefs]
-    t_diam = max(tdist(a, b) for a in Trefs for b in Trefs)
-    e_diam = max(e_refs) - min(e_refs)
+    d_ours = float(np.median([tdist(T, t) for t in Trefs]))
+    d_ref = float(np.median([tdist(a, b) for i, a in enumerate(Trefs) for b in Trefs[i + 1:]]))
+    lo, hi = min(e_refs), max(e_refs)
     print(f"solver.h defaults: energy {e0:.4g} -> ours {e_ours:.4g}, reference {[round(e, 4) for e in e_refs]}; "
-          f"transforms: ours to nearest reference run {min(tdist(T, t) for t in Trefs):.3g}, "
-          f"reference diameter {t_diam:.3g}")
-    assert e_ours > e0 and min(e_refs) > e0
-    assert min(tdist(T, t) for t in Trefs) <= t_diam
-    assert min(abs(e_ours - e) for e in e_refs) <= max(e_diam, E_TOL * e_ours)
+          f"transforms: median distance ours-reference {d_ours:.3g}, reference-reference {d_ref:.3g}")
+    assert e_ours > e0 and lo > e0
+    assert d_ours <= 1.5 * d_ref
+    assert lo - 0.5 * (hi - lo) <= e_ours <= hi + 0.5 * (hi - lo)

@@ -1,0 +1,149 @@
+"""The voxel kNN oracle (oracle/cf_oracle_voxelknn.c, restating
+compute_voxel_knn_kernel, src/warp_field.cu:299-405) against the golden
+fixture made by the reference's own kernel on a B200
+(tests/golden/make_voxelknn_golden.py), and against an independent numpy
+restatement of the same rule.
+
+Bars: ids bit for bit; weights within 2e-6 of the reference's (its build uses
+--use_fast_math: the approximate exp and divisions put its weights up to
+1.04e-6 from correctly rounded ones on the golden scene), within 1e-6 between
+IEEE implementations."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from cudafusion_b200 import synth
+from cudafusion_b200.types import NODE_DTYPE
+from conftest import ROOT
+
+GOLDEN = os.path.join(ROOT, "tests", "golden", "voxelknn_ref.npz")
+W_TOL = 1e-6      # between IEEE implementations (this oracle, the device kernel)
+W_TOL_REF = 2e-6  # against the reference's --use_fast_math weights
+
+
+def golden_case(z, name):
+    w = z[name + "_weights"]
+    vox = np.zeros((w.size, 3), np.float32)
+    vox[:, 0] = 1.0
+    vox[:, 1] = w
+    vox.view(np.uint32)[:, 2] = 0x00808080
+    params = dict(dims=z[name + "_dims"], origin=z[name + "_origin"], voxel_size=float(z[name + "_voxel_size"]))
+    nodes = z[name + "_nodes"].view(NODE_DTYPE)
+    return params, vox, nodes, z[name + "_ids"], z[name + "_ws"]
+
+
+def numpy_knn(vox, params, nodes, vidx):
+    """The reference's rule restated with numpy: for each listed voxel, the 4
+    smallest (squared distance, index) pairs among the nodes closer than
+    1e30, the squared distance as fmaf(dz, dz, fmaf(dy, dy, dx * dx)) (each
+    fused step evaluated in float64 from float32 operands and rounded to
+    float32: the fused result except in the rare double-rounding case, which
+    these samples do not meet)."""
+    dims = np.asarray(params["dims"], np.int64)
+    vs = np.float32(params["voxel_size"])
+    org = np.asarray(params["origin"], np.float32)
+    x = vidx % dims[0]
+    y = (vidx // dims[0]) % dims[1]
+    zz = vidx // (dims[0] * dims[1])
+    c = np.stack([(np.float32(v) + np.float32(0.5)) for v in (x.astype(np.float32), y.astype(np.float32),
+                                                              zz.astype(np.float32))], -1)
+    # fmaf(v + 0.5, vs, o): exact product in float64, one rounding
+    p = (c.astype(np.float64) * np.float64(vs) + org.astype(np.float64)).astype(np.float32)
+    q = nodes["pos"].astype(np.float32)
+    ids = np.full((len(vidx), 4), -1, np.int32)
+    for r in range(len(vidx)):
+        if not (vox[vidx[r], 1] > 0) and not np.isnan(vox[vidx[r], 1]):
+            continue
+        d = (p[r][None, :] - q).astype(np.float32).astype(np.float64)
+        d2 = (d[:, 0] ** 2).astype(np.float32)
+        d2 = (d[:, 1] ** 2 + d2.astype(np.float64)).astype(np.float32)
+        d2 = (d[:, 2] ** 2 + d2.astype(np.float64)).astype(np.float32)
+        ok = np.where(d2 < np.float32(1e30))[0]
+        order = ok[np.lexsort((ok, d2[ok]))][:4]
+        ids[r, : len(order)] = order
+    return ids
+
+
+@pytest.fixture(scope="module")
+def golden():
+    return np.load(GOLDEN)
+
+
+@pytest.mark.parametrize("name", ["scene", "lattice", "edge"])
+def test_oracle_matches_reference_kernel(golden, name):
+    params, vox, nodes, ids_ref, ws_ref = golden_case(golden, name)
+    ids, ws = O.voxel_knn(vox, params, nodes, nthreads=os.cpu_count() or 1)
+    assert np.array_equal(ids, ids_ref)
+    assert np.abs(ws - ws_ref).max() <= W_TOL_REF
+
+
+def test_golden_cases_cover_the_edges(golden):
+    """The fixture holds what the rule's edges need: exact ties (duplicated
+    nodes, the dyadic lattice), inactive, negative and NaN weights, fewer
+    valid nodes than 4 (NaN and far nodes never taken)."""
+    _, vox, nodes, ids, ws = golden_case(golden, "edge")
+    w = vox[:, 1]
+    assert np.all(ids[w <= 0] == -1) and np.all(ws[w <= 0] == 0)
+    nan_rows = np.isnan(w)
+    assert nan_rows.any() and np.all(ids[nan_rows][:, :2] >= 0)
+    assert not np.isin(ids, [1, 3]).any()  # the NaN node and the node beyond 1e30
+    assert np.all(ids[~(w <= 0)][:, 2:] == -1)
+    _, _, _, ids, _ = golden_case(golden, "lattice")
+    assert np.all(ids >= 0)
+    params, vox, nodes, ids, _ = golden_case(golden, "scene")
+    dup = len(nodes) - 24
+    pos = nodes["pos"]
+    active = ~(vox[:, 1] <= 0)
+    # a repeated position is listed only right after a lower index at the
+    # same position (its twin, or an earlier repeat of it)
+    hits = 0
+    for j in range(dup, len(nodes)):
+        rows, cols = np.where(ids == j)
+        hits += len(rows)
+        assert np.all(cols > 0)
+        prev = ids[rows, cols - 1]
+        assert np.all(prev < j) and np.all((pos[prev] == pos[j]).all(1))
+    assert hits > 0 and active.sum() > 1000
+
+
+@pytest.mark.parametrize("name", ["scene", "lattice", "edge"])
+def test_oracle_matches_numpy_restatement(golden, name):
+    params, vox, nodes, ids_ref, _ = golden_case(golden, name)
+    rng = np.random.default_rng(5)
+    V = vox.shape[0]
+    vidx = np.unique(np.concatenate([rng.integers(0, V, 1500), np.arange(min(V, 600))])).astype(np.int64)
+    ids, _ = O.voxel_knn_list(vox, params, nodes, vidx, nthreads=os.cpu_count() or 1)
+    assert np.array_equal(ids, numpy_knn(vox, params, nodes, vidx))
+    assert np.array_equal(ids, ids_ref[vidx])
+
+
+def test_oracle_weights_follow_the_skinning_rule(golden):
+    """exp(-d / (2 r^2)) normalised over the found nodes (src/warp_field.cu:
+    375-404), in float64 here; a voxel whose weights sum to 1e-8 or less
+    (far from every node: the exponentials underflow) keeps all-zero
+    weights (:398)."""
+    params, vox, nodes, ids, ws = golden_case(golden, "scene")
+    active = np.where(~(vox[:, 1] <= 0))[0][:3000]
+    oi, ow = O.voxel_knn_list(vox, params, nodes, active)
+    dims = np.asarray(params["dims"], np.int64)
+    x, y, zz = active % dims[0], (active // dims[0]) % dims[1], active // (dims[0] * dims[1])
+    p = np.stack([params["origin"][a] + (v + 0.5) * params["voxel_size"] for a, v in enumerate((x, y, zz))], -1)
+    q = nodes["pos"][oi].astype(np.float64)
+    d2 = ((p[:, None, :] - q) ** 2).sum(-1)
+    r = np.maximum(nodes["radius"][oi].astype(np.float64), 1e-6)
+    w = np.exp(-d2 / (2 * r * r))
+    tot = w.sum(1)
+    near = tot > 2e-8
+    far = tot < 0.5e-8
+    assert near.sum() > 1000 and far.any()
+    assert np.abs(ow[near] - w[near] / tot[near, None]).max() < 1e-5
+    assert np.abs(ow[near].sum(1) - 1).max() < 1e-6
+    assert np.all(ow[far] == 0)
+
+
+def test_no_nodes_leaves_the_field_untouched():
+    f = synth.voxelknn_frame(dims=(16, 16, 16), nodes_xy=(4, 3))
+    ids, ws = O.voxel_knn(f.voxels, f.params, f.nodes[:0])
+    assert np.all(ids == -2) and np.all(np.isnan(ws))
