@@ -17,10 +17,12 @@
  *     1e-6), normalised by their sum when it exceeds 1e-8 (:375-404).
  *
  * Arithmetic: the centre is fmaf(v + 0.5, voxel_size, origin) and the squared
- * distance fmaf(dz, dz, fmaf(dy, dy, dx * dx)) (the contractions of the
- * reference's device build, pinned by the golden fixture made from its
- * kernel); the weights use expf and IEEE division (the reference's build uses
- * --use_fast_math, so weights agree with it to rounding, not bit for bit).
+ * distance fmaf(dz, dz, fmaf(dx, dx, dy * dy)), the contraction of the
+ * reference's device build (pinned by the golden fixture made from its kernel
+ * and by the two voxels of the 256^3 benchmark volume whose order a different
+ * nesting changes); the weights use expf and IEEE division (the reference's
+ * build uses --use_fast_math, so weights agree with it to rounding, not bit
+ * for bit).
  */
 #include <math.h>
 #include <stddef.h>
@@ -35,7 +37,7 @@ static inline float vk_centre(long long v, float vs, float o) { return fmaf((flo
 
 static inline float vk_dist2(float px, float py, float pz, const float* q) {
   float dx = px - q[0], dy = py - q[1], dz = pz - q[2];
-  return fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+  return fmaf(dz, dz, fmaf(dx, dx, dy * dy));
 }
 
 /* One voxel's list; `vox` = the 12-byte voxel records as floats (tsdf,

@@ -37,7 +37,7 @@ def golden_case(z, name):
 def numpy_knn(vox, params, nodes, vidx):
     """The reference's rule restated with numpy: for each listed voxel, the 4
     smallest (squared distance, index) pairs among the nodes closer than
-    1e30, the squared distance as fmaf(dz, dz, fmaf(dy, dy, dx * dx)) (each
+    1e30, the squared distance as fmaf(dz, dz, fmaf(dx, dx, dy * dy)) (each
     fused step evaluated in float64 from float32 operands and rounded to
     float32: the fused result except in the rare double-rounding case, which
     these samples do not meet)."""
@@ -57,8 +57,8 @@ def numpy_knn(vox, params, nodes, vidx):
         if not (vox[vidx[r], 1] > 0) and not np.isnan(vox[vidx[r], 1]):
             continue
         d = (p[r][None, :] - q).astype(np.float32).astype(np.float64)
-        d2 = (d[:, 0] ** 2).astype(np.float32)
-        d2 = (d[:, 1] ** 2 + d2.astype(np.float64)).astype(np.float32)
+        d2 = (d[:, 1] ** 2).astype(np.float32)
+        d2 = (d[:, 0] ** 2 + d2.astype(np.float64)).astype(np.float32)
         d2 = (d[:, 2] ** 2 + d2.astype(np.float64)).astype(np.float32)
         ok = np.where(d2 < np.float32(1e30))[0]
         order = ok[np.lexsort((ok, d2[ok]))][:4]
