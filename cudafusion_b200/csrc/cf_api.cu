@@ -1782,6 +1782,12 @@ struct cf_raster {
   int cache_cap = 0;                   // triangles the cache and the list hold
   bool dirty = false;                  // a call failed after the buffer may have been written
   long long launches = 0;
+  // the launch sequence of a call, captured once and replayed while the
+  // call's arguments (and these buffers) are unchanged
+  cudaGraphExec_t graph_exec = nullptr;
+  std::vector<unsigned char> graph_key;
+  bool graph_failed = false;
+  long long graph_launches = 0;
 };
 
 cf_status cf_raster_create(int max_width, int max_height, cf_raster** out) {
@@ -1809,6 +1815,7 @@ cf_status cf_raster_create(int max_width, int max_height, cf_raster** out) {
 
 cf_status cf_raster_destroy(cf_raster* h) {
   if (!h) return CF_OK;
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   cudaFree(h->ztri);
   cudaFree(h->cache);
   cudaFree(h->big);
@@ -1817,43 +1824,149 @@ cf_status cf_raster_destroy(cf_raster* h) {
   return CF_OK;
 }
 
-cf_status cf_rasterize_live_surface(cf_raster* h, const float* d_canonical, const float* d_warped,
-                                    const int* d_triangles, int num_vertices, int num_triangles, const cf_camera* cam,
-                                    const cf_mat4* T_cam_world, const cf_voxel_grid* grid, float* d_live_vertices,
-                                    float* d_live_normals, int* d_hit_voxel_idx, void* stream) {
-  if (!h || !cam || !T_cam_world || !grid || num_vertices < 0 || num_triangles < 0) return CF_ERR_INVALID_ARG;
-  if (cam->width < 0 || cam->height < 0) return CF_ERR_INVALID_ARG;
-  if (cam->width > h->max_w || cam->height > h->max_h) return CF_ERR_CAPACITY;
-  if ((long long)cam->width * cam->height == 0) return CF_OK;
-  if (!d_live_vertices || !d_live_normals || !d_hit_voxel_idx) return CF_ERR_INVALID_ARG;
-  if (num_triangles > 0 && (!d_canonical || !d_warped || !d_triangles)) return CF_ERR_INVALID_ARG;
-  if (!(grid->voxel_size > 0.f) || grid->dims[0] < 0 || grid->dims[1] < 0 || grid->dims[2] < 0)
+namespace {
+
+// The arguments of one prediction (skin = false: the rasterisation alone).
+struct RasterCall {
+  bool skin;
+  const float* canon;
+  float* warped;
+  const int* tris;
+  int V, NT;
+  const cf_deform_node* nodes;
+  const cf_dual_quat* T;
+  int N;
+  const int* vk;
+  const float* vw;
+  cf_camera cam;
+  cf_mat4 Tcw;
+  cf_voxel_grid grid;
+  float *lv, *ln;
+  int* hit;
+};
+
+// Checks the call and readies the handle's buffers (their growth allocates
+// and synchronises; a failed earlier call's buffers are reset on the stream).
+cf_status raster_prepare(cf_raster* h, const RasterCall& c, cudaStream_t s) {
+  if (c.cam.width < 0 || c.cam.height < 0) return CF_ERR_INVALID_ARG;
+  if (c.cam.width > h->max_w || c.cam.height > h->max_h) return CF_ERR_CAPACITY;
+  if ((long long)c.cam.width * c.cam.height == 0) return CF_OK;
+  if (!c.lv || !c.ln || !c.hit) return CF_ERR_INVALID_ARG;
+  if (c.NT > 0 && (!c.canon || !c.warped || !c.tris)) return CF_ERR_INVALID_ARG;
+  if (!(c.grid.voxel_size > 0.f) || c.grid.dims[0] < 0 || c.grid.dims[1] < 0 || c.grid.dims[2] < 0)
     return CF_ERR_INVALID_ARG;
-  cudaStream_t s = (cudaStream_t)stream;
-  if (num_triangles > h->cache_cap) {  // grows with the mesh (synchronous allocation)
+  if (c.NT > h->cache_cap) {  // grows with the mesh (synchronous allocation)
     CF_TRY(cudaStreamSynchronize(s));
     cudaFree(h->cache);
     cudaFree(h->big);
     h->cache = nullptr;
     h->big = nullptr;
     h->cache_cap = 0;
-    CF_TRY(dalloc(&h->cache, (size_t)num_triangles * 7));
-    CF_TRY(dalloc(&h->big, (size_t)num_triangles));
-    h->cache_cap = num_triangles;
+    CF_TRY(dalloc(&h->cache, (size_t)c.NT * 7));
+    CF_TRY(dalloc(&h->big, (size_t)c.NT));
+    h->cache_cap = c.NT;
   }
   if (h->dirty) {
     CF_TRY(cudaMemsetAsync(h->ztri, 0xff, (size_t)h->max_w * h->max_h * sizeof(unsigned long long), s));
     CF_TRY(cudaMemsetAsync(h->big_count, 0, sizeof(int), s));
     h->dirty = false;
   }
-  const cudaError_t e = launch_raster(d_canonical, d_warped, d_triangles, num_vertices, num_triangles, cam,
-                                      T_cam_world, grid, h->ztri, h->cache, h->big, h->big_count, d_live_vertices,
-                                      d_live_normals, d_hit_voxel_idx, s, &h->launches);
-  if (e != cudaSuccess) {
-    h->dirty = true;
-    return from_cuda(e);
-  }
   return CF_OK;
+}
+
+// The call's launches (skinning, rasterisation, big boxes, resolve).
+cudaError_t raster_enqueue(cf_raster* h, const RasterCall& c, cudaStream_t s) {
+  if (c.skin && c.V > 0) {
+    cudaError_t e = launch_mesh_skin(c.canon, c.warped, c.V, &c.grid, c.nodes, c.T, c.N, c.vk, c.vw, s);
+    if (e != cudaSuccess) return e;
+    h->launches += 1;
+  }
+  return launch_raster(c.canon, c.warped, c.tris, c.V, c.NT, &c.cam, &c.Tcw, &c.grid, h->ztri, h->cache, h->big,
+                       h->big_count, c.lv, c.ln, c.hit, s, &h->launches);
+}
+
+// On a stream of the caller's (not the legacy stream, not capturing), the
+// launches run as a CUDA graph captured on the first call and replayed while
+// the arguments and the handle's buffers are unchanged (the line search
+// predicts eleven times with the same ones); otherwise they are launched
+// directly.
+cf_status raster_run(cf_raster* h, const RasterCall& c, cudaStream_t s) {
+  cf_status st = raster_prepare(h, c, s);
+  if (st != CF_OK || (long long)c.cam.width * c.cam.height == 0) return st;
+  auto direct = [&]() -> cf_status {
+    const cudaError_t e = raster_enqueue(h, c, s);
+    if (e != cudaSuccess) {
+      h->dirty = true;
+      return from_cuda(e);
+    }
+    return CF_OK;
+  };
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (s == nullptr || cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    return direct();
+  }
+  std::vector<unsigned char> key(sizeof(RasterCall) + 3 * sizeof(void*));
+  const void* bufs[3] = {h->cache, h->big, h->ztri};
+  memcpy(key.data(), &c, sizeof(RasterCall));
+  memcpy(key.data() + sizeof(RasterCall), bufs, sizeof(bufs));
+  if (key == h->graph_key) {
+    if (h->graph_failed) return direct();
+    h->launches += h->graph_launches;
+    CF_TRY(cudaGraphLaunch(h->graph_exec, s));
+    return CF_OK;
+  }
+  if (h->graph_exec) {
+    cudaGraphExecDestroy(h->graph_exec);
+    h->graph_exec = nullptr;
+  }
+  h->graph_key = key;
+  h->graph_failed = false;
+  const long long before = h->launches;
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    e = raster_enqueue(h, c, s);
+    const cudaError_t e2 = cudaStreamEndCapture(s, &g);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&h->graph_exec, g, 0);
+  }
+  if (g) cudaGraphDestroy(g);
+  h->graph_launches = h->launches - before;
+  h->launches = before;
+  if (e != cudaSuccess) {  // not capturable here: remember, and launch directly
+    cudaGetLastError();
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    h->graph_exec = nullptr;
+    h->graph_failed = true;
+    return direct();
+  }
+  h->launches += h->graph_launches;
+  CF_TRY(cudaGraphLaunch(h->graph_exec, s));
+  return CF_OK;
+}
+
+}  // namespace
+
+cf_status cf_rasterize_live_surface(cf_raster* h, const float* d_canonical, const float* d_warped,
+                                    const int* d_triangles, int num_vertices, int num_triangles, const cf_camera* cam,
+                                    const cf_mat4* T_cam_world, const cf_voxel_grid* grid, float* d_live_vertices,
+                                    float* d_live_normals, int* d_hit_voxel_idx, void* stream) {
+  if (!h || !cam || !T_cam_world || !grid || num_vertices < 0 || num_triangles < 0) return CF_ERR_INVALID_ARG;
+  RasterCall c{};
+  c.skin = false;
+  c.canon = d_canonical;
+  c.warped = const_cast<float*>(d_warped);
+  c.tris = d_triangles;
+  c.V = num_vertices;
+  c.NT = num_triangles;
+  c.cam = *cam;
+  c.Tcw = *T_cam_world;
+  c.grid = *grid;
+  c.lv = d_live_vertices;
+  c.ln = d_live_normals;
+  c.hit = d_hit_voxel_idx;
+  return raster_run(h, c, (cudaStream_t)stream);
 }
 
 cf_status cf_predict_live_surface(cf_raster* h, const float* d_canonical, float* d_warped, const int* d_triangles,
@@ -1862,13 +1975,46 @@ cf_status cf_predict_live_surface(cf_raster* h, const float* d_canonical, float*
                                   const float* d_voxel_knn_w, const cf_camera* cam, const cf_mat4* T_cam_world,
                                   const cf_voxel_grid* grid, float* d_live_vertices, float* d_live_normals,
                                   int* d_hit_voxel_idx, void* stream) {
-  if (!h) return CF_ERR_INVALID_ARG;
-  cf_status st = cf_skin_mesh_vertices(d_canonical, d_warped, num_vertices, grid, d_nodes, d_transforms, num_nodes,
-                                       d_voxel_knn, d_voxel_knn_w, stream);
-  if (st != CF_OK) return st;
-  if (num_vertices > 0) h->launches += 1;
-  return cf_rasterize_live_surface(h, d_canonical, d_warped, d_triangles, num_vertices, num_triangles, cam,
-                                   T_cam_world, grid, d_live_vertices, d_live_normals, d_hit_voxel_idx, stream);
+  if (!h || !cam || !T_cam_world || !grid || num_vertices < 0 || num_triangles < 0 || num_nodes < 0)
+    return CF_ERR_INVALID_ARG;
+  // the checks of cf_skin_mesh_vertices
+  if (num_vertices > 0) {
+    if (!d_canonical || !d_warped) return CF_ERR_INVALID_ARG;
+    if (!(grid->voxel_size > 0.f) || grid->dims[0] < 0 || grid->dims[1] < 0 || grid->dims[2] < 0)
+      return CF_ERR_INVALID_ARG;
+    if ((long long)grid->dims[0] * grid->dims[1] * grid->dims[2] > (1LL << 31) / CF_K_NEIGHBORS)
+      return CF_ERR_CAPACITY;
+  }
+  RasterCall c{};
+  c.skin = true;
+  c.canon = d_canonical;
+  c.warped = d_warped;
+  c.tris = d_triangles;
+  c.V = num_vertices;
+  c.NT = num_triangles;
+  c.nodes = d_nodes;
+  c.T = d_transforms;
+  c.N = num_nodes;
+  c.vk = d_voxel_knn;
+  c.vw = d_voxel_knn_w;
+  c.cam = *cam;
+  c.Tcw = *T_cam_world;
+  c.grid = *grid;
+  c.lv = d_live_vertices;
+  c.ln = d_live_normals;
+  c.hit = d_hit_voxel_idx;
+  const cudaStream_t s = (cudaStream_t)stream;
+  // with an empty image the skinning alone runs (the rasterisation has nothing to draw)
+  if ((long long)cam->width * cam->height == 0) {
+    if (cam->width < 0 || cam->height < 0) return CF_ERR_INVALID_ARG;
+    if (num_vertices > 0) {
+      CF_TRY(launch_mesh_skin(d_canonical, d_warped, num_vertices, grid, d_nodes, d_transforms, num_nodes,
+                              d_voxel_knn, d_voxel_knn_w, s));
+      h->launches += 1;
+    }
+    return CF_OK;
+  }
+  return raster_run(h, c, s);
 }
 
 cf_status cf_raster_launch_count(const cf_raster* h, long long* launches) {
