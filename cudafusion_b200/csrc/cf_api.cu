@@ -1777,8 +1777,8 @@ struct cf_raster {
   int max_w = 0, max_h = 0;
   unsigned long long* ztri = nullptr;  // per pixel: depth bits << 32 | triangle, all ones = empty
   float4* cache = nullptr;             // per triangle: projection, area, normal, corners (112 B)
-  int* big = nullptr;                  // triangles whose boxes exceed 64 pixels
-  int* big_count = nullptr;            // their number (reset by the resolve)
+  int* big = nullptr;                  // (triangle, first row item) of the boxes over 128 pixels
+  unsigned long long* big_ctr = nullptr;  // their number << 32 | row items (reset by the resolve)
   int cache_cap = 0;                   // triangles the cache and the list hold
   bool dirty = false;                  // a call failed after the buffer may have been written
   long long launches = 0;
@@ -1801,11 +1801,11 @@ cf_status cf_raster_create(int max_width, int max_height, cf_raster** out) {
   const size_t P = (size_t)max_width * max_height;
   cudaError_t e = dalloc(&h->ztri, P);
   if (e == cudaSuccess) e = cudaMemset(h->ztri, 0xff, P * sizeof(unsigned long long));
-  if (e == cudaSuccess) e = dalloc(&h->big_count, 1);
-  if (e == cudaSuccess) e = cudaMemset(h->big_count, 0, sizeof(int));
+  if (e == cudaSuccess) e = dalloc(&h->big_ctr, 1);
+  if (e == cudaSuccess) e = cudaMemset(h->big_ctr, 0, sizeof(unsigned long long));
   if (e != cudaSuccess) {
     cudaFree(h->ztri);
-    cudaFree(h->big_count);
+    cudaFree(h->big_ctr);
     delete h;
     return from_cuda(e);
   }
@@ -1819,7 +1819,7 @@ cf_status cf_raster_destroy(cf_raster* h) {
   cudaFree(h->ztri);
   cudaFree(h->cache);
   cudaFree(h->big);
-  cudaFree(h->big_count);
+  cudaFree(h->big_ctr);
   delete h;
   return CF_OK;
 }
@@ -1863,12 +1863,12 @@ cf_status raster_prepare(cf_raster* h, const RasterCall& c, cudaStream_t s) {
     h->big = nullptr;
     h->cache_cap = 0;
     CF_TRY(dalloc(&h->cache, (size_t)c.NT * 7));
-    CF_TRY(dalloc(&h->big, (size_t)c.NT));
+    CF_TRY(dalloc(&h->big, 2 * (size_t)c.NT));
     h->cache_cap = c.NT;
   }
   if (h->dirty) {
     CF_TRY(cudaMemsetAsync(h->ztri, 0xff, (size_t)h->max_w * h->max_h * sizeof(unsigned long long), s));
-    CF_TRY(cudaMemsetAsync(h->big_count, 0, sizeof(int), s));
+    CF_TRY(cudaMemsetAsync(h->big_ctr, 0, sizeof(unsigned long long), s));
     h->dirty = false;
   }
   return CF_OK;
@@ -1882,7 +1882,7 @@ cudaError_t raster_enqueue(cf_raster* h, const RasterCall& c, cudaStream_t s) {
     h->launches += 1;
   }
   return launch_raster(c.canon, c.warped, c.tris, c.V, c.NT, &c.cam, &c.Tcw, &c.grid, h->ztri, h->cache, h->big,
-                       h->big_count, c.lv, c.ln, c.hit, s, &h->launches);
+                       h->big_ctr, c.lv, c.ln, c.hit, s, &h->launches);
 }
 
 // On a stream of the caller's (not the legacy stream, not capturing), the

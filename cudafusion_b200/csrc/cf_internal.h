@@ -277,8 +277,8 @@ cudaError_t launch_mesh_skin(const float* canon, float* warped, int V, const cf_
                              cudaStream_t s);
 cudaError_t launch_raster(const float* canon, const float* warped, const int* tris, int V, int NT,
                           const cf_camera* cam, const cf_mat4* Tcw, const cf_voxel_grid* grid,
-                          unsigned long long* ztri, float4* cache, int* big, int* big_count, float* lv, float* ln,
-                          int* hit, cudaStream_t s, long long* launches);
+                          unsigned long long* ztri, float4* cache, int* big, unsigned long long* big_ctr, float* lv,
+                          float* ln, int* hit, cudaStream_t s, long long* launches);
 cudaError_t launch_corr_search(const cf_corr_frame* f, const cf_camera* cam, const cf_mat4* Tcw, const cf_mat4* Twc,
                                const cf_corr_params* p, const CorrScratch& sc, int chunks, cf_correspondence* out,
                                int* num_valid, int* stats, cudaStream_t s, long long* launches);

@@ -20,13 +20,14 @@
 //
 // Launches per frame: mesh_skin_kernel (one thread per vertex, when the caller
 // skins); raster_kernel (one thread per triangle: the set-up, the record the
-// resolve reads, and the pixels of a box of up to 64; a larger box goes to a
-// list); raster_big_kernel (one warp per listed triangle, its pixels shared
-// out over the lanes); resolve_kernel (one thread per pixel; it writes every pixel
-// and resets the depth buffer and the list for the next frame, which replaces
-// the reference's three memsets).  A pixel centre is tested against each edge
-// without dividing unless the edge value lies within a narrow band of the
-// threshold.
+// resolve reads, and the pixels of a box of up to 128; a larger box goes to a
+// list as row items); raster_big_kernel (one warp per row item, the row's
+// pixels shared out over the lanes); resolve_kernel (one thread per two
+// pixels; it writes every pixel and resets the depth buffer and the list for
+// the next frame, which replaces the reference's three memsets).  Only the
+// pixels of each row's conservative span are tested (a pixel outside it
+// cannot pass), and a pixel centre is tested against each edge without
+// dividing unless the edge value lies within a narrow band of the threshold.
 #include <cmath>
 
 #include "cf_device.cuh"
@@ -167,7 +168,7 @@ __device__ __forceinline__ bool rs_out(const RsEdgeTest& g, float e, float area)
 // corners, the area, the face normal and the warped and canonical corners,
 // 7 float4 (112 B), so that a pixel's owner is one record away.
 constexpr int kRsRec = 7;
-constexpr int kRsSmallBox = 64;  // boxes up to this many pixels: one thread; larger: one warp
+constexpr int kRsSmallBox = 128;  // boxes up to this many pixels: one thread; larger: one warp
 
 // A drawn triangle's set-up in registers.
 struct RsTri {
@@ -237,78 +238,171 @@ __device__ __forceinline__ bool rs_setup(int ti, const float* __restrict__ canon
   return true;
 }
 
-// One thread per triangle: a box of up to kRsSmallBox pixels is drawn here;
-// a larger one goes to the big list for raster_big_kernel.
-__global__ void __launch_bounds__(256) raster_kernel(const float* __restrict__ canon, const float* __restrict__ warped,
-                                                     const int3* __restrict__ tris, int V, int NT,
-                                                     const RasterConsts k, unsigned long long* __restrict__ ztri,
-                                                     float4* __restrict__ cache, int* __restrict__ big,
-                                                     int* __restrict__ big_count) {
+// Row spans: the pixels of a row whose centres can pass the edge tests.  For
+// edge i, from a to b, the test computes e = fmaf(dx, B, -(dy * C)) with
+// dx = q.x - a.x, dy = q.y - a.y, B = b.y - a.y and C = b.x - a.x each
+// rounded once, so |e - (X B - Y C)| <= 3.01 u (|X||B| + |Y||C|) + 2^-140
+// for the exact X = q.x - a.x, Y = q.y - a.y (u = 2^-24; the last term for
+// results in the subnormal range).  A centre passes only when s e >= Lb (s the
+// sign of the area, Lb the outer edge of the test's band), hence only when
+// s (X B - Y C) >= Lb - 4u (Xmax |B| + |Y||C|) - 2^-140, Xmax bounding |X|
+// over the box.  For B != 0 that bounds X in each row: X >= R + Y C/B -
+// 4u |Y||C/B| when s B > 0, X <= R + Y C/B + 4u |Y||C/B| when s B < 0, with
+// R = (Lb - 4u Xmax |B| - 2^-140) / (s B).  The float evaluation of the
+// bound, fmaf(q.y - a.y, C/B, base), is widened by 32u times the magnitudes
+// it combines, which exceeds the sum of its rounding errors and of the
+// 4u |Y||C/B| term.  An edge with B == 0 bounds nothing; since the rounded
+// B of the three edges are the signed differences of the corners' y, a
+// triangle of nonzero area has an edge of each sign, so every row gets a
+// lower and an upper bound.  A pixel outside its row's span fails the
+// reference's test, so skipping it leaves the depth keys unchanged.
+struct RsSpan {
+  float ay[3], slope[3], base[3];
+  int kind[3];  // +1: lower bound on x, -1: upper bound, 0: none
+};
+
+__device__ __forceinline__ void rs_span_edge(float2 a, float2 b, float s, float Lb, float xlo, float xhi, float ylo,
+                                             float yhi, float& ay, float& slope, float& base, int& kind) {
+  constexpr float u = 0x1p-24f;
+  const float B = __fsub_rn(b.y, a.y), C = __fsub_rn(b.x, a.x);
+  ay = a.y;
+  slope = 0.f;
+  base = 0.f;
+  kind = 0;
+  if (B == 0.f) return;
+  const float sB = s * B;
+  const float xmax = fmaxf(fabsf(__fsub_rn(xlo, a.x)), fabsf(__fsub_rn(xhi, a.x)));
+  const float ymax = fmaxf(fabsf(__fsub_rn(ylo, a.y)), fabsf(__fsub_rn(yhi, a.y)));
+  const float ex = __fmul_rn(__fmul_rn(xmax, fabsf(B)), 5.f * u);  // >= 4u Xmax |B| after its own roundings
+  const float R = __fdiv_rn(__fsub_rn(__fsub_rn(Lb, ex), 0x1p-140f), sB);
+  slope = __fdiv_rn(C, B);
+  const float mag = __fadd_rn(__fadd_rn(__fmul_rn(fabsf(slope), ymax), fabsf(a.x)), __fadd_rn(fabsf(R), 1.f));
+  const float margin = __fadd_rn(__fmul_rn(mag, 32.f * u), 1e-6f);
+  kind = sB > 0.f ? 1 : -1;
+  // the pixel index bound: x >= bound - 0.5 (lower) or x <= bound - 0.5 (upper)
+  base = __fsub_rn(__fadd_rn(a.x, R), 0.5f);
+  base = kind > 0 ? __fsub_rn(base, margin) : __fadd_rn(base, margin);
+}
+
+__device__ __forceinline__ void rs_span_setup(const RsTri& r, RsSpan& sp) {
+  const float s = r.area > 0.f ? 1.f : -1.f;
+  const float Lb = r.area > 0.f ? r.lo : -r.hi;
+  const float xlo = __fadd_rn((float)r.min_u, 0.5f), xhi = __fadd_rn((float)(r.min_u + r.bw - 1), 0.5f);
+  const float ylo = __fadd_rn((float)r.min_v, 0.5f), yhi = __fadd_rn((float)(r.min_v + r.bh - 1), 0.5f);
+  rs_span_edge(r.p1, r.p2, s, Lb, xlo, xhi, ylo, yhi, sp.ay[0], sp.slope[0], sp.base[0], sp.kind[0]);
+  rs_span_edge(r.p2, r.p0, s, Lb, xlo, xhi, ylo, yhi, sp.ay[1], sp.slope[1], sp.base[1], sp.kind[1]);
+  rs_span_edge(r.p0, r.p1, s, Lb, xlo, xhi, ylo, yhi, sp.ay[2], sp.slope[2], sp.base[2], sp.kind[2]);
+}
+
+// The span [x0, x1] of row y, inside the box (empty when x0 > x1).  A NaN
+// bound (an infinite slope at a zero offset) is ignored by fmaxf / fminf.
+__device__ __forceinline__ void rs_span_row(const RsTri& r, const RsSpan& sp, int y, int& x0, int& x1) {
+  const float qy = __fadd_rn((float)y, 0.5f);
+  float lo = -1e9f, hi = 1e9f;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const float t = fmaf(__fsub_rn(qy, sp.ay[i]), sp.slope[i], sp.base[i]);
+    if (sp.kind[i] > 0) lo = fmaxf(lo, t);
+    if (sp.kind[i] < 0) hi = fminf(hi, t);
+  }
+  x0 = max(r.min_u, __float2int_ru(fminf(lo, 1e9f)));
+  x1 = min(r.min_u + r.bw - 1, __float2int_rd(fmaxf(hi, -1e9f)));
+}
+
+// One thread per triangle: the set-up, the record, and the pixels of a box
+// of up to kRsSmallBox, row by row over the rows' spans.  A larger box joins
+// the big list as one entry and ceil(rows / G) row items: a single 64-bit
+// atomic on big_ctr (entries in the high word, items in the low word) gives
+// the entry its index and its first item, so the entries' first items
+// increase with their index.  128-thread CTAs at 9 per SM: 5120 warps of a
+// 164k-triangle mesh fit in one wave.
+__global__ void __launch_bounds__(128, 9) raster_kernel(const float* __restrict__ canon, const float* __restrict__ warped,
+                                                        const int3* __restrict__ tris, int V, int NT,
+                                                        const RasterConsts k, int G,
+                                                        unsigned long long* __restrict__ ztri,
+                                                        float4* __restrict__ cache, int2* __restrict__ big,
+                                                        unsigned long long* __restrict__ big_ctr) {
   const int ti = blockIdx.x * blockDim.x + threadIdx.x;
   if (ti >= NT) return;
   RsTri r;
   if (!rs_setup(ti, canon, warped, tris, V, k, cache, r)) return;
   if (r.bw * r.bh > kRsSmallBox) {
-    big[atomicAdd(big_count, 1)] = ti;
+    const unsigned items = (unsigned)((r.bh + G - 1) / G);
+    const unsigned long long old = atomicAdd(big_ctr, (1ull << 32) | items);
+    big[(int)(old >> 32)] = make_int2(ti, (int)(unsigned)old);
     return;
   }
-  for (int y = r.min_v; y < r.min_v + r.bh; ++y)
-    for (int x = r.min_u; x < r.min_u + r.bw; ++x) rs_fragment(r, ti, x, y, k, ztri);
+  RsSpan sp;
+  rs_span_setup(r, sp);
+  for (int y = r.min_v; y < r.min_v + r.bh; ++y) {
+    int x0, x1;
+    rs_span_row(r, sp, y, x0, x1);
+    for (int x = x0; x <= x1; ++x) rs_fragment(r, ti, x, y, k, ztri);
+  }
 }
 
-// The big list, one warp per triangle: every lane repeats the set-up (the
-// same operations, so the same values) and the lanes stride over the box's
-// pixels.  The 64-bit min is order-free: the keys equal a sequential pass's.
+// The big list, one warp per row item: the warp finds the item's entry (the
+// last whose first item is at or below it) by a 32-way search, repeats the
+// entry's set-up (the same operations, so the same values) and shares each
+// row's span out over its lanes.  The 64-bit min is order-free: the keys
+// equal a sequential pass's.
 __global__ void __launch_bounds__(256) raster_big_kernel(const float* __restrict__ canon,
                                                          const float* __restrict__ warped,
                                                          const int3* __restrict__ tris, int V, const RasterConsts k,
-                                                         unsigned long long* __restrict__ ztri,
-                                                         const int* __restrict__ big,
-                                                         const int* __restrict__ big_count) {
+                                                         int G, unsigned long long* __restrict__ ztri,
+                                                         const int2* __restrict__ big,
+                                                         const unsigned long long* __restrict__ big_ctr) {
   const int lane = threadIdx.x & 31;
   const int warps = gridDim.x * (blockDim.x >> 5);
-  const int n = *big_count;
-  for (int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < n; w += warps) {
-    const int ti = big[w];
+  const unsigned long long ctr = *big_ctr;
+  const int n = (int)(ctr >> 32);
+  const unsigned total = (unsigned)ctr;
+  for (unsigned item = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); item < total; item += warps) {
+    // entries [lo, hi) hold the answer; big[lo].y <= item always (big[0].y == 0)
+    int lo = 0, hi = n;
+    while (hi - lo > 32) {
+      const int step = (hi - lo + 31) >> 5;
+      const int at = lo + lane * step;
+      const unsigned m = __ballot_sync(0xffffffffu, at < hi && (unsigned)big[at].y <= item);
+      const int last = 31 - __clz(m);  // lane 0 always qualifies
+      lo += last * step;
+      hi = min(hi, lo + step);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, lo + lane < hi && (unsigned)big[lo + lane].y <= item);
+    const int2 e = big[lo + 31 - __clz(m)];
     RsTri r;
-    if (!rs_setup(ti, canon, warped, tris, V, k, nullptr, r)) continue;  // drew in raster_kernel: cannot fail
-    const int cnt = r.bw * r.bh;
-    const float inv_w = 1.f / (float)r.bw;
-    for (int idx = lane; idx < cnt; idx += 32) {
-      int row = __float2int_rz((float)idx * inv_w);
-      if (row * r.bw > idx) --row;
-      if ((row + 1) * r.bw <= idx) ++row;
-      rs_fragment(r, ti, r.min_u + (idx - row * r.bw), r.min_v + row, k, ztri);
+    if (!rs_setup(e.x, canon, warped, tris, V, k, nullptr, r)) continue;  // drew in raster_kernel: cannot fail
+    RsSpan sp;
+    rs_span_setup(r, sp);
+    const int y0 = r.min_v + (int)(item - (unsigned)e.y) * G;
+    const int y1 = min(r.min_v + r.bh, y0 + G);
+    for (int y = y0; y < y1; ++y) {
+      int x0, x1;
+      rs_span_row(r, sp, y, x0, x1);
+      for (int x = x0 + lane; x <= x1; x += 32) rs_fragment(r, e.x, x, y, k, ztri);
     }
   }
 }
 
-__global__ void __launch_bounds__(256) resolve_kernel(const RasterConsts k, unsigned long long* __restrict__ ztri,
-                                                      const float4* __restrict__ cache, float* __restrict__ lv,
-                                                      float* __restrict__ ln, int* __restrict__ hit,
-                                                      int* __restrict__ big_count) {
-  const int px = blockIdx.x * blockDim.x + threadIdx.x;
-  if (px == 0) *big_count = 0;  // the big list is consumed: ready for the next frame
-  if (px >= k.W * k.H) return;
-  const unsigned long long packed = ztri[px];
-  ztri[px] = kRsEmpty;  // ready for the next frame
+// One thread per two pixels (px and px + half: both rows coalesced), every
+// load of both issued before either is used, so that the grid fits one wave.
+__device__ __forceinline__ void rs_resolve_px(const RasterConsts& k, int px, unsigned long long packed,
+                                              const float4 (&rc)[kRsRec], float* __restrict__ lv,
+                                              float* __restrict__ ln, int* __restrict__ hit) {
   float3 v = make_float3(0.f, 0.f, 0.f), n = v;
   int h = -1;
   if (packed != kRsEmpty) {
     // the owner's record: the projection, area, face normal and corners that
     // resolve_rasterized_triangles_kernel recomputes (src/mesh_raster_kernels.cu:162-199)
-    const int ti = (int)(packed & 0xffffffffull);
-    const float4* rec = cache + (size_t)kRsRec * ti;
-    const float4 r0 = rec[0], r1 = rec[1];
-    const float2 p[3] = {make_float2(r0.x, r0.y), make_float2(r0.z, r0.w), make_float2(r1.x, r1.y)};
-    const float area = r1.z;
+    const float2 p[3] = {make_float2(rc[0].x, rc[0].y), make_float2(rc[0].z, rc[0].w), make_float2(rc[1].x, rc[1].y)};
+    const float area = rc[1].z;
     float w0, w1, w2;
     const int y = px / k.W, x = px - y * k.W;
     if (rs_bary(p, area, make_float2(__fadd_rn((float)x, 0.5f), __fadd_rn((float)y, 0.5f)), w0, w1, w2)) {
-      const float4 r2 = rec[2], r3 = rec[3], r4 = rec[4], r5 = rec[5], r6 = rec[6];
+      const float4 r2 = rc[2], r3 = rc[3], r4 = rc[4], r5 = rc[5], r6 = rc[6];
       v = make_float3(rs_lerp3(w0, w1, w2, r2.z, r3.y, r4.x), rs_lerp3(w0, w1, w2, r2.w, r3.z, r4.y),
                       rs_lerp3(w0, w1, w2, r3.x, r3.w, r4.z));
-      n = make_float3(r1.w, r2.x, r2.y);
+      n = make_float3(rc[1].w, r2.x, r2.y);
       h = rs_voxel(k, make_float3(rs_lerp3(w0, w1, w2, r4.w, r5.z, r6.y), rs_lerp3(w0, w1, w2, r5.x, r5.w, r6.z),
                                   rs_lerp3(w0, w1, w2, r5.y, r6.x, r6.w)));
     }
@@ -320,6 +414,34 @@ __global__ void __launch_bounds__(256) resolve_kernel(const RasterConsts k, unsi
   ln[3 * px + 1] = n.y;
   ln[3 * px + 2] = n.z;
   hit[px] = h;
+}
+
+__global__ void __launch_bounds__(256) resolve_kernel(const RasterConsts k, unsigned long long* __restrict__ ztri,
+                                                      const float4* __restrict__ cache, float* __restrict__ lv,
+                                                      float* __restrict__ ln, int* __restrict__ hit,
+                                                      unsigned long long* __restrict__ big_ctr) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) *big_ctr = 0;  // the big list is consumed: ready for the next frame
+  const int P = k.W * k.H, half = (P + 1) >> 1;
+  if (t >= half) return;
+  const int pa = t, pb = t + half;
+  const bool hb = pb < P;
+  const unsigned long long ka = ztri[pa], kb = hb ? ztri[pb] : kRsEmpty;
+  ztri[pa] = kRsEmpty;  // ready for the next frame
+  if (hb) ztri[pb] = kRsEmpty;
+  float4 ra[kRsRec], rb[kRsRec];
+  if (ka != kRsEmpty) {
+    const float4* rec = cache + (size_t)kRsRec * (int)(ka & 0xffffffffull);
+#pragma unroll
+    for (int q = 0; q < kRsRec; ++q) ra[q] = rec[q];
+  }
+  if (kb != kRsEmpty) {
+    const float4* rec = cache + (size_t)kRsRec * (int)(kb & 0xffffffffull);
+#pragma unroll
+    for (int q = 0; q < kRsRec; ++q) rb[q] = rec[q];
+  }
+  rs_resolve_px(k, pa, ka, ra, lv, ln, hit);
+  if (hb) rs_resolve_px(k, pb, kb, rb, lv, ln, hit);
 }
 
 RasterConsts raster_consts(const cf_camera* cam, const cf_mat4* Tcw, const cf_voxel_grid* g) {
@@ -355,26 +477,31 @@ cudaError_t launch_mesh_skin(const float* canon, float* warped, int V, const cf_
 
 cudaError_t launch_raster(const float* canon, const float* warped, const int* tris, int V, int NT,
                           const cf_camera* cam, const cf_mat4* Tcw, const cf_voxel_grid* grid,
-                          unsigned long long* ztri, float4* cache, int* big, int* big_count, float* lv, float* ln,
-                          int* hit, cudaStream_t s, long long* launches) {
+                          unsigned long long* ztri, float4* cache, int* big, unsigned long long* big_ctr, float* lv,
+                          float* ln, int* hit, cudaStream_t s, long long* launches) {
   const RasterConsts k = raster_consts(cam, Tcw, grid);
   const int P = k.W * k.H;
   if (P == 0) return cudaSuccess;
   const int3* t3 = reinterpret_cast<const int3*>(tris);
+  int2* big2 = reinterpret_cast<int2*>(big);
   if (NT > 0) {
-    // the big list is at most NT long; its kernel strides over it, one warp per
-    // triangle, with a grid of 8 CTAs of 8 warps per SM
-    static int sms_times_8 = 0;
-    if (sms_times_8 == 0) {
+    // rows per big-list item: 1 unless NT * H items could pass 2^31 (the
+    // counter's low word then stays below 2^32)
+    const long long worst = (long long)NT * k.H;
+    const int G = worst < (1LL << 31) ? 1 : (int)((worst >> 31) + 1);
+    // the big list's kernel strides over the row items, one warp per item,
+    // with a grid of 2 CTAs of 8 warps per SM
+    static int sms_times_2 = 0;
+    if (sms_times_2 == 0) {
       int dev = 0, sms = 148;
       if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      sms_times_8 = 8 * sms;
+      sms_times_2 = 2 * sms;
     }
-    raster_kernel<<<(NT + 255) / 256, 256, 0, s>>>(canon, warped, t3, V, NT, k, ztri, cache, big, big_count);
-    raster_big_kernel<<<sms_times_8, 256, 0, s>>>(canon, warped, t3, V, k, ztri, big, big_count);
+    raster_kernel<<<(NT + 127) / 128, 128, 0, s>>>(canon, warped, t3, V, NT, k, G, ztri, cache, big2, big_ctr);
+    raster_big_kernel<<<sms_times_2, 256, 0, s>>>(canon, warped, t3, V, k, G, ztri, big2, big_ctr);
     *launches += 2;
   }
-  resolve_kernel<<<(P + 255) / 256, 256, 0, s>>>(k, ztri, cache, lv, ln, hit, big_count);
+  resolve_kernel<<<((P + 1) / 2 + 255) / 256, 256, 0, s>>>(k, ztri, cache, lv, ln, hit, big_ctr);
   *launches += 1;
   return cudaGetLastError();
 }

@@ -75,6 +75,86 @@ def test_degenerate_triangles(oracle):
     check_exact(oracle, g)
 
 
+def _screen_soup(width, height, n, seed):
+    """A triangle soup placed in screen space (camera at the origin) to
+    stress the per-row span bounds: corners on pixel centres and edges,
+    slivers at every angle (horizontal, within 1e-6 rad of it, vertical),
+    zero-width and sub-pixel triangles, boxes that leave the image, both
+    windings, and depths that interleave; the few image-sized triangles lie
+    behind the rest."""
+    rng = np.random.default_rng(seed)
+    uv = np.empty((n, 3, 2))
+    kind = rng.choice(5, n, p=[0.3, 0.3, 0.15, 0.2, 0.05])
+    c = np.stack([rng.uniform(-8, width + 8, n), rng.uniform(-8, height + 8, n)], 1)
+    # corners snapped to pixel centres, edges and quarter points
+    snap = np.floor(c)[:, None, :] + rng.integers(-6, 7, (n, 3, 2)) + rng.choice([0.0, 0.25, 0.5], (n, 3, 2))
+    # slivers: a long edge at a chosen angle, the third corner a hair off it
+    ang = rng.choice([0.0, 1e-6, 1e-3, np.pi / 2, np.pi / 4], n) + np.where(rng.random(n) < 0.3,
+                                                                           rng.uniform(0, np.pi, n), 0.0)
+    ln = rng.uniform(1, 60, n)
+    wd = rng.choice([0.0, 1e-6, 1e-4, 1e-2, 0.3], n)
+    d = np.stack([np.cos(ang), np.sin(ang)], 1)
+    nrm = np.stack([-d[:, 1], d[:, 0]], 1)
+    sliver = np.stack([c, c + ln[:, None] * d, c + 0.5 * ln[:, None] * d + wd[:, None] * nrm], 1)
+    tiny = c[:, None, :] + rng.uniform(-0.6, 0.6, (n, 3, 2))
+    flat = snap.copy()
+    flat[:, 1, 1] = flat[:, 0, 1]  # one edge on a row
+    large = rng.uniform(-0.5 * width, 1.5 * width, (n, 3, 2)) * np.array([1.0, height / width])
+    for k_, arr in enumerate([snap, sliver, tiny, flat, large]):
+        uv[kind == k_] = arr[kind == k_]
+    flip = rng.random(n) < 0.5
+    uv[flip] = uv[flip][:, ::-1]
+    z = rng.uniform(0.5, 3.0, (n, 3))
+    z[kind == 4] += 6.0  # the large ones behind the rest
+    return uv, z
+
+
+def test_adversarial_triangles_bit_exact(oracle):
+    """Each triangle's pixels are visited only within its rows' spans; pixels
+    outside them must fail the reference's edge test, so the maps equal the
+    oracle's, which tests every pixel of the box."""
+    base = synth.mesh_frame(160, 120, n_theta=32, n_axial=16, seed=79)
+    fx, fy, cx, cy = [float(v) for v in base.cam]
+    for seed, n in ((80, 6000), (81, 6000)):
+        uv, z = _screen_soup(base.width, base.height, n, seed)
+        pts = np.stack([(uv[..., 0] - cx) * z / fx, (uv[..., 1] - cy) * z / fy, z], -1).reshape(-1, 3)
+        pts = pts.astype(np.float32)
+        tris = np.arange(pts.shape[0], dtype=np.int32).reshape(-1, 3)
+        g = dataclasses.replace(base, triangles=tris, warped=pts, canonical=pts.copy(),
+                                T_cam_world=np.eye(4, dtype=np.float32))
+        lv, ln, hit, _ = check_exact(oracle, g)
+        assert (np.linalg.norm(lv, axis=1) > 0).mean() > 0.3
+        # most pixels belong to the small triangles, not the backdrop
+        _, _, _, keys = oracle.rasterize(g)
+        owners = np.unique(keys[keys != np.uint64(2**64 - 1)] & np.uint64(0xFFFFFFFF))
+        assert owners.size > n // 4
+
+
+def test_big_list_row_groups(oracle):
+    """A 16 x 140000 image and 16000 triangles: triangles x rows passes 2^31,
+    so each item of the big list covers two rows; tall triangles of 50 to
+    3000 rows go through it, among small ones."""
+    W, H, n = 16, 140000, 16000
+    rng = np.random.default_rng(82)
+    cam = np.array([100.0, 100.0, W / 2.0, H / 2.0], np.float32)
+    top = rng.uniform(-20, H + 20, n)
+    tall = rng.random(n) < 0.02
+    h = np.where(tall, rng.uniform(50, 3000, n), rng.uniform(0.5, 4, n))
+    uv = np.empty((n, 3, 2))
+    uv[:, 0] = np.stack([rng.uniform(-2, W + 2, n), top], 1)
+    uv[:, 1] = np.stack([rng.uniform(-2, W + 2, n), top + h * rng.uniform(0.3, 1.0, n)], 1)
+    uv[:, 2] = np.stack([rng.uniform(-2, W + 2, n), top + h], 1)
+    z = rng.uniform(0.5, 3.0, (n, 3))
+    fx, fy, cx, cy = [float(v) for v in cam]
+    pts = np.stack([(uv[..., 0] - cx) * z / fx, (uv[..., 1] - cy) * z / fy, z], -1).reshape(-1, 3).astype(np.float32)
+    base = synth.mesh_frame(64, 48, n_theta=32, n_axial=16, seed=83)
+    g = dataclasses.replace(base, width=W, height=H, cam=cam, triangles=np.arange(3 * n, dtype=np.int32).reshape(-1, 3),
+                            warped=pts, canonical=pts.copy(), T_cam_world=np.eye(4, dtype=np.float32))
+    assert n * H >= 2**31
+    lv, ln, hit, _ = check_exact(oracle, g)
+    assert (np.linalg.norm(lv, axis=1) > 0).mean() > 0.05
+
+
 def test_empty_mesh_and_buffer_reset(oracle):
     f = synth.mesh_frame(64, 48, n_theta=32, n_axial=16, seed=74)
     r = LiveSurfaceRaster(64, 48)
