@@ -120,7 +120,7 @@ void free_pattern(Pattern& p) {
 
 void free_work(Work& w) {
   dfree(w.pk_src); dfree(w.pk_dst); dfree(w.pk_nrm); dfree(w.pk_ids); dfree(w.pk_ws);
-  dfree(w.c_srcfw); dfree(w.c_nres); dfree(w.c_fr); dfree(w.cnt); dfree(w.node_total); dfree(w.row_order); dfree(w.inc_start);
+  dfree(w.c_srcfw); dfree(w.c_nres); dfree(w.c_fr); dfree(w.cnt); dfree(w.node_total); dfree(w.row_order); dfree(w.asm_meta); dfree(w.inc_start);
   dfree(w.inc); dfree(w.trip); dfree(w.ekeys); dfree(w.rhs); dfree(w.plain); dfree(w.x); dfree(w.z); dfree(w.p0); dfree(w.p1);
   dfree(w.partials); dfree(w.barrier); dfree(w.err); dfree(w.e_data_part); dfree(w.e_arap_part); dfree(w.stats); dfree(w.timers);
   dfree(w.nodes_cat); dfree(w.T_cat); dfree(w.r); dfree(w.ap); dfree(w.minv32);
@@ -141,7 +141,7 @@ cudaError_t alloc_work(Work& w, int max_nodes, int max_corrs, int bin_ctas_max) 
 #define A_(ptr, n) if ((e = dalloc(&(ptr), (n))) != cudaSuccess) return e
   A_(w.pk_src, M); A_(w.pk_dst, M); A_(w.pk_nrm, M); A_(w.pk_ids, M); A_(w.pk_ws, M);
   A_(w.c_srcfw, M); A_(w.c_nres, M); A_(w.c_fr, M);
-  A_(w.node_total, N); A_(w.row_order, N); A_(w.inc_start, N + 1);
+  A_(w.node_total, N); A_(w.row_order, N); A_(w.asm_meta, 3 * N); A_(w.inc_start, N + 1);
   A_(w.inc, 4 * M); A_(w.trip, 16 * M); A_(w.ekeys, 4 * M);
   A_(w.rhs, 6 * N); A_(w.plain, N); A_(w.x, 6 * N); A_(w.z, 6 * N); A_(w.p0, 6 * N); A_(w.p1, 6 * N);
   A_(w.partials, (size_t)2 * 3 * kMaxPcgCtas); A_(w.barrier, (size_t)kMaxPcgCtas); A_(w.err, 1);

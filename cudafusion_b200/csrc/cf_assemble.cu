@@ -155,6 +155,20 @@ __global__ void __launch_bounds__(kThreads) expand_kernel(Work w, Pattern pt, in
       }
       carry += __shfl_sync(0xffffffffu, incl, 31);
     }
+    // the assembly's metadata of this launch position, so that its first
+    // load is one 48-byte record instead of a chain of dependent lookups:
+    // {row, first incidence, incidences, diagonal position}, {upper blocks,
+    // first upper-block index, first ARAP incidence, ARAP incidences},
+    // {first block edge past the diagonal, block edges, entries, 0}
+    if (lane == 0) {
+      const int u0 = pt.ustart[r];
+      const int a0 = pt.arap_row_ptr[r], a1 = pt.arap_row_ptr[r + 1];
+      const int be0 = pt.arap_blk_ptr[u0 + 1], be1 = pt.arap_blk_ptr[u0 + nu];
+      int4* m = w.asm_meta + 3 * (size_t)blockIdx.x;
+      m[0] = make_int4(r, i0, i1 - i0, dpos);
+      m[1] = make_int4(nu, u0, a0, a1 - a0);
+      m[2] = make_int4(be0, be1 - be0, carry, 0);
+    }
   }
   __syncthreads();
   // ---- pass 2: stable scatter of the entries ----
@@ -285,10 +299,13 @@ __host__ __device__ constexpr int sym3(int p, int q) {
 //     blocks written with their transposes, the rhs and the row's ARAP energy.
 __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern pt, AsmArgs aa) {
   extern __shared__ float4 stage_buf[];
-  const int r = w.row_order[blockIdx.x], lane = lane_id(), wid = threadIdx.x >> 5;  // longest rows first
+  // the row's metadata (written by the expand, longest rows first)
+  const int4 m0 = __ldg(w.asm_meta + 3 * (size_t)blockIdx.x), m1 = __ldg(w.asm_meta + 3 * (size_t)blockIdx.x + 1),
+             m2 = __ldg(w.asm_meta + 3 * (size_t)blockIdx.x + 2);
+  const int r = m0.x, lane = lane_id(), wid = threadIdx.x >> 5;
   const int cap = aa.stage_cap;
-  const int i0 = w.inc_start[r], n_inc = w.inc_start[r + 1] - i0;
-  const int dpos = pt.diag_pos[r], nb = pt.row_ptr[r + 1] - dpos;  // upper blocks of the row, diagonal first
+  const int i0 = m0.y, n_inc = m0.z;
+  const int dpos = m0.w, nb = m1.x;  // upper blocks of the row, diagonal first
   const int U = pt.max_upper_row;
   const int Up = (U + 4) & ~3;
   float4* s_eterm = stage_buf + 3 * cap;     // [kRowEdges][7]: the row's share of its edges' diagonal terms
@@ -304,7 +321,7 @@ __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern p
   float* s_sum = s_part + (size_t)(U + kWarps) * kPartVals;       // [U][27] the blocks' sums
   RowRecords R;
   R.ns = min(n_inc, cap);
-  R.nt = min(pt.seg_off[dpos + nb - 1] + pt.seg_cnt[dpos + nb - 1] - 4 * i0, 4 * cap);
+  R.nt = min(m2.z, 4 * cap);
   R.s_u = stage_buf;
   R.s_n = stage_buf + cap;
   R.s_ws = stage_buf + 2 * cap;
@@ -314,10 +331,10 @@ __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern p
   R.trip = w.trip + 4 * (size_t)i0;
   R.xr = node_pos(aa.nodes, r);
   // block info, ARAP terms of the row's edges and of its blocks' edges
-  const int u0 = pt.ustart[r];
-  const int a0 = pt.arap_row_ptr[r], a1 = pt.arap_row_ptr[r + 1] - a0, na = min(a1, kRowEdges);
-  const int be0 = pt.arap_blk_ptr[u0 + 1];  // the row's off-diagonal upper blocks are u0+1 .. u0+nb-1
-  const int be1 = pt.arap_blk_ptr[u0 + nb] - be0, nbe = min(be1, kRowEdges);
+  const int u0 = m1.y;
+  const int a0 = m1.z, a1 = m1.w, na = min(a1, kRowEdges);
+  const int be0 = m2.x;  // the row's off-diagonal upper blocks are u0+1 .. u0+nb-1
+  const int be1 = m2.y, nbe = min(be1, kRowEdges);
   for (int k = threadIdx.x; k < nb; k += kThreads) {
     const int pos = dpos + k;
     s_blk[k] = make_int4(pt.seg_off[pos] - 4 * i0, pt.seg_cnt[pos], pt.col_idx[pos], pt.trans_pos[pos]);

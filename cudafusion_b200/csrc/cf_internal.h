@@ -135,6 +135,7 @@ struct Work {
   long long cnt_cap = 0;      // words allocated for cnt
   int* node_total = nullptr;  // [max_nodes]
   int* row_order = nullptr;   // [max_nodes] rows by decreasing incidence count (launch order of the per-row kernels)
+  int4* asm_meta = nullptr;   // [3*max_nodes] per launch position: the assembly's row metadata, written by the expand
   int* inc_start = nullptr;   // [max_nodes+1]
   int* inc = nullptr;         // [4*max_corrs]: (c << 2) | a
   int* trip = nullptr;        // [16*max_corrs]: (c << 4) | (a << 2) | b
