@@ -16,9 +16,9 @@
 // Parameters and activations are BF16 (parameters kept in FP32 for Adam and
 // rounded to BF16 after every step); every sum accumulates in FP32, in a
 // fixed order, so forward and gradients are deterministic.  The layers are
-// tiny (N x 128 x 64); each runs on CUDA cores from shared-memory tiles of 16
-// nodes (forward) or 32 (gradients, as per-CTA partial sums reduced in CTA
-// order).
+// tiny (N x 128 x 64): the forward runs on the tensor cores (BF16 mma.sync
+// over shared-memory tiles of 16 nodes), the gradients on CUDA cores over
+// tiles of 32 (per-CTA partial sums reduced in CTA order).
 #include <cuda_bf16.h>
 
 #include "cf_device.cuh"
@@ -40,30 +40,65 @@ static_assert(kParams == CF_MPNN_PARAMS, "parameter count");
 __device__ __forceinline__ float bf(__nv_bfloat16 v) { return __bfloat162float(v); }
 __device__ __forceinline__ __nv_bfloat16 tobf(float v) { return __float2bfloat16_rn(v); }
 
-// Forward of one message-passing layer over a tile of kFwdTile nodes:
-// out = act(W [in_i, mean_j in_j] + b).  FIRST: `in` is the FP32 feature
+// Forward of one message-passing layer over a tile of kFwdTile = 16 nodes on
+// the tensor cores: out = act(W [in_i, mean_j in_j] + b) as one
+// mma.sync.m16n8k16 (BF16 operands, FP32 accumulation) per 16 input columns
+// and 8 output units, a warp per 8 units.  FIRST: `in` is the FP32 feature
 // array (rounded to BF16 on load).  AGG=false (output layer): out = W in + b
-// + x[0:6] (FP32 out).  Latency-bound at this size, so every phase issues
-// all its loads before it uses them: the weights as 16-B chunks of 8 BF16,
-// the neighbour lists, then the neighbours' features; the products run
-// several nodes per thread in independent chains.  The sums keep the order
-// of a plain loop (bias, then k ascending; neighbours in list order).
+// + x[0:6] (FP32 out).  The node's own inputs are BF16 already; the FP32
+// neighbour mean enters as two BF16 terms, hi = bf16(mean) and lo =
+// bf16(mean - hi), both against the same weight columns, so it keeps ~16
+// significant bits.  Operands sit in shared memory as BF16 rows: each half of
+// [in, mean] padded with zeros to a multiple of 16 columns, W padded the same
+// way (and to a multiple of 8 units), row strides 8 elements past the padded
+// width so that the fragment loads of the 8 row groups x 4 column pairs hit
+// 32 distinct banks.  Loads are issued before use: the weights as 16-B chunks,
+// the neighbour lists, then the neighbours' features.  Accumulation: the bias,
+// then the 16-column steps in ascending order, then the mean's low terms.
 constexpr int kFwdTile = 16;
+template <int DIN, int DOUT, bool AGG>
+struct FwdShape {
+  static constexpr int DINP = (DIN + 15) / 16 * 16;
+  static constexpr int CAT = AGG ? 2 * DIN : DIN;      // the weight row's width in global memory
+  static constexpr int CATP = AGG ? 2 * DINP : DINP;   // ... padded, in shared memory
+  static constexpr int DOUTP = (DOUT + 7) / 8 * 8;
+  static constexpr int LD = CATP + 8;                  // BF16 row stride of sW and sX
+  static constexpr int LDL = DINP + 8;                 // ... of the mean's low terms
+  static constexpr int SMEM = (DOUTP * LD + kFwdTile * LD + (AGG ? kFwdTile * LDL : 0)) * 2 + DOUTP * 4;
+};
+
+__device__ __forceinline__ unsigned ld_bf16x2(const __nv_bfloat16* p) {
+  return *reinterpret_cast<const unsigned*>(p);
+}
+// D += A B: A 16x16 row-major (4 regs), B 16x8 column-major (2 regs), D 16x8 FP32
+__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], unsigned a0, unsigned a1, unsigned a2, unsigned a3,
+                                               unsigned b0, unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
 template <int DIN, int DOUT, bool FIRST, bool AGG, bool RELU>
 __global__ void __launch_bounds__(kThreads) layer_fwd(const void* in_, const int* __restrict__ nbr,
                                                       const float* __restrict__ inv_deg,
                                                       const __nv_bfloat16* __restrict__ W,
                                                       const __nv_bfloat16* __restrict__ b, void* out_,
                                                       const float* __restrict__ x_skip, int N) {
-  constexpr int CAT = AGG ? 2 * DIN : DIN;
+  using S = FwdShape<DIN, DOUT, AGG>;
+  constexpr int CAT = S::CAT, CATP = S::CATP, DINP = S::DINP, DOUTP = S::DOUTP, LD = S::LD, LDL = S::LDL;
   static_assert(CAT % 8 == 0, "weight rows in 16-B chunks");
-  extern __shared__ float fsm[];
-  float* sW = fsm;                 // [CAT][DOUT]: transposed, so that the lanes (consecutive
-                                   // output units) read consecutive banks
-  float* sB = sW + DOUT * CAT;     // [DOUT]
-  float* sX = sB + DOUT;           // [kFwdTile][CAT]
+  extern __shared__ __align__(16) unsigned char fsm_raw[];
+  __nv_bfloat16* sW = reinterpret_cast<__nv_bfloat16*>(fsm_raw);  // [DOUTP][LD]
+  __nv_bfloat16* sX = sW + DOUTP * LD;                            // [kFwdTile][LD]: in | mean (hi)
+  __nv_bfloat16* sLo = sX + kFwdTile * LD;                        // [kFwdTile][LDL]: mean (lo)
+  float* sB = reinterpret_cast<float*>(sLo + (AGG ? kFwdTile * LDL : 0));  // [DOUTP]
   const int tid = threadIdx.x;
   const int n0 = blockIdx.x * kFwdTile;
+  const __nv_bfloat16 zero = tobf(0.f);
+  // column c of a global weight row -> its padded column
+  auto wcol = [](int c) { return c < DIN ? c : DINP + (c - DIN); };
   {
     constexpr int NCH = DOUT * CAT / 8, PER = (NCH + kThreads - 1) / kThreads;
     uint4 wv[PER];
@@ -79,13 +114,23 @@ __global__ void __launch_bounds__(kThreads) layer_fwd(const void* in_, const int
         const __nv_bfloat16* h = reinterpret_cast<const __nv_bfloat16*>(&wv[j]);
 #pragma unroll
         for (int t = 0; t < 8; t++) {
-          const int idx = 8 * q + t, u = idx / CAT, k = idx % CAT;
-          sW[k * DOUT + u] = bf(h[t]);
+          const int idx = 8 * q + t, u = idx / CAT, c = idx % CAT;
+          sW[u * LD + wcol(c)] = h[t];
         }
       }
     }
+    // the padding (columns past each half's width, units past DOUT): zeros
+    constexpr int PADC = CATP - CAT;
+    if constexpr (PADC > 0) {
+      for (int e = tid; e < DOUT * PADC; e += kThreads) {
+        const int u = e / PADC, pc = e % PADC;
+        const int col = AGG ? (pc < DINP - DIN ? DIN + pc : DINP + DIN + (pc - (DINP - DIN))) : DIN + pc;
+        sW[u * LD + col] = zero;
+      }
+    }
+    for (int e = tid; e < (DOUTP - DOUT) * CATP; e += kThreads) sW[(DOUT + e / CATP) * LD + e % CATP] = zero;
   }
-  for (int k = tid; k < DOUT; k += kThreads) sB[k] = bf(b[k]);
+  for (int k = tid; k < DOUTP; k += kThreads) sB[k] = k < DOUT ? bf(b[k]) : 0.f;
   auto load_in = [&](int i, int k) -> float {
     if (FIRST) return bf(tobf(reinterpret_cast<const float*>(in_)[(size_t)i * DIN + k]));
     return bf(reinterpret_cast<const __nv_bfloat16*>(in_)[(size_t)i * DIN + k]);
@@ -117,8 +162,24 @@ __global__ void __launch_bounds__(kThreads) layer_fwd(const void* in_, const int
           a *= inv_deg[i];
         }
       }
-      sX[s * CAT + k] = v;
-      if (AGG) sX[s * CAT + DIN + k] = a;
+      sX[s * LD + k] = tobf(v);  // exact: v is a BF16 value
+      if (AGG) {
+        const __nv_bfloat16 hi = tobf(a);
+        sX[s * LD + DINP + k] = hi;
+        sLo[s * LDL + k] = tobf(a - bf(hi));
+      }
+    }
+    // the input padding columns: zeros
+    constexpr int PADX = DINP - DIN;
+    if constexpr (PADX > 0) {
+      for (int e = tid; e < kFwdTile * PADX; e += kThreads) {
+        const int s = e / PADX, k = DIN + e % PADX;
+        sX[s * LD + k] = zero;
+        if (AGG) {
+          sX[s * LD + DINP + k] = zero;
+          sLo[s * LDL + k] = zero;
+        }
+      }
     }
   }
   __syncthreads();
@@ -130,34 +191,36 @@ __global__ void __launch_bounds__(kThreads) layer_fwd(const void* in_, const int
       reinterpret_cast<float*>(out_)[(size_t)i * DOUT + u] = acc + x_skip[(size_t)i * kIn + u];
     }
   };
-  if constexpr (kFwdTile * DOUT >= kThreads && kThreads % DOUT == 0) {
-    // unit u = tid % DOUT, nodes tid / DOUT + r * (kThreads / DOUT): NR chains per thread
-    constexpr int SPR = kThreads / DOUT, NR = kFwdTile / SPR;
-    static_assert(kFwdTile % SPR == 0, "whole rounds of nodes");
-    const int u = tid % DOUT, s0 = tid / DOUT;
-    float acc[NR];
+  // fragments of m16n8k16: row group g = lane / 4, column pair t = lane % 4
+  const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+  for (int nt = warp; nt < DOUTP / 8; nt += kThreads / 32) {
+    const int u0 = nt * 8;
+    float d[4];
+    d[0] = d[2] = sB[u0 + 2 * t];
+    d[1] = d[3] = sB[u0 + 2 * t + 1];
+    const __nv_bfloat16* wr = sW + (u0 + g) * LD + 2 * t;
+    const __nv_bfloat16* x0 = sX + g * LD + 2 * t;
+    const __nv_bfloat16* x8 = sX + (g + 8) * LD + 2 * t;
 #pragma unroll
-    for (int r = 0; r < NR; r++) acc[r] = sB[u];
-#pragma unroll 8
-    for (int k = 0; k < CAT; k++) {
-      const float wk = sW[k * DOUT + u];
+    for (int k0 = 0; k0 < CATP; k0 += 16)
+      mma_bf16_16816(d, ld_bf16x2(x0 + k0), ld_bf16x2(x8 + k0), ld_bf16x2(x0 + k0 + 8), ld_bf16x2(x8 + k0 + 8),
+                     ld_bf16x2(wr + k0), ld_bf16x2(wr + k0 + 8));
+    if (AGG) {
+      const __nv_bfloat16* l0 = sLo + g * LDL + 2 * t;
+      const __nv_bfloat16* l8 = sLo + (g + 8) * LDL + 2 * t;
 #pragma unroll
-      for (int r = 0; r < NR; r++) acc[r] = fmaf(wk, sX[(s0 + r * SPR) * CAT + k], acc[r]);
+      for (int k0 = 0; k0 < DINP; k0 += 16)
+        mma_bf16_16816(d, ld_bf16x2(l0 + k0), ld_bf16x2(l8 + k0), ld_bf16x2(l0 + k0 + 8), ld_bf16x2(l8 + k0 + 8),
+                       ld_bf16x2(wr + DINP + k0), ld_bf16x2(wr + DINP + k0 + 8));
     }
 #pragma unroll
-    for (int r = 0; r < NR; r++) {
-      const int i = n0 + s0 + r * SPR;
-      if (i < N) store(i, u, acc[r]);
-    }
-  } else {
-    for (int e = tid; e < kFwdTile * DOUT; e += kThreads) {
-      const int s = e / DOUT, u = e % DOUT, i = n0 + s;
-      if (i >= N) continue;
-      float acc = sB[u];
-      const float* xx = sX + s * CAT;
-#pragma unroll 8
-      for (int k = 0; k < CAT; k++) acc = fmaf(sW[k * DOUT + u], xx[k], acc);
-      store(i, u, acc);
+    for (int h = 0; h < 2; h++) {
+      const int i = n0 + g + 8 * h;
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const int u = u0 + 2 * t + e;
+        if (i < N && u < DOUT) store(i, u, d[2 * h + e]);
+      }
     }
   }
 }
@@ -511,7 +574,6 @@ inline int cdiv(int a, int b) { return (a + b - 1) / b; }
 int mpnn_param_count() { return kParams; }
 
 static int layer_bwd_smem(int din) { return (kHid * 2 * din + kTileNodes * 2 * din + kTileNodes * kHid) * 4; }
-static int layer_fwd_smem(int cat, int dout) { return (dout * cat + dout + kFwdTile * cat) * 4; }
 
 template <typename T>
 static cudaError_t alloc_n(T** p, size_t n) {
@@ -565,7 +627,8 @@ cudaError_t mpnn_forward(const Mpnn& m, const float* feat, float* out, cudaStrea
   if (N <= 0) return cudaSuccess;
   const int g = cdiv(N, kFwdTile);
   const __nv_bfloat16* wb = reinterpret_cast<const __nv_bfloat16*>(m.wb);
-  const int s0 = layer_fwd_smem(2 * kIn, kHid), s1 = layer_fwd_smem(2 * kHid, kHid), so = layer_fwd_smem(kHid, kOut);
+  const int s0 = FwdShape<kIn, kHid, true>::SMEM, s1 = FwdShape<kHid, kHid, true>::SMEM,
+            so = FwdShape<kHid, kOut, false>::SMEM;
   cudaError_t e = cudaFuncSetAttribute(layer_fwd<kHid, kHid, false, true, true>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, s1);
   if (e != cudaSuccess) return e;
