@@ -1224,7 +1224,7 @@ def run_tsdf(args, world, rank, local):
     # for the voxels updated (the depth map and the nodes stay in L2)
     alg_bytes = 4 * V + 32 * gated_in + 16 * updated
     achieved = alg_bytes / (value * 1e-3) / 1e9
-    traffic = load_traffic("tsdf_integrate_kernel")
+    traffic = load_traffic("tsdf_gated_kernel")
     cpu = None
     if not args.no_cpu_baseline:
         import oracle as O
@@ -1268,7 +1268,7 @@ def run_tsdf(args, world, rank, local):
             "l2": "flushed between steps (256 MiB write)",
             "parallelism": f"replicas x{world}",
         },
-        "roofline": {"kernel": "tsdf_integrate_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm,
+        "roofline": {"kernel": "tsdf_gated_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm,
                      "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                      "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": value,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
