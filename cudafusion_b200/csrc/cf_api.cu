@@ -1780,6 +1780,8 @@ struct cf_raster {
   int* big = nullptr;                  // (triangle, first row item) of the boxes over 128 pixels
   unsigned long long* big_ctr = nullptr;  // their number << 32 | row items (reset by the resolve)
   int cache_cap = 0;                   // triangles the cache and the list hold
+  cf_dual_quat* plain = nullptr;       // per node: the plain DQ the skinning blends
+  int plain_cap = 0;
   bool dirty = false;                  // a call failed after the buffer may have been written
   long long launches = 0;
   // the launch sequence of a call, captured once and replayed while the
@@ -1820,6 +1822,7 @@ cf_status cf_raster_destroy(cf_raster* h) {
   cudaFree(h->cache);
   cudaFree(h->big);
   cudaFree(h->big_ctr);
+  cudaFree(h->plain);
   delete h;
   return CF_OK;
 }
@@ -1866,6 +1869,14 @@ cf_status raster_prepare(cf_raster* h, const RasterCall& c, cudaStream_t s) {
     CF_TRY(dalloc(&h->big, 2 * (size_t)c.NT));
     h->cache_cap = c.NT;
   }
+  if (c.skin && c.N > h->plain_cap) {  // grows with the graph (synchronous allocation)
+    CF_TRY(cudaStreamSynchronize(s));
+    cudaFree(h->plain);
+    h->plain = nullptr;
+    h->plain_cap = 0;
+    CF_TRY(dalloc(&h->plain, (size_t)c.N));
+    h->plain_cap = c.N;
+  }
   if (h->dirty) {
     CF_TRY(cudaMemsetAsync(h->ztri, 0xff, (size_t)h->max_w * h->max_h * sizeof(unsigned long long), s));
     CF_TRY(cudaMemsetAsync(h->big_ctr, 0, sizeof(unsigned long long), s));
@@ -1877,9 +1888,20 @@ cf_status raster_prepare(cf_raster* h, const RasterCall& c, cudaStream_t s) {
 // The call's launches (skinning, rasterisation, big boxes, resolve).
 cudaError_t raster_enqueue(cf_raster* h, const RasterCall& c, cudaStream_t s) {
   if (c.skin && c.V > 0) {
-    cudaError_t e = launch_mesh_skin(c.canon, c.warped, c.V, &c.grid, c.nodes, c.T, c.N, c.vk, c.vw, s);
+    // the nodes' plain DQs once, then the vertices (lists read 16 B at a
+    // time when aligned); without nodes the vertices are copied
+    const bool plain = c.N > 0 && c.nodes && c.T && c.vk && c.vw &&
+                       ((reinterpret_cast<uintptr_t>(c.vk) | reinterpret_cast<uintptr_t>(c.vw)) & 15u) == 0;
+    cudaError_t e;
+    if (plain) {
+      e = launch_tsdf_plain(c.nodes, c.T, h->plain, c.N, s);
+      if (e == cudaSuccess) e = launch_mesh_skin_plain(c.canon, c.warped, c.V, &c.grid, h->plain, c.N, c.vk, c.vw, s);
+      h->launches += 2;
+    } else {
+      e = launch_mesh_skin(c.canon, c.warped, c.V, &c.grid, c.nodes, c.T, c.N, c.vk, c.vw, s);
+      h->launches += 1;
+    }
     if (e != cudaSuccess) return e;
-    h->launches += 1;
   }
   return launch_raster(c.canon, c.warped, c.tris, c.V, c.NT, &c.cam, &c.Tcw, &c.grid, h->ztri, h->cache, h->big,
                        h->big_ctr, c.lv, c.ln, c.hit, s, &h->launches);
@@ -1906,8 +1928,8 @@ cf_status raster_run(cf_raster* h, const RasterCall& c, cudaStream_t s) {
     cudaGetLastError();
     return direct();
   }
-  std::vector<unsigned char> key(sizeof(RasterCall) + 3 * sizeof(void*));
-  const void* bufs[3] = {h->cache, h->big, h->ztri};
+  std::vector<unsigned char> key(sizeof(RasterCall) + 4 * sizeof(void*));
+  const void* bufs[4] = {h->cache, h->big, h->ztri, h->plain};
   memcpy(key.data(), &c, sizeof(RasterCall));
   memcpy(key.data() + sizeof(RasterCall), bufs, sizeof(bufs));
   if (key == h->graph_key) {

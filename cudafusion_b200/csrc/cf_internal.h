@@ -276,6 +276,8 @@ cudaError_t launch_voxel_knn(const float* vox, const cf_tsdf_params* p, const cf
 cudaError_t launch_mesh_skin(const float* canon, float* warped, int V, const cf_voxel_grid* grid,
                              const cf_deform_node* nodes, const cf_dual_quat* T, int N, const int* vk, const float* vw,
                              cudaStream_t s);
+cudaError_t launch_mesh_skin_plain(const float* canon, float* warped, int V, const cf_voxel_grid* grid,
+                                   const cf_dual_quat* plain, int N, const int* vk, const float* vw, cudaStream_t s);
 cudaError_t launch_raster(const float* canon, const float* warped, const int* tris, int V, int NT,
                           const cf_camera* cam, const cf_mat4* Tcw, const cf_voxel_grid* grid,
                           unsigned long long* ztri, float4* cache, int* big, unsigned long long* big_ctr, float* lv,

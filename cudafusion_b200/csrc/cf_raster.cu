@@ -141,6 +141,24 @@ __global__ void mesh_skin_kernel(const float* __restrict__ canon, float* __restr
   warped[3 * i + 2] = o.z;
 }
 
+// The same skinning from the nodes' plain dual quaternions (dq_centered of
+// each node, computed once per call by the caller's launch), blended as the
+// solve's skinning does: no per-vertex centring.  The lists are read as one
+// 16-byte load each.
+__global__ void mesh_skin_plain_kernel(const float* __restrict__ canon, float* __restrict__ warped, int V,
+                                       const RasterConsts k, const cf_dual_quat* __restrict__ plain, int N,
+                                       const int4* __restrict__ vk, const float4* __restrict__ vw) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V) return;
+  const float3 p = rs_ld3(canon, i);
+  float3 o = p;
+  const int v = rs_voxel(k, p);
+  if (v >= 0) o = blend_warp(p, __ldg(vk + v), __ldg(vw + v), plain, N);
+  warped[3 * i] = o.x;
+  warped[3 * i + 1] = o.y;
+  warped[3 * i + 2] = o.z;
+}
+
 // Whether e / area rounds below -1e-5f, mostly without the division: e is
 // compared with the exact threshold kRsOutside * area (an FP64 product of
 // 25- and 24-bit significands, so exact) through a float band around it
@@ -472,6 +490,16 @@ cudaError_t launch_mesh_skin(const float* canon, float* warped, int V, const cf_
   if (V <= 0) return cudaSuccess;
   const RasterConsts k = raster_consts(nullptr, nullptr, grid);
   mesh_skin_kernel<<<(V + 255) / 256, 256, 0, s>>>(canon, warped, V, k, nodes, T, N, vk, vw);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mesh_skin_plain(const float* canon, float* warped, int V, const cf_voxel_grid* grid,
+                                   const cf_dual_quat* plain, int N, const int* vk, const float* vw, cudaStream_t s) {
+  if (V <= 0) return cudaSuccess;
+  const RasterConsts k = raster_consts(nullptr, nullptr, grid);
+  mesh_skin_plain_kernel<<<(V + 255) / 256, 256, 0, s>>>(canon, warped, V, k, plain, N,
+                                                         reinterpret_cast<const int4*>(vk),
+                                                         reinterpret_cast<const float4*>(vw));
   return cudaGetLastError();
 }
 
