@@ -256,6 +256,33 @@ __device__ __forceinline__ bool rs_setup(int ti, const float* __restrict__ canon
   return true;
 }
 
+// A drawn triangle's set-up again, from its record in the cache: the same
+// fields rs_setup computed (the corners and area as stored, the band from the
+// area, each corner's camera depth from its warped corner, the box from the
+// corners), by the same operations.
+__device__ __forceinline__ void rs_from_record(const float4* __restrict__ rec, const RasterConsts& k, RsTri& r) {
+  const float4 r0 = rec[0], r1 = rec[1], r2 = rec[2], r3 = rec[3], r4 = rec[4];
+  const float2 p[3] = {make_float2(r0.x, r0.y), make_float2(r0.z, r0.w), make_float2(r1.x, r1.y)};
+  const float3 wc[3] = {make_float3(r2.z, r2.w, r3.x), make_float3(r3.y, r3.z, r3.w), make_float3(r4.x, r4.y, r4.z)};
+  const float* c = k.cw;
+  r.z0 = __fadd_rn(rs_dot(c[8], c[9], c[10], wc[0].x, wc[0].y, wc[0].z), c[11]);
+  r.z1 = __fadd_rn(rs_dot(c[8], c[9], c[10], wc[1].x, wc[1].y, wc[1].z), c[11]);
+  r.z2 = __fadd_rn(rs_dot(c[8], c[9], c[10], wc[2].x, wc[2].y, wc[2].z), c[11]);
+  r.min_u = max(0, __float2int_rd(fminf(p[0].x, fminf(p[1].x, p[2].x))));
+  const int max_u = min(k.W - 1, __float2int_ru(fmaxf(p[0].x, fmaxf(p[1].x, p[2].x))));
+  r.min_v = max(0, __float2int_rd(fminf(p[0].y, fminf(p[1].y, p[2].y))));
+  const int max_v = min(k.H - 1, __float2int_ru(fmaxf(p[0].y, fmaxf(p[1].y, p[2].y))));
+  const RsEdgeTest g = rs_edge_test(r1.z);
+  r.p0 = p[0];
+  r.p1 = p[1];
+  r.p2 = p[2];
+  r.area = r1.z;
+  r.lo = g.lo;
+  r.hi = g.hi;
+  r.bw = max_u - r.min_u + 1;
+  r.bh = max_v - r.min_v + 1;
+}
+
 // Row spans: the pixels of a row whose centres can pass the edge tests.  For
 // edge i, from a to b, the test computes e = fmaf(dx, B, -(dy * C)) with
 // dx = q.x - a.x, dy = q.y - a.y, B = b.y - a.y and C = b.x - a.x each
@@ -360,13 +387,11 @@ __global__ void __launch_bounds__(128, 9) raster_kernel(const float* __restrict_
 }
 
 // The big list, one warp per row item: the warp finds the item's entry (the
-// last whose first item is at or below it) by a 32-way search, repeats the
-// entry's set-up (the same operations, so the same values) and shares each
-// row's span out over its lanes.  The 64-bit min is order-free: the keys
+// last whose first item is at or below it) by a 32-way search, rebuilds the
+// entry's set-up from its record (the same values) and shares each row's span
+// out over its lanes.  The 64-bit min is order-free: the keys
 // equal a sequential pass's.
-__global__ void __launch_bounds__(256) raster_big_kernel(const float* __restrict__ canon,
-                                                         const float* __restrict__ warped,
-                                                         const int3* __restrict__ tris, int V, const RasterConsts k,
+__global__ void __launch_bounds__(256) raster_big_kernel(const float4* __restrict__ cache, const RasterConsts k,
                                                          int G, unsigned long long* __restrict__ ztri,
                                                          const int2* __restrict__ big,
                                                          const unsigned long long* __restrict__ big_ctr) {
@@ -389,7 +414,7 @@ __global__ void __launch_bounds__(256) raster_big_kernel(const float* __restrict
     const unsigned m = __ballot_sync(0xffffffffu, lo + lane < hi && (unsigned)big[lo + lane].y <= item);
     const int2 e = big[lo + 31 - __clz(m)];
     RsTri r;
-    if (!rs_setup(e.x, canon, warped, tris, V, k, nullptr, r)) continue;  // drew in raster_kernel: cannot fail
+    rs_from_record(cache + (size_t)kRsRec * e.x, k, r);
     RsSpan sp;
     rs_span_setup(r, sp);
     const int y0 = r.min_v + (int)(item - (unsigned)e.y) * G;
@@ -526,7 +551,7 @@ cudaError_t launch_raster(const float* canon, const float* warped, const int* tr
       sms_times_2 = 2 * sms;
     }
     raster_kernel<<<(NT + 127) / 128, 128, 0, s>>>(canon, warped, t3, V, NT, k, G, ztri, cache, big2, big_ctr);
-    raster_big_kernel<<<sms_times_2, 256, 0, s>>>(canon, warped, t3, V, k, G, ztri, big2, big_ctr);
+    raster_big_kernel<<<sms_times_2, 256, 0, s>>>(cache, k, G, ztri, big2, big_ctr);
     *launches += 2;
   }
   resolve_kernel<<<((P + 1) / 2 + 255) / 256, 256, 0, s>>>(k, ztri, cache, lv, ln, hit, big_ctr);
