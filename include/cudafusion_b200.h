@@ -530,9 +530,10 @@ CF_API cf_status cf_skin_mesh_vertices(const float* d_canonical, float* d_warped
                                        const float* d_voxel_knn_w, void* stream);
 
 /* Opaque raster handle: owns the 64-bit depth/triangle buffer of the largest
- * frame (8 B per pixel) and a per-triangle record and list (116 B per
- * triangle, allocated by the first call with a larger mesh, which then
- * synchronises `stream`). */
+ * frame (8 B per pixel), a per-triangle record and list entry (120 B per
+ * triangle) and, for cf_predict_live_surface, each node's plain dual
+ * quaternion (32 B per node); the latter two are allocated by the first call
+ * with a larger mesh or graph, which then synchronises `stream`. */
 typedef struct cf_raster cf_raster;
 CF_API cf_status cf_raster_create(int max_width, int max_height, cf_raster** out);
 CF_API cf_status cf_raster_destroy(cf_raster* h);
@@ -555,8 +556,12 @@ CF_API cf_status cf_rasterize_live_surface(cf_raster* h, const float* d_canonica
                                            float* d_live_normals, int* d_hit_voxel_idx, void* stream);
 
 /* rasterize_deformed_mesh_live_surface once the mesh is extracted: the
- * canonical vertices skinned into d_warped (cf_skin_mesh_vertices), then
- * rasterised and resolved (cf_rasterize_live_surface), on one stream.
+ * canonical vertices skinned into d_warped (the skinning of
+ * cf_skin_mesh_vertices, from each node's plain dual quaternion computed once
+ * per call on the handle when the voxel tables are 16-byte aligned), then
+ * rasterised and resolved (cf_rasterize_live_surface), on one stream.  On a
+ * stream of the caller's the launches are captured once and replayed as a
+ * CUDA graph while the arguments and the handle's buffers are unchanged.
  * Asynchronous on `stream`. */
 CF_API cf_status cf_predict_live_surface(cf_raster* h, const float* d_canonical, float* d_warped, const int* d_triangles,
                                          int num_vertices, int num_triangles, const cf_deform_node* d_nodes,
