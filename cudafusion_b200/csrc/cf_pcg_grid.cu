@@ -46,7 +46,7 @@ __host__ __device__ inline GLayout glayout(int nblk, int nrows, int nhalo, bool 
   L.minv = o; o += gal16(nrows * 36 * 8);
   L.scr = o; o += (kThreads / 8) * 72 * 8;  // inversion scratch, 72 doubles per 8-lane group
   L.st = o;
-  o += pipe ? gal16(nrows * 6 * 8) * 8 + gal16(nrows * 6 * 4) : gal16(nrows * 6 * 4) * 4 + gal16(nhalo * 6 * 4) * 2;
+  o += pipe ? gal16(nrows * 6 * 8) * 8 + gal16(nrows * 6 * 4) : gal16((nrows + nhalo) * 6 * 4) + gal16(nrows * 6 * 4) * 4;
   L.red = o; o += 64 * 8;
   L.tn = o; o += gal16(nrows * 48);  // per row: the transform and the node position, read in the prologue
   L.total = o;
@@ -298,13 +298,15 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
   double rr_last = 0.0;
   if (!PIPE) {
     // ================= standard PCG =================
-    const int vs = gal16(n6 * 4) / 4, hs = gal16(h6 * 4) / 4;
+    // sZ: z of own rows then halo; sV: the previous p, own rows then halo (the
+    // SpMV forms p = z + beta p_old as it reads, so p is never stored for the
+    // halo); sPn: this iteration's p of own rows
+    const int vs = gal16(n6 * 4) / 4, zs = gal16((n6 + h6) * 4) / 4;
     float* sZ = reinterpret_cast<float*>(smem + L.st);
-    float* sX = sZ + vs;
+    float* sX = sZ + zs;
     float* sR = sX + vs;
     float* sAp = sR + vs;
-    float* sHz = sAp + vs;
-    float* sHp = sHz + hs;
+    float* sPn = sAp + vs;
     // lanes per row element of the SpMV: 4, 2 or 1, as many as the CTA's threads allow
     const int spl_log = (n6 * 4 <= kThreads) ? 2 : (n6 * 2 <= kThreads) ? 1 : 0, spl = 1 << spl_log;
     double prz = 0.0, pbb = 0.0;
@@ -349,8 +351,8 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
         } else {
           for (int e = tid - 32; e < h6; e += kThreads - 32) {
             const int col = sHalo[e / 6], c = e % 6;
-            sHz[e] = __ldcg(w.z + col * 6 + c);
-            if (it > 0) sHp[e] = __ldcg(pold + col * 6 + c);
+            sZ[n6 + e] = __ldcg(w.z + col * 6 + c);
+            if (it > 0) sV[n6 + e] = __ldcg(pold + col * 6 + c);
           }
         }
         __syncthreads();
@@ -368,18 +370,13 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
         rz = rzn;
       }
       if (it >= a.pcg_iterations) break;
-      // ---- p = z + beta p_old on own rows and halo ----
-      for (int t = tid; t < n6; t += kThreads) {
-        const float pt_ = (it == 0) ? sZ[t] : __fmaf_rn(betaf, sV[t], sZ[t]);
-        sV[t] = pt_;
-        pnew[r0 * 6 + t] = pt_;
-      }
-      for (int e = tid; e < h6; e += kThreads) sV[n6 + e] = (it == 0) ? sHz[e] : __fmaf_rn(betaf, sHp[e], sHz[e]);
-      __syncthreads();
-      clk.mark(3);  // p update
-      // ---- Ap (solver_kernels.cu:406-432) and p.Ap ----
+      clk.mark(3);  // (p is formed inside the SpMV)
+      // ---- p = z + beta p_old and Ap (solver_kernels.cu:406-432), p.Ap ----
       // S adjacent lanes per row element, lane k over the row's blocks k, k+S, ...,
-      // combined by an xor butterfly: the CTA's time is its longest row / S
+      // combined by an xor butterfly: the CTA's time is its longest row / S.
+      // Each operand value is formed as it is read, fmaf(beta, p_old, z) (z
+      // alone in the first iteration), the value the p update would store.
+      const bool first = it == 0;
       double ppap = 0.0;
       for (int u0 = 0; u0 < n6 * spl; u0 += kThreads) {
         const int u = u0 + tid, t = u >> spl_log, k = u & (spl - 1);
@@ -388,15 +385,23 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
           const int i = t / 6, c = t % 6;
           for (int bl = sRow[i] + k; bl < sRow[i + 1]; bl += spl) {
             const float* Ab = A_SMEM ? (sA + bl * 36 + c * 6) : (gA + bl * 36 + c * 6);
-            const float* vv = sV + sVidx[bl] * 6;
+            const int o = sVidx[bl] * 6;
+            const float* zz = sZ + o;
+            const float* pp = sV + o;
 #pragma unroll
-            for (int q = 0; q < 6; q++) y = __fmaf_rn(A_SMEM ? Ab[q] : __ldcg(Ab + q), vv[q], y);
+            for (int q = 0; q < 6; q++) {
+              const float pv = first ? zz[q] : __fmaf_rn(betaf, pp[q], zz[q]);
+              y = __fmaf_rn(A_SMEM ? Ab[q] : __ldcg(Ab + q), pv, y);
+            }
           }
         }
         for (int o = spl >> 1; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
         if (k == 0 && t < n6) {
+          const float pt_ = first ? sZ[t] : __fmaf_rn(betaf, sV[t], sZ[t]);
+          sPn[t] = pt_;
+          pnew[r0 * 6 + t] = pt_;
           sAp[t] = y;
-          ppap += (double)sV[t] * y;
+          ppap += (double)pt_ * y;
         }
       }
       clk.mark(4);  // spmv
@@ -419,8 +424,9 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_grid_kernel(GridArgs P) {
       if (fabs(pAp) < 1e-12) break;  // solver_kernels.cu:647-653
       const float af = (float)(rz / pAp);
       for (int t = tid; t < n6; t += kThreads) {
-        sX[t] = __fmaf_rn(af, sV[t], sX[t]);
+        sX[t] = __fmaf_rn(af, sPn[t], sX[t]);
         sR[t] = __fmaf_rn(-af, sAp[t], sR[t]);
+        sV[t] = sPn[t];  // p_old of the next iteration
       }
       __syncthreads();
       double prr = 0.0, przn = 0.0;
