@@ -391,11 +391,18 @@ __device__ __forceinline__ bool cs_any_depth(const CorrConsts& k, const CsPixel&
 
 // Writes pixel px's record from its winner bi (-1: none) and adds the
 // pixel to the valid count and to its debug counter (code, -1: none), both
-// reduced per warp first.  Called by every thread of the warp.
+// reduced per warp first.  Called by every thread of the warp, whose lanes
+// hold consecutive pixels (the in-image ones a prefix): each lane's 19-word
+// record goes to the warp's staging area (kCsRecWords words per lane, in
+// shared memory), and the warp writes its records' words out in order, 32
+// consecutive words per store.
+constexpr int kCsRecWords = (int)(sizeof(cf_correspondence) / 4);
+static_assert(sizeof(cf_correspondence) == 4 * kCsRecWords, "a record is whole words");
 __device__ __forceinline__ void cs_emit(const CorrConsts& k, const CsPixel& p, bool inimg, int px, int bi, int code,
                                         const float4* __restrict__ A, const float2* __restrict__ B,
                                         const KnnSrc& knn, cf_correspondence* __restrict__ out,
-                                        int* __restrict__ num_valid, int* __restrict__ stats, int lane) {
+                                        int* __restrict__ num_valid, int* __restrict__ stats, int lane,
+                                        float* __restrict__ stage) {
   const bool valid = bi >= 0;
   if (inimg) {
     int ids[CF_K_NEIGHBORS];
@@ -454,18 +461,28 @@ __device__ __forceinline__ void cs_emit(const CorrConsts& k, const CsPixel& p, b
         ws[j] = 0.f;
       }
     }
-    float* o = reinterpret_cast<float*>(out + px);
+    float* o = stage + lane * kCsRecWords;
     o[0] = src.x; o[1] = src.y; o[2] = src.z;
     o[3] = dst.x; o[4] = dst.y; o[5] = dst.z;
     o[6] = nrm.x; o[7] = nrm.y; o[8] = nrm.z;
-    int* oi = reinterpret_cast<int*>(o + 9);
 #pragma unroll
     for (int j = 0; j < CF_K_NEIGHBORS; ++j) {
-      oi[j] = ids[j];
+      o[9 + j] = __int_as_float(ids[j]);
       o[13 + j] = ws[j];
     }
     o[17] = weight;
-    reinterpret_cast<int*>(o)[18] = valid ? 1 : 0;  // bool valid + 3 zero pad bytes
+    o[18] = __int_as_float(valid ? 1 : 0);  // bool valid + 3 zero pad bytes
+  }
+  {
+    const unsigned mi = __ballot_sync(0xffffffffu, inimg);
+    const int px0 = __shfl_sync(0xffffffffu, px, 0);
+    __syncwarp();
+    if (mi & 1u) {
+      float* dst = reinterpret_cast<float*>(out + px0);
+      const int words = __popc(mi) * kCsRecWords;
+      for (int w = lane; w < words; w += 32) dst[w] = stage[w];
+    }
+    __syncwarp();
   }
   const unsigned mv = __ballot_sync(0xffffffffu, valid);
   if (lane == 0 && mv) atomicAdd(num_valid, __popc(mv));
@@ -633,7 +650,9 @@ __global__ void __launch_bounds__(kCsThreads, kCsCtasPerSm)
         }
         code = bi >= 0 ? 5 : (saw_depth ? 3 : 2);
       }
-      cs_emit(k, p, img, px, bi, code, A, B, knn, out, num_valid, stats, threadIdx.x);
+      // the band buffer is free once every band is scanned: stage the records there
+      cs_emit(k, p, img, px, bi, code, A, B, knn, out, num_valid, stats, threadIdx.x,
+              reinterpret_cast<float*>(cs_smem) + threadIdx.y * (32 * kCsRecWords));
     }
   } else {
     if (img0) {
@@ -652,6 +671,7 @@ __global__ void __launch_bounds__(256)
                       const float4* __restrict__ A, const float2* __restrict__ B, const int* __restrict__ flag,
                       const float* __restrict__ part_pd, const int* __restrict__ part_idx, const KnnSrc knn,
                       cf_correspondence* __restrict__ out, int* __restrict__ num_valid, int* __restrict__ stats) {
+  __shared__ float s_stage[256 / 32][32 * kCsRecWords];
   const int px = blockIdx.x * blockDim.x + threadIdx.x;
   const bool inimg = px < k.P;
   CsPixel p;
@@ -678,7 +698,7 @@ __global__ void __launch_bounds__(256)
     }
     code = bi >= 0 ? 5 : (saw_depth ? 3 : 2);
   }
-  cs_emit(k, p, inimg, px, bi, code, A, B, knn, out, num_valid, stats, threadIdx.x & 31);
+  cs_emit(k, p, inimg, px, bi, code, A, B, knn, out, num_valid, stats, threadIdx.x & 31, s_stage[threadIdx.x >> 5]);
 }
 
 __global__ void pixel_knn_kernel(const int* __restrict__ hit, int P, const int* __restrict__ vk,
