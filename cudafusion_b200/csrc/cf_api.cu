@@ -1665,10 +1665,15 @@ struct cf_corr_search {
   cf::CorrScratch sc = {};
   int chunks = 0;  // row chunks per tile; 0 = chosen per frame
   long long launches = 0;
+  // cf_line_search: its best trial's outputs and the chain of best RMSEs
+  // (allocated by the first line search, grown with the frame)
+  unsigned char* keep = nullptr;
+  size_t keep_bytes = 0;
 };
 
 namespace {
 void corr_free(cf_corr_search* h) {
+  cudaFree(h->keep);
   cudaFree(h->sc.A);
   cudaFree(h->sc.B);
   cudaFree(h->sc.part_pd);
@@ -1885,8 +1890,8 @@ cf_status raster_prepare(cf_raster* h, const RasterCall& c, cudaStream_t s) {
   return CF_OK;
 }
 
-// The call's launches (skinning, rasterisation, big boxes, resolve).
-cudaError_t raster_enqueue(cf_raster* h, const RasterCall& c, cudaStream_t s) {
+// The call's skinning launches (when it skins).
+cudaError_t raster_skin(cf_raster* h, const RasterCall& c, cudaStream_t s) {
   if (c.skin && c.V > 0) {
     // the nodes' plain DQs once, then the vertices (lists read 16 B at a
     // time when aligned); without nodes the vertices are copied
@@ -1903,6 +1908,13 @@ cudaError_t raster_enqueue(cf_raster* h, const RasterCall& c, cudaStream_t s) {
     }
     if (e != cudaSuccess) return e;
   }
+  return cudaSuccess;
+}
+
+// The call's launches (skinning, rasterisation, big boxes, resolve).
+cudaError_t raster_enqueue(cf_raster* h, const RasterCall& c, cudaStream_t s) {
+  const cudaError_t e = raster_skin(h, c, s);
+  if (e != cudaSuccess) return e;
   return launch_raster(c.canon, c.warped, c.tris, c.V, c.NT, &c.cam, &c.Tcw, &c.grid, h->ztri, h->cache, h->big,
                        h->big_ctr, c.lv, c.ln, c.hit, s, &h->launches);
 }
@@ -1910,7 +1922,7 @@ cudaError_t raster_enqueue(cf_raster* h, const RasterCall& c, cudaStream_t s) {
 // On a stream of the caller's (not the legacy stream, not capturing), the
 // launches run as a CUDA graph captured on the first call and replayed while
 // the arguments and the handle's buffers are unchanged (the line search
-// predicts eleven times with the same ones); otherwise they are launched
+// predicts ten times with the same ones); otherwise they are launched
 // directly.
 cf_status raster_run(cf_raster* h, const RasterCall& c, cudaStream_t s) {
   cf_status st = raster_prepare(h, c, s);
@@ -2174,20 +2186,80 @@ cf_status cf_line_search(cf_raster* raster, cf_corr_search* search, const float*
                                                 d_num_valid, nullptr, stream);
     return r;
   };
+  // The best trial's outputs are kept on the search handle while the trials
+  // run (ls_keep_kernel applies the acceptance rule after each RMSE), so the
+  // accepted trial is not predicted and searched again: its records, maps and
+  // valid count are copied back, its transforms recomputed and the mesh
+  // re-skinned, which gives the bits of a repeated trial.
+  const size_t Pz = (size_t)P;
+  const bool pk_out = frame->d_pixel_knn_out && frame->d_pixel_knn_w_out;
+  auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  const size_t off_kept = al(sizeof(double) * (CF_LINE_SEARCH_TRIALS + 1));
+  const size_t off_nv = off_kept + 256, off_corr = off_nv + 256;
+  const size_t off_lv = al(off_corr + Pz * sizeof(cf_correspondence));
+  const size_t off_ln = al(off_lv + Pz * 12), off_hit = al(off_ln + Pz * 12);
+  const size_t off_pk = al(off_hit + Pz * 4), off_pw = al(off_pk + (pk_out ? Pz * 16 : 0));
+  const size_t keep_need = off_pw + (pk_out ? Pz * 16 : 0);
+  if (search->keep_bytes < keep_need) {  // grows with the frame (synchronous allocation)
+    CF_TRY(cudaStreamSynchronize(s));
+    cudaFree(search->keep);
+    search->keep = nullptr;
+    search->keep_bytes = 0;
+    CF_TRY(dalloc(&search->keep, keep_need));
+    search->keep_bytes = keep_need;
+  }
+  unsigned char* kb = search->keep;
+  double* best_chain = reinterpret_cast<double*>(kb);
+  int* kept = reinterpret_cast<int*>(kb + off_kept);
+  CF_TRY(cudaMemsetAsync(kept, 0xff, sizeof(int), s));
+  const int need = (int)(0.75f * (float)base_valid);
+  LsKeepArgs ka{};
+  ka.best0 = base_rmse;
+  ka.kept = kept;
+  ka.min_valid = params->min_valid_corrs;
+  ka.need = need;
+  struct KeepBuf {
+    int* live;
+    size_t off, words;
+  };
+  std::vector<KeepBuf> bufs = {{d_num_valid, off_nv, 1},
+                               {reinterpret_cast<int*>(d_corrs), off_corr, Pz * (sizeof(cf_correspondence) / 4)},
+                               {reinterpret_cast<int*>(lv), off_lv, Pz * 3},
+                               {reinterpret_cast<int*>(ln), off_ln, Pz * 3},
+                               {hit, off_hit, Pz}};
+  if (pk_out) {
+    bufs.push_back({frame->d_pixel_knn_out, off_pk, Pz * 4});
+    bufs.push_back({reinterpret_cast<int*>(frame->d_pixel_knn_w_out), off_pw, Pz * 4});
+  }
+  ka.nbuf = (int)bufs.size();
+  for (int i = 0; i < ka.nbuf; ++i) {
+    ka.src[i] = bufs[i].live;
+    ka.dst[i] = reinterpret_cast<int*>(kb + bufs[i].off);
+    ka.words[i] = bufs[i].words;
+  }
   CF_TRY(cudaMemcpyAsync(d_scratch_transforms, d_transforms, tbytes, cudaMemcpyDeviceToDevice, s));  // save
   for (int t = 0; t < CF_LINE_SEARCH_TRIALS && st == CF_OK; ++t) {
     st = apply(scales[t]);
     if (st == CF_OK) st = from_cuda(launch_corr_rmse(d_corrs, P, partials, slots + 3 * t, d_num_valid, s));
+    if (st == CF_OK) {
+      ka.slot = slots + 3 * t;
+      ka.best_in = t > 0 ? best_chain + t : nullptr;
+      ka.best_out = best_chain + t + 1;
+      ka.trial = t;
+      st = from_cuda(launch_ls_keep(ka, s));
+    }
   }
   if (st != CF_OK) {
     cudaMemcpyAsync(d_transforms, d_scratch_transforms, tbytes, cudaMemcpyDeviceToDevice, s);
     return st;
   }
   double h[3 * CF_LINE_SEARCH_TRIALS];
+  int h_kept = -1;
   CF_TRY(cudaMemcpyAsync(h, slots, sizeof(h), cudaMemcpyDeviceToHost, s));
+  CF_TRY(cudaMemcpyAsync(&h_kept, kept, sizeof(int), cudaMemcpyDeviceToHost, s));
   CF_TRY(cudaStreamSynchronize(s));
   // the acceptance of each trial (fusion_app.h:575-582)
-  const int need = (int)(0.75f * (float)base_valid);
+  int best_t = -1;
   for (int t = 0; t < CF_LINE_SEARCH_TRIALS; ++t) {
     const double sum = h[3 * t], wsum = h[3 * t + 1];
     const int valid = (int)h[3 * t + 2];
@@ -2197,11 +2269,35 @@ cf_status cf_line_search(cf_raster* raster, cf_corr_search* search, const float*
     if (valid >= params->min_valid_corrs && valid >= need && std::isfinite(rmse) && rmse < *best_rmse) {
       *best_rmse = rmse;
       *best_scale = scales[t];
+      best_t = t;
     }
   }
   if (*best_scale == 0.f) {  // fusion_app.h:586-592: restore and stop; the maps stay the last trial's
     CF_TRY(cudaMemcpyAsync(d_transforms, d_scratch_transforms, tbytes, cudaMemcpyDeviceToDevice, s));
-  } else {
+  } else if (h_kept == best_t) {
+    // the accepted trial's transforms (as apply computes them), its skinned
+    // mesh (the prediction's skinning launches), its records and maps
+    CF_TRY(cudaMemcpyAsync(d_transforms, d_scratch_transforms, tbytes, cudaMemcpyDeviceToDevice, s));
+    st = cf_scale_delta(d_delta_x, num_nodes, params->max_update_rot, params->max_update_trans, *best_scale,
+                        d_scratch_delta, stream);
+    if (st == CF_OK) st = cf_warp_apply_twist(d_transforms, d_scratch_delta, num_nodes, params->max_update_rot,
+                                              params->max_update_trans, 1.0f, stream);
+    if (st != CF_OK) return st;
+    RasterCall c{};
+    c.skin = true;
+    c.canon = d_mesh_canonical;
+    c.warped = d_mesh_warped;
+    c.V = num_vertices;
+    c.nodes = d_nodes;
+    c.T = d_transforms;
+    c.N = num_nodes;
+    c.vk = d_voxel_knn;
+    c.vw = d_voxel_knn_w;
+    c.grid = *grid;
+    CF_TRY(raster_skin(raster, c, s));
+    for (const KeepBuf& kbuf : bufs)
+      CF_TRY(cudaMemcpyAsync(kbuf.live, kb + kbuf.off, kbuf.words * 4, cudaMemcpyDeviceToDevice, s));
+  } else {  // (the device's record disagrees with the host's choice: predict and search again)
     st = apply(*best_scale);
     if (st != CF_OK) return st;
   }

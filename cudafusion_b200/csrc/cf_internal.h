@@ -255,6 +255,19 @@ cudaError_t launch_update_stats(const float* dx, int N, float update_scale, floa
                                 double* sums, unsigned* maxima, int* finite, cudaStream_t s);
 cudaError_t launch_scale_delta(const float* dx, int N, float max_rot, float max_trans, float scale, float* out,
                                cudaStream_t s);
+// The line search's record of its best trial (ls_keep_kernel).
+struct LsKeepArgs {
+  const double* slot;
+  const double* best_in;  // nullptr: best0
+  double best0;
+  double* best_out;
+  int* kept;
+  int trial, min_valid, need, nbuf;
+  const int* src[8];
+  int* dst[8];
+  size_t words[8];
+};
+cudaError_t launch_ls_keep(const LsKeepArgs& a, cudaStream_t s);
 cudaError_t launch_corr_rmse(const cf_correspondence* corrs, int M, double* partials, double* out, const int* valid,
                              cudaStream_t s);
 cudaError_t launch_tsdf_plain(const cf_deform_node* nodes, const cf_dual_quat* T, cf_dual_quat* plain, int N,

@@ -141,7 +141,38 @@ __global__ void rmse_final_kernel(const double* __restrict__ part, int blocks, d
   if (threadIdx.x == 2 && valid) out[2] = (double)*valid;
 }
 
+// After a trial's RMSE (slot: its sum, wsum and valid count): whether the
+// trial is the best so far under the line search's acceptance rule
+// (fusion_app.h:575-582, the host's arithmetic: IEEE double quotient and
+// square root), chaining the best RMSE from best_in (or best0) to best_out;
+// a kept trial's index goes to *kept and its outputs (4-byte words) are
+// copied aside, so that the accepted trial need not be predicted and searched
+// again.
+__global__ void __launch_bounds__(256) ls_keep_kernel(LsKeepArgs a) {
+  const double sum = a.slot[0], wsum = a.slot[1];
+  const int valid = (int)a.slot[2];
+  const double rmse = wsum > 0.0 ? sqrt(sum / wsum) : (double)INFINITY;
+  const double best = a.best_in ? *a.best_in : a.best0;
+  const bool take = valid >= a.min_valid && valid >= a.need && isfinite(rmse) && rmse < best;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *a.best_out = take ? rmse : best;
+    if (take) *a.kept = a.trial;
+  }
+  if (!take) return;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (int b = 0; b < a.nbuf; ++b) {
+    const int* src = a.src[b];
+    int* dst = a.dst[b];
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.words[b]; i += stride) dst[i] = src[i];
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_ls_keep(const LsKeepArgs& a, cudaStream_t s) {
+  ls_keep_kernel<<<296, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_update_stats(const float* dx, int N, float update_scale, float max_rot, float max_trans,
                                 double* sums, unsigned* maxima, int* finite, cudaStream_t s) {

@@ -79,17 +79,19 @@ class LineSearch:
         self.rmse = torch.empty(_lib.CF_LINE_SEARCH_SCRATCH, dtype=torch.float64, device=device)
 
     def run(self, raster, search, mesh, frame, transforms, delta_x, base_rmse, base_valid, params=None,
-            corr_params=None, warped=None, stream=None):
+            corr_params=None, warped=None, pixel_knn_out=None, stream=None):
         """One GN iteration's line search (fusion_app.h:493-641): `transforms`
         (device DQs of mesh's graph) is updated in place; frame's live maps and
-        hit voxels, search.corrs and search.num_valid hold the accepted warp's.
-        Returns dict(best_scale, best_rmse, trial_rmse, trial_valid)."""
+        hit voxels, search.corrs and search.num_valid hold the accepted warp's,
+        and so do the (ids, weights) device tensors pixel_knn_out (4 per
+        pixel) when given.  Returns dict(best_scale, best_rmse, trial_rmse,
+        trial_valid)."""
         from .corr import CorrParams
 
         params = params or LineSearchParams()
         corr_params = corr_params or CorrParams()
         warped = warped if warped is not None else torch.empty_like(mesh.canonical)
-        f = frame_args(frame, use_voxels=True)
+        f = frame_args(frame, use_voxels=True, pixel_knn_out=pixel_knn_out)
         cam = frame.camera()
         bs = ctypes.c_float()
         br = ctypes.c_double()

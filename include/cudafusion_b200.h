@@ -646,9 +646,13 @@ CF_API cf_status cf_correspondence_rmse(const cf_correspondence* d_corrs, int nu
  * RMSE is finite and below the best so far (starting at base_rmse).  The
  * ten trials are enqueued without synchronising and read back once.  Then
  * the saved transforms are restored and, when a trial was kept, its
- * increment applied and the mesh and correspondences predicted and searched
- * again for it; when none was, the maps and records stay the last trial's,
- * as in the reference.  d_transforms holds the warp on entry and the
+ * increment applied, the mesh skinned with it and the kept trial's maps,
+ * hit voxels, records, valid count and pixel node lists put back (a copy of
+ * that trial's outputs held on `search` while the trials run: the same bits
+ * as predicting and searching again); when none was, the maps and records
+ * stay the last trial's, as in the reference.  The first call, and a call
+ * on a larger frame, allocates that copy (about 130 B per pixel) and
+ * synchronises.  d_transforms holds the warp on entry and the
  * accepted warp on exit; d_scratch_transforms (num_nodes), d_scratch_delta
  * (6 num_nodes) and d_scratch_rmse (CF_LINE_SEARCH_SCRATCH doubles) are the
  * caller's device scratch.  *best_scale = 0 means no update; trial_rmse /

@@ -8,7 +8,10 @@ decision exactly.  The device RMSE agrees with the oracle's sequential sum to
 1e-12 relative.  The line search's ten trials agree with the reference's
 host loop driven step by step (restore, scale, twist, predict, search,
 download the records, RMSE on the host): the same valid counts, RMSEs to
-1e-12, the same chosen scale and bit-identical transforms afterwards."""
+1e-12, the same chosen scale and bit-identical transforms afterwards, and
+the accepted trial's warped mesh, live maps, hit voxels, records, valid
+count and pixel node lists bit for bit (the last trial's maps and records
+when none is accepted)."""
 import ctypes
 import dataclasses
 
@@ -17,7 +20,7 @@ import pytest
 import torch
 
 from cudafusion_b200 import _lib, synth
-from cudafusion_b200.corr import CorrespondenceSearch, CorrParams, DeviceCorrFrame
+from cudafusion_b200.corr import CORR_BYTES, CorrespondenceSearch, CorrParams, DeviceCorrFrame
 from cudafusion_b200.linesearch import (LineSearch, LineSearchParams, correspondence_rmse, scale_delta,
                                         validate_update)
 from cudafusion_b200.raster import DeviceMesh, LiveSurfaceRaster
@@ -123,9 +126,11 @@ def _scene(seed=96):
     return est, frame, dx.astype(np.float32)
 
 
-def test_line_search_matches_host_flow(oracle):
+@pytest.mark.parametrize("knn_out", [True, False])
+def test_line_search_matches_host_flow(oracle, knn_out):
     est, frame, dx = _scene()
     N = est.nodes.shape[0]
+    P = 96 * 72
     mesh = DeviceMesh(est)
     dframe = DeviceCorrFrame(frame)
     raster = LiveSurfaceRaster(96, 72)
@@ -139,14 +144,19 @@ def test_line_search_matches_host_flow(oracle):
         w = torch.empty_like(mesh.canonical)
         mesh.transforms = T
         raster.predict(mesh, w)
-        dframe.live_vertices.copy_(raster.live_vertices[: 3 * 96 * 72])
-        dframe.live_normals.copy_(raster.live_normals[: 3 * 96 * 72])
-        dframe.hit_voxel_idx.copy_(raster.hit_voxel_idx[: 96 * 72])
-        n = search.find_correspondences(dframe, cprm, use_voxels=True)
-        return n, search.records(96 * 72)
+        dframe.live_vertices.copy_(raster.live_vertices[: 3 * P])
+        dframe.live_normals.copy_(raster.live_normals[: 3 * P])
+        dframe.hit_voxel_idx.copy_(raster.hit_voxel_idx[: P])
+        search.launch(dframe, cprm, use_voxels=True, pixel_knn_out=True)
+        torch.cuda.synchronize()
+        n = int(search.num_valid.item())
+        outs = dict(warped=w, lv=dframe.live_vertices.clone(), ln=dframe.live_normals.clone(),
+                    hit=dframe.hit_voxel_idx.clone(), corrs=search.corrs[: P * CORR_BYTES].clone(),
+                    pk=search.pixel_knn.clone(), pkw=search.pixel_knn_w.clone())
+        return n, search.records(P), outs
 
     # the base: the warp as it stands
-    base_valid, base_recs = predict_and_search(T0.clone())
+    base_valid, base_recs, _ = predict_and_search(T0.clone())
     base_rmse = oracle.corr_rmse(base_recs)[2]
     # the reference's host loop, step by step
     u = lp.update_scale
@@ -158,30 +168,47 @@ def test_line_search_matches_host_flow(oracle):
         _lib.check(_lib.lib().cf_warp_apply_twist(ctypes.c_void_p(T.data_ptr()), ctypes.c_void_p(sd.data_ptr()), N,
                                                   lp.max_update_rot, lp.max_update_trans, 1.0, None), "twist")
         torch.cuda.synchronize()
-        n, recs = predict_and_search(T)
-        host.append((n, oracle.corr_rmse(recs)[2], T.clone()))
+        n, recs, outs = predict_and_search(T)
+        host.append((n, oracle.corr_rmse(recs)[2], T.clone(), outs))
     best, best_rmse = 0.0, base_rmse
     need = int(np.float32(0.75) * np.float32(base_valid))
-    for sc, (n, rm, _) in zip(scales, host):
+    for sc, (n, rm, _, _) in zip(scales, host):
         if n >= lp.min_valid_corrs and n >= need and np.isfinite(rm) and rm < best_rmse:
             best, best_rmse = sc, rm
-    # the device line search from the same start
+    # the device line search from the same start, its outputs poisoned first
     mesh.transforms = T0.clone()
     Tls = mesh.transforms
+    warped = torch.full_like(mesh.canonical, float("nan"))
+    pk = torch.full((P * 4,), -7, dtype=torch.int32, device="cuda")
+    pkw = torch.full((P * 4,), float("nan"), dtype=torch.float32, device="cuda")
+    search.corrs.fill_(0xA5)
     ls = LineSearch(N)
-    res = ls.run(raster, search, mesh, dframe, Tls, d_dx, base_rmse, base_valid, lp, cprm)
-    for t, (n, rm, _) in enumerate(host):
+    res = ls.run(raster, search, mesh, dframe, Tls, d_dx, base_rmse, base_valid, lp, cprm, warped=warped,
+                 pixel_knn_out=(pk, pkw) if knn_out else None)
+    torch.cuda.synchronize()
+    for t, (n, rm, _, _) in enumerate(host):
         assert res["trial_valid"][t] == n
         assert abs(res["trial_rmse"][t] - rm) <= 1e-12 * rm, (t, res["trial_rmse"][t], rm)
     assert res["best_scale"] == np.float32(best)
     if best != 0.0:
-        want = host[scales.index(best)][2]
-        assert torch.equal(Tls, want)
+        n_want, _, T_want, outs = host[scales.index(best)]
+        assert torch.equal(Tls, T_want)
         assert abs(res["best_rmse"] - best_rmse) <= 1e-12 * best_rmse
-        # the records are the accepted warp's
-        assert int(search.num_valid.item()) == host[scales.index(best)][0]
+        # the accepted warp's skinned mesh (the host flow's skins the same warp)
+        assert torch.equal(warped.view(torch.int32), outs["warped"].view(torch.int32))
     else:
+        n_want, _, _, outs = host[-1]
         assert torch.equal(Tls, T0)
+    # maps, hit voxels, records, valid count and node lists: the accepted
+    # trial's (the last trial's when none was accepted)
+    assert int(search.num_valid.item()) == n_want
+    assert torch.equal(dframe.live_vertices.view(torch.int32), outs["lv"].view(torch.int32))
+    assert torch.equal(dframe.live_normals.view(torch.int32), outs["ln"].view(torch.int32))
+    assert torch.equal(dframe.hit_voxel_idx, outs["hit"])
+    assert torch.equal(search.corrs[: P * CORR_BYTES], outs["corrs"])
+    if knn_out:
+        assert torch.equal(pk, outs["pk"])
+        assert torch.equal(pkw.view(torch.int32), outs["pkw"].view(torch.int32))
     print(f"base RMSE {base_rmse:.6e} ({base_valid} valid); trials {np.array(res['trial_rmse'])}; "
           f"best scale {res['best_scale']}")
 
