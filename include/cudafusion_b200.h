@@ -651,9 +651,9 @@ CF_API cf_status cf_correspondence_rmse(const cf_correspondence* d_corrs, int nu
  * that trial's outputs held on `search` while the trials run: the same bits
  * as predicting and searching again); when none was, the maps and records
  * stay the last trial's, as in the reference.  The first call, and a call
- * on a larger frame, allocates that copy (about 130 B per pixel) and
- * synchronises.  d_transforms holds the warp on entry and the
- * accepted warp on exit; d_scratch_transforms (num_nodes), d_scratch_delta
+ * on a larger frame, allocates that copy (104 B per pixel, 136 B with the
+ * pixel node lists) and synchronises.  d_transforms holds the warp on entry
+ * and the accepted warp on exit; d_scratch_transforms (num_nodes), d_scratch_delta
  * (6 num_nodes) and d_scratch_rmse (CF_LINE_SEARCH_SCRATCH doubles) are the
  * caller's device scratch.  *best_scale = 0 means no update; trial_rmse /
  * trial_valid (CF_LINE_SEARCH_TRIALS each, may be NULL) receive every
