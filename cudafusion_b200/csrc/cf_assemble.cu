@@ -30,6 +30,9 @@ constexpr int kColMap = 16384;      // nodes up to which expand finds a column t
 constexpr int kStageCap = 896;
 constexpr int kRowEdges = 32;
 constexpr int kRound = 32 * kEpl;
+// staged incidences per assembly thread (the stage capacity is kStageCap)
+constexpr int kIncPerThread = (kStageCap + kThreads - 1) / kThreads;
+static_assert(kIncPerThread * kThreads >= kStageCap && kStageCap % 4 == 0, "assembly staging layout");
 
 __device__ __forceinline__ int find_col(const int* cols, int n, int v) {
   int lo = 0, hi = n - 1;
@@ -335,37 +338,55 @@ __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern p
   const int a0 = m1.z, a1 = m1.w, na = min(a1, kRowEdges);
   const int be0 = m2.x;  // the row's off-diagonal upper blocks are u0+1 .. u0+nb-1
   const int be1 = m2.y, nbe = min(be1, kRowEdges);
+  // Every plain load is issued before the first cp.async (whose memory
+  // clobber would otherwise hold later loads back), so that the row's
+  // incidences, ARAP incidences and block information arrive in one round
+  // trip after the metadata; everything else is copied asynchronously.
+  float4* su = stage_buf;
+  float4* sn = stage_buf + cap;
+  int ev[kIncPerThread];
+#pragma unroll
+  for (int k = 0; k < kIncPerThread; k++) {
+    const int ii = threadIdx.x + k * kThreads;
+    ev[k] = ii < R.ns ? __ldg(R.inc + ii) : 0;
+  }
+  // (threads from the back take the edges, so that they overlap the block-info loads)
+  const int te = kThreads - 1 - threadIdx.x;
+  const bool row_edge = te < na, blk_edge = te >= kRowEdges && te < kRowEdges + nbe;
+  int einc = 0;
+  if (row_edge) einc = __ldg(pt.arap_row_inc + a0 + te);
+  else if (blk_edge) einc = __ldg(pt.arap_blk_edge + be0 + (te - kRowEdges));
   for (int k = threadIdx.x; k < nb; k += kThreads) {
     const int pos = dpos + k;
     s_blk[k] = make_int4(pt.seg_off[pos] - 4 * i0, pt.seg_cnt[pos], pt.col_idx[pos], pt.trans_pos[pos]);
     s_boff[k] = k == 0 ? 0 : pt.arap_blk_ptr[u0 + k] - be0;
   }
-  // (threads from the back, so that they overlap the block-info loads)
-  const int te = kThreads - 1 - threadIdx.x;
-  if (te < na) {
-    const int inc = pt.arap_row_inc[a0 + te];
-    const int ed = inc >> 1, role = inc & 1;
+  // the entries, 16 B at a time (the row's list starts 16-B aligned and
+  // holds 4 slots per incidence, so the last chunk stays inside it)
+  for (int t4 = threadIdx.x; 4 * t4 < R.nt; t4 += kThreads) cp_async16(s_trip + 4 * t4, R.trip + 4 * t4);
+  if (row_edge) {
+    const int ed = einc >> 1, role = einc & 1;
     s_erole[te] = role;
     const float4* src = pt.edge_terms + (size_t)kEdgeTerms4 * ed + 7 * role;
 #pragma unroll
     for (int k = 0; k < 7; k++) cp_async16(s_eterm + 7 * te + k, src + k);
-    s_eng[te] = role == 0 ? pt.edge_energy[ed] : 0.0;
-  } else if (te >= kRowEdges && te < kRowEdges + nbe) {
-    const int e = te - kRowEdges;
-    const float4* src = pt.edge_terms + (size_t)kEdgeTerms4 * pt.arap_blk_edge[be0 + e] + 14;
+    if (role == 0) cp_async8(s_eng + te, pt.edge_energy + ed);
+    else s_eng[te] = 0.0;
+  } else if (blk_edge) {
+    const float4* src = pt.edge_terms + (size_t)kEdgeTerms4 * einc + 14;
 #pragma unroll
-    for (int k = 0; k < 9; k++) cp_async16(s_bterm + 9 * e + k, src + k);
+    for (int k = 0; k < 9; k++) cp_async16(s_bterm + 9 * (te - kRowEdges) + k, src + k);
   }
-  for (int t = threadIdx.x; t < R.nt; t += kThreads) s_trip[t] = __ldg(R.trip + t);
-  float4* su = stage_buf;
-  float4* sn = stage_buf + cap;
-  for (int ii = threadIdx.x; ii < R.ns; ii += kThreads) {
-    const int e = __ldg(R.inc + ii);
-    const int c = e >> 2;
-    s_a[ii] = e & 3;
-    cp_async16(su + ii, w.c_srcfw + c);
-    cp_async16(sn + ii, w.c_nres + c);
-    cp_async16(stage_buf + 2 * cap + ii, w.pk_ws + c);
+#pragma unroll
+  for (int k = 0; k < kIncPerThread; k++) {
+    const int ii = threadIdx.x + k * kThreads;
+    if (ii < R.ns) {
+      const int c = ev[k] >> 2;
+      s_a[ii] = ev[k] & 3;
+      cp_async16(su + ii, w.c_srcfw + c);
+      cp_async16(sn + ii, w.c_nres + c);
+      cp_async16(stage_buf + 2 * cap + ii, w.pk_ws + c);
+    }
   }
   cp_async_commit_wait_all();
   // each thread turns the records it staged into the factors (its own
@@ -377,13 +398,21 @@ __global__ void __launch_bounds__(kThreads, 3) assemble_kernel(Work w, Pattern p
     sn[ii] = n;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    int run = 0;
-    for (int k = 0; k < nb; k++) {
-      s_wpre[k] = run;
-      run += (s_blk[k].y + 31) >> 5;
+  if (wid == 0) {  // window prefix over the blocks: a warp scan, 32 blocks at a time
+    int carry = 0;
+    for (int k0 = 0; k0 < nb; k0 += 32) {
+      const int k = k0 + lane;
+      const int v = k < nb ? (s_blk[k].y + 31) >> 5 : 0;
+      int incl = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int x = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += x;
+      }
+      if (k < nb) s_wpre[k] = carry + incl - v;
+      carry += __shfl_sync(0xffffffffu, incl, 31);
     }
-    s_wpre[nb] = run;
+    if (lane == 0) s_wpre[nb] = carry;
   }
   __syncthreads();
 

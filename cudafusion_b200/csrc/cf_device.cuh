@@ -439,10 +439,14 @@ __device__ __forceinline__ float warp_sum_f(float v) {
 }
 
 // ---- memory-order primitives for the bounded grid barrier ----
-// asynchronous global -> shared copies (16 B: both addresses 16-B aligned; 4 B: 4-B aligned)
+// asynchronous global -> shared copies (16, 8 or 4 B: both addresses aligned to the size)
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gsrc) : "memory");
 }
 __device__ __forceinline__ void cp_async4(void* smem_dst, const void* gsrc) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
