@@ -37,6 +37,14 @@ __device__ __forceinline__ DQ load_dq(const cf_dual_quat* p) {
   d.d = __ldg(q + 1);
   return d;
 }
+// through L1: for DQs written by an earlier launch and not during this one
+__device__ __forceinline__ DQ load_dq_ldg(const cf_dual_quat* p) {
+  const float4* q = reinterpret_cast<const float4*>(p);
+  DQ d;
+  d.r = __ldg(q);
+  d.d = __ldg(q + 1);
+  return d;
+}
 __device__ __forceinline__ DQ load_dq_cg(const cf_dual_quat* p) {
   const float4* q = reinterpret_cast<const float4*>(p);
   DQ d;
@@ -225,7 +233,7 @@ __device__ __forceinline__ float3 blend_warp(float3 p, int4 ids, float4 ws, cons
     int nid = idv[k];
     float w = wv[k];
     if (nid < 0 || nid >= N || w < 1e-8f) continue;
-    DQ d = load_dq_cg(plain + nid);
+    DQ d = load_dq_ldg(plain + nid);  // (the plain DQs come from an earlier launch)
     if (qdot(d.r, br) < 0.f) {
       d.r.x = -d.r.x; d.r.y = -d.r.y; d.r.z = -d.r.z; d.r.w = -d.r.w;
       d.d.x = -d.d.x; d.d.y = -d.d.y; d.d.z = -d.d.z; d.d.w = -d.d.w;
@@ -395,7 +403,7 @@ __device__ __forceinline__ Edge eval_edge(const cf_deform_node* nodes, const cf_
   const float* nwp = reinterpret_cast<const float*>(nodes + i) + 15 + k;  // neighbor_w[k]
   float nw = fmaxf(__ldg(nwp), 0.05f);
   float3 xi = node_pos(nodes, i), xj = node_pos(nodes, j);
-  DQ Ti = load_dq_cg(T + i), Tj = load_dq_cg(T + j);
+  DQ Ti = load_dq_ldg(T + i), Tj = load_dq_ldg(T + j);  // (T comes from an earlier launch)
   float3 ti_xj = dq_transform_point_centered(Ti, xj, xi);
   float3 ti_xi = dq_transform_point_centered(Ti, xi, xi);
   float3 tj_xj = dq_transform_point_centered(Tj, xj, xj);

@@ -103,7 +103,7 @@ __device__ __forceinline__ float3 ts_warp(float3 p, int4 ids, float4 ws, const c
     const int nid = idv[k];
     const float w = wv[k];
     if (nid < 0 || nid >= N || w < 1e-8f) continue;
-    DQ d = load_dq_cg(plain + nid);
+    DQ d = load_dq_ldg(plain + nid);  // (the plain DQs come from an earlier launch)
     if (ts_qdot(d.r, br) < 0.f) {
       d.r = make_float4(-d.r.x, -d.r.y, -d.r.z, -d.r.w);
       d.d = make_float4(-d.d.x, -d.d.y, -d.d.z, -d.d.w);
