@@ -138,6 +138,9 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_cluster_kernel(CluArgs P) {
   double* sParts = reinterpret_cast<double*>(smem + L.parts);
   double* sRed = reinterpret_cast<double*>(smem + L.red);
   const int n6 = nrows * 6, h6 = nhalo * 6;
+  int spl_log = 0;  // lanes per row element of the SpMV: 1, 2 or 4, all in one pass
+  while (spl_log < 2 && (n6 << (spl_log + 1)) <= kThreads) spl_log++;
+  const int spl = 1 << spl_log;
   int* err = w.err;
   PhaseClock clk((a.timers && crank == 0 && tid == 0) ? a.timers : nullptr);
 
@@ -283,27 +286,34 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_cluster_kernel(CluArgs P) {
     __syncthreads();
     clk.mark(5);  // p and halo
     // ---- Ap (solver_kernels.cu:406-432): the upper blocks of own rows, and
-    //      their transposed products pushed to the rows of their columns ----
-    for (int t = tid; t < n6; t += kThreads) {
-      const int i = t / 6, c = t % 6;
-      float pi[6];
-#pragma unroll
-      for (int q = 0; q < 6; q++) pi[q] = V[i * 6 + q];
+    //      their transposed products pushed to the rows of their columns.
+    //      spl adjacent lanes per row element (as many as the CTA's threads
+    //      allow, up to 4): lane k takes the row's blocks k, k + spl, ...,
+    //      the lanes' sums combined by an xor butterfly ----
+    for (int u0 = 0; u0 < n6 * spl; u0 += kThreads) {
+      const int u = u0 + tid, t = u >> spl_log, kk = u & (spl - 1);
       float y = 0.f;
-      for (int k = sUrow[i]; k < sUrow[i + 1]; k++) {
-        const float* Ab = sA + k * 36;
-        const float* vj = V + sOpnd[k] * 6;
+      if (t < n6) {
+        const int i = t / 6, c = t % 6;
+        float pi[6];
 #pragma unroll
-        for (int q = 0; q < 6; q++) y = __fmaf_rn(Ab[c * 6 + q], vj[q], y);
-        const int pk = sPush[k];
-        if (pk >= 0) {
-          float u = 0.f;
+        for (int q = 0; q < 6; q++) pi[q] = V[i * 6 + q];
+        for (int k = sUrow[i] + kk; k < sUrow[i + 1]; k += spl) {
+          const float* Ab = sA + k * 36;
+          const float* vj = V + sOpnd[k] * 6;
 #pragma unroll
-          for (int q = 0; q < 6; q++) u = __fmaf_rn(Ab[q * 6 + c], pi[q], u);
-          cluster.map_shared_rank(sRecv, pk >> 24)[(pk & 0xffffff) * 6 + c] = u;
+          for (int q = 0; q < 6; q++) y = __fmaf_rn(Ab[c * 6 + q], vj[q], y);
+          const int pk = sPush[k];
+          if (pk >= 0) {
+            float uu = 0.f;
+#pragma unroll
+            for (int q = 0; q < 6; q++) uu = __fmaf_rn(Ab[q * 6 + c], pi[q], uu);
+            cluster.map_shared_rank(sRecv, pk >> 24)[(pk & 0xffffff) * 6 + c] = uu;
+          }
         }
       }
-      sAp[t] = y;
+      for (int o = spl >> 1; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+      if (kk == 0 && t < n6) sAp[t] = y;
     }
     clk.mark(6);  // upper products, pushes
     cluster.sync();  // B: every transposed product delivered
