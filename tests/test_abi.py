@@ -89,3 +89,43 @@ def test_library_is_sm100a(cflib):
     ELF targets; nothing is disassembled)."""
     out = os.popen(f"cuobjdump --list-elf {cflib._name} 2>/dev/null").read()
     assert "sm_100a" in out
+
+
+def test_pipeline_argument_errors_without_device(cflib):
+    """The pipeline entry points check their arguments before any CUDA call:
+    null handles and outputs, negative sizes and sizes past the handles'
+    index range return status codes; empty work succeeds."""
+    from cudafusion_b200 import _lib
+
+    bad, cap = _lib.CF_ERR_INVALID_ARG, _lib.CF_ERR_CAPACITY
+    h = ctypes.c_void_p()
+    # handles
+    assert cflib.cf_raster_create(64, 48, None) == bad
+    assert cflib.cf_raster_create(0, 48, ctypes.byref(h)) == bad and not h.value
+    assert cflib.cf_raster_create(1 << 16, 1 << 16, ctypes.byref(h)) == cap and not h.value
+    assert cflib.cf_corr_search_create(64, 48, None) == bad
+    assert cflib.cf_corr_search_create(64, -1, ctypes.byref(h)) == bad and not h.value
+    assert cflib.cf_corr_search_create(1 << 15, 1 << 15, ctypes.byref(h)) == cap and not h.value
+    # calls on a null handle
+    assert cflib.cf_find_correspondences(*([None] * 10)) == bad
+    assert cflib.cf_predict_live_surface(None, None, None, None, 0, 0, None, None, 0, None, None, None, None, None,
+                                         None, None, None, None) == bad
+    ls = [None] * 32
+    for k in (5, 6, 10, 23):
+        ls[k] = 0
+    ls[22] = 0.0
+    assert cflib.cf_line_search(*ls) == bad
+    # the update's statistics, scaled increment and RMSE
+    lp = _lib.LineSearchParams()
+    stats = _lib.UpdateStats()
+    assert cflib.cf_validate_update(None, -1, ctypes.byref(lp), ctypes.byref(stats), None) == bad
+    assert cflib.cf_validate_update(None, 4, ctypes.byref(lp), ctypes.byref(stats), None) == bad
+    assert cflib.cf_scale_delta(None, -1, 0.1, 0.1, 1.0, None, None) == bad
+    assert cflib.cf_scale_delta(None, 0, 0.1, 0.1, 1.0, None, None) == 0
+    assert cflib.cf_scale_delta(None, 8, 0.1, 0.1, 1.0, None, None) == bad
+    assert cflib.cf_correspondence_rmse(None, -1, None, None, None) == bad
+    assert cflib.cf_correspondence_rmse(None, 10, None, None, None) == bad
+    # the volume's integration and kNN field without a volume description
+    assert cflib.cf_tsdf_integrate(None, None, None, None, None, None, None, 0, None, None, None, 0, None,
+                                   None) == bad
+    assert cflib.cf_compute_voxel_knn(None, None, None, 0, None, None, None) == bad
